@@ -1,0 +1,210 @@
+/*
+ * sap_b200.h — C ABI of the B200-native SPIKE-preconditioned Krylov solver.
+ *
+ * The reference (spikegpu/SaPLibrary) exposes this path only as C++
+ * templates; every entry point below names the reference interface it
+ * replaces (file:line, relative to the reference project root).  Plain
+ * pointers and sizes only: no CUDA, torch or C++ types cross the boundary.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 on success, one of the
+ *    sap::system_error::Reason values (sap/exception.h:16-23) for the
+ *    reference's own failures, or one of the SAP_ERR_* codes below.
+ *  - `memspace` arguments say where a caller buffer lives:
+ *    SAP_HOST (pageable or pinned host memory) or SAP_DEVICE (memory of the
+ *    current CUDA device).
+ *  - All device work of one solver runs on that solver's own CUDA stream;
+ *    a call returns after its results are complete (setup, update, solve),
+ *    except the *_async device-pointer helpers, which only enqueue.
+ *  - Handles are not re-entrant (the reference Solver is not either:
+ *    sap/solver.h:153-225 keeps mutable work vectors).
+ */
+#ifndef SAP_B200_H
+#define SAP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  SAP_OK = 0,
+  /* sap::system_error::Reason (sap/exception.h:16-23) */
+  SAP_ZERO_PIVOTING = -1,
+  SAP_NEGATIVE_DB_WEIGHT = -2,
+  SAP_ILLEGAL_UPDATE = -3,
+  SAP_ILLEGAL_SOLVE = -4,
+  SAP_MATRIX_SINGULAR = -5,
+  /* library errors with no reference counterpart */
+  SAP_ERR_INVALID_ARGUMENT = -100,
+  SAP_ERR_CUDA = -101,
+  SAP_ERR_OUT_OF_MEMORY = -102,
+  SAP_ERR_UNSUPPORTED = -103,
+  SAP_ERR_DEVICE_TIMEOUT = -104
+};
+
+enum { SAP_HOST = 0, SAP_DEVICE = 1 };
+
+/* KrylovSolverType (sap/common.h:71-82); CUSP solvers are not provided. */
+enum {
+  SAP_BICGSTAB_C = 0, SAP_GMRES_C = 1, SAP_CG_C = 2, SAP_CR_C = 3,
+  SAP_BICGSTAB1 = 4, SAP_BICGSTAB2 = 5, SAP_BICGSTAB = 6, SAP_MINRES = 7
+};
+/* FactorizationMethod (sap/common.h:86-89) */
+enum { SAP_LU_UL = 0, SAP_LU_ONLY = 1 };
+/* PreconditionerType (sap/common.h:94-98) */
+enum { SAP_PRECOND_SPIKE = 0, SAP_PRECOND_BLOCK = 1, SAP_PRECOND_NONE = 2 };
+/* Preconditioner value type: the Solver's PrecValueType template argument
+ * (sap/solver.h:153). */
+enum { SAP_PREC_FLOAT = 0, SAP_PREC_DOUBLE = 1 };
+
+/* sap::Options (sap/solver.h:52-81); same fields, same defaults
+ * (sap/solver.h:233-256).  Booleans are ints (0/1). */
+typedef struct sap_options {
+  int solverType;
+  int maxNumIterations;
+  double relTol;
+  double absTol;
+  int testDB;
+  int isSPD;
+  int saveMem;
+  int performReorder;
+  int performDB;
+  int dbFirstStageOnly;
+  int applyScaling;
+  int maxBandwidth;
+  int gpuCount;
+  double dropOffFraction;
+  int factMethod;
+  int precondType;
+  int safeFactorization;
+  int variableBandwidth;
+  int trackReordering;
+  int useBCR;
+  int ilu_level;
+} sap_options;
+
+/* sap::Stats (sap/solver.h:89-140); times in milliseconds as in the
+ * reference's timers (sap/timer.h). */
+typedef struct sap_stats {
+  double timeSetup, timeUpdate, timeSolve;
+  double time_DB, time_DB_pre, time_DB_first, time_DB_second, time_DB_post;
+  double d_p1, d_p1_ori, diag_dom, diag_dom_ori;
+  double time_reorder, time_dropOff, time_cpu_assemble, time_transfer;
+  double time_toBanded, time_offDiags, time_bandLU, time_bandUL;
+  double time_fullLU, time_assembly, time_shuffle;
+  int bandwidthReorder, bandwidthDB, bandwidth;
+  double nuKf, flops_LU;
+  int numPartitions;
+  double actualDropOff;
+  float numIterations;
+  double rhsNorm, residualNorm, relResidualNorm;
+  int actual_nnz;
+} sap_stats;
+
+typedef struct sap_solver sap_solver;   /* sap::Solver<Array,PrecValueType> */
+typedef struct sap_banded sap_banded;   /* sap::BandedMatrix<Array> */
+typedef struct sap_csr sap_csr;         /* cusp::csr_matrix<int,double,device> */
+typedef struct sap_spmv sap_spmv;       /* SpMV functor (MVBanded / SpmvCusp) */
+
+/* ---- errors ------------------------------------------------------------- */
+/* Message of the last failure on the calling thread (what() of the
+ * reference's sap::system_error, or the CUDA error string). */
+const char* sap_last_error(void);
+
+/* ---- options ------------------------------------------------------------ */
+/* Options::Options() (sap/solver.h:233-256). */
+int sap_options_default(sap_options* opts);
+
+/* ---- matrices ----------------------------------------------------------- */
+/* BandedMatrix(n, k, d) (sap/banded_matrix.h:59-95) from caller data: a
+ * row-major band of n*(2k+1) doubles, element (i,j) at i*(2k+1)+k+(j-i).
+ * The data is copied to the device. */
+int sap_banded_create(int n, int k, const double* band_rowmajor, int memspace,
+                      sap_banded** out);
+/* BandedMatrix(n, k, d) generated in place (sap/banded_matrix.h:59-95).
+ * dist: 0 = uniform[-10,10] from the C library rand() seeded with `seed`
+ * (the reference generator), 1 = uniform[-1,1], 2 = standard normal; the
+ * diagonal is d * (sum of |off-diagonals| of the row).  dists 1 and 2 use a
+ * counter-based generator, identical for any thread count. */
+int sap_banded_generate(int n, int k, double d, int dist, uint64_t seed, sap_banded** out);
+/* The generator of sap_banded_generate run on the host into `out`
+ * (n*(2k+1) doubles, row-major); needs no GPU. */
+int sap_generate_band_host(int n, int k, double d, int dist, uint64_t seed, double* out);
+/* Copy the row-major band back (host or device destination). */
+int sap_banded_copy_out(const sap_banded* A, double* dst, int memspace);
+int sap_banded_info(const sap_banded* A, int* n, int* k);
+int sap_banded_destroy(sap_banded* A);
+
+/* CSR matrix (int32 indices, FP64 values), copied to the device; the
+ * reference's cusp::csr_matrix<int,double,device_memory>. */
+int sap_csr_create(int n, int nnz, const int* row_offsets, const int* column_indices,
+                   const double* values, int memspace, sap_csr** out);
+int sap_csr_info(const sap_csr* A, int* n, int* nnz);
+int sap_csr_destroy(sap_csr* A);
+
+/* ---- SpMV functors (sap/spmv.h) ------------------------------------------ */
+/* MVBanded(A) (sap/spmv.h:27-74): y = A x on the row-major FP64 band. */
+int sap_spmv_banded_create(const sap_banded* A, sap_spmv** out);
+/* SpmvCusp(A) (sap/spmv.h:83-129): y = A x, FP64 CSR. */
+int sap_spmv_csr_create(const sap_csr* A, sap_spmv** out);
+/* A user operator: fn(ctx, x, y, stream) computes y = A x on device
+ * pointers, enqueued on `stream` (a cudaStream_t). */
+typedef void (*sap_spmv_fn)(void* ctx, const double* x, double* y, void* stream);
+int sap_spmv_callback_create(int n, sap_spmv_fn fn, void* ctx, sap_spmv** out);
+/* operator()(v, Av) (sap/spmv.h:39-56, 110-121); device pointers. */
+int sap_spmv_apply(sap_spmv* op, const double* x, double* y);
+int sap_spmv_destroy(sap_spmv* op);
+
+/* ---- solver --------------------------------------------------------------- */
+/* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297). */
+int sap_solver_create(int num_partitions, const sap_options* opts, int prec_dtype,
+                      sap_solver** out);
+int sap_solver_destroy(sap_solver* s);
+
+/* Solver::setup(A) (sap/solver.h:171, 339-404) for a BandedMatrix. */
+int sap_solver_setup_banded(sap_solver* s, const sap_banded* A);
+/* Solver::setup(A) for a CSR matrix (reordering per opts.performReorder). */
+int sap_solver_setup_csr(sap_solver* s, const sap_csr* A);
+
+/* Solver::update(entries) (sap/solver.h:174, 421-462): `entries` are the
+ * nnz new CSR values in the pattern given to setup.  *accepted is 0 when
+ * nnz differs from the setup matrix (the reference returns false). */
+int sap_solver_update(sap_solver* s, const double* entries, int64_t nnz, int memspace,
+                      int* accepted);
+
+/* Solver::solve(spmv, b, x) (sap/solver.h:177-179, 477-562).  b and x live
+ * in `memspace`; x is the initial guess on entry and the solution on exit.
+ * *converged receives the reference's bool return value. */
+int sap_solver_solve(sap_solver* s, sap_spmv* spmv, const double* b, double* x, int memspace,
+                     int* converged);
+
+/* Precond::operator()(v, z) (sap/precond.h:1370-1386): z = M^{-1} v on
+ * device pointers of length n. */
+int sap_precond_apply(sap_solver* s, const double* v, double* z);
+
+/* Solver::getStats() (sap/solver.h:182). */
+int sap_solver_get_stats(const sap_solver* s, sap_stats* out);
+/* getMonitorCode / getMonitorMessage (sap/solver.h:183-194). */
+int sap_solver_get_monitor(const sap_solver* s, int* code, const char** message);
+/* Number of rows, the effective half-bandwidth and partition count after
+ * setup (Precond::getBandwidth / getNumPartitions, sap/precond.h:152-157). */
+int sap_solver_info(const sap_solver* s, int* n, int* k, int* num_partitions);
+/* The cudaStream_t all device work of this solver is enqueued on. */
+void* sap_solver_stream(const sap_solver* s);
+/* Number of kernels this library has enqueued since load (all handles). */
+int64_t sap_kernel_launch_count(void);
+/* Live kernel timing with CUDA events on the launching stream: while a
+ * kernel name is selected, every launch of that kernel is bracketed by an
+ * event pair; sap_profile_read returns the summed duration (ms) and the
+ * number of launches since the selection (NULL or "" switches it off). */
+int sap_profile_select(const char* kernel_name);
+int sap_profile_read(double* total_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SAP_B200_H */

@@ -1,0 +1,136 @@
+"""ORACLE — test infrastructure only (not product code).
+
+CPU restatement of the SaP SPIKE-preconditioned BiCGStab(L) solve of the
+reference (see sap_oracle.cpp for the per-function citations).  Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline / reference leg may use
+it, and only as the checker or the CPU baseline; the product library never
+loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+SRC = os.path.join(HERE, "sap_oracle.cpp")
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", SRC, "-o", LIB], check=True)
+    return LIB
+
+
+class OrcResult(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int), ("iterations", ctypes.c_float), ("rhs_norm", ctypes.c_double),
+                ("res_norm", ctypes.c_double), ("rel_res_norm", ctypes.c_double), ("n", ctypes.c_int),
+                ("K", ctypes.c_int), ("P", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB)
+        vp, ip, dp, i = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int
+        L.orc_precond_create.restype = vp
+        L.orc_precond_create.argtypes = [i, i, i, i, i]
+        L.orc_precond_destroy.argtypes = [vp]
+        L.orc_setup_banded.argtypes = [vp, i, i, dp]
+        L.orc_setup_csr.argtypes = [vp, i, ip, ip, dp]
+        L.orc_info.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.orc_apply.argtypes = [vp, dp, dp]
+        L.orc_factor_copy.restype = ctypes.c_longlong
+        L.orc_factor_copy.argtypes = [vp, i, dp]
+        L.orc_spmv_banded.argtypes = [i, i, dp, dp, dp]
+        L.orc_spmv_csr.argtypes = [i, ip, ip, dp, dp, dp]
+        L.orc_solve.argtypes = [vp, i, i, dp, ip, ip, dp, dp, dp, i, i, ctypes.c_double, ctypes.c_double,
+                                ctypes.POINTER(OrcResult)]
+        L.orc_num_threads.restype = i
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Precond:
+    """The oracle's preconditioner: setup on a band or CSR matrix, apply."""
+
+    def __init__(self, P, fact=0, ptype=0, safe=False, dtype="float"):
+        self.h = lib().orc_precond_create(int(P), int(fact), int(ptype), int(bool(safe)),
+                                          0 if dtype == "float" else 1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_precond_destroy(self.h)
+            self.h = None
+
+    def setup_banded(self, band_rowmajor: np.ndarray, n: int, K: int) -> int:
+        self._band = np.ascontiguousarray(band_rowmajor, dtype=np.float64)
+        return lib().orc_setup_banded(self.h, n, K, _p(self._band))
+
+    def setup_csr(self, n, rp, ci, v) -> int:
+        self._csr = [np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
+                     np.ascontiguousarray(v, np.float64)]
+        return lib().orc_setup_csr(self.h, n, *[_p(a) for a in self._csr])
+
+    def info(self):
+        n, K, P = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lib().orc_info(self.h, ctypes.byref(n), ctypes.byref(K), ctypes.byref(P))
+        return n.value, K.value, P.value
+
+    def apply(self, v: np.ndarray) -> np.ndarray:
+        v = np.ascontiguousarray(v, np.float64)
+        z = np.empty_like(v)
+        lib().orc_apply(self.h, _p(v), _p(z))
+        return z
+
+    def factor(self, which: int) -> np.ndarray:
+        """0 band factors, 1 V tips, 2 W tips, 3 LU of S, 4 coupling blocks (as float64)."""
+        cnt = lib().orc_factor_copy(self.h, which, None)
+        out = np.empty(cnt, np.float64)
+        if cnt:
+            lib().orc_factor_copy(self.h, which, _p(out))
+        return out
+
+    def solve(self, b, x0=None, band=None, K=0, csr=None, L=2, maxit=100, reltol=1e-6, abstol=0.0):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        res = OrcResult()
+        if band is not None:
+            band = np.ascontiguousarray(band, np.float64)
+            lib().orc_solve(self.h, b.size, K, _p(band), None, None, None, _p(b), _p(x), L, maxit, reltol, abstol,
+                            ctypes.byref(res))
+        else:
+            rp, ci, v = [np.ascontiguousarray(a) for a in csr]
+            lib().orc_solve(self.h, b.size, 0, None, _p(rp), _p(ci), _p(v), _p(b), _p(x), L, maxit, reltol, abstol,
+                            ctypes.byref(res))
+        return x, res
+
+
+def spmv_banded(band, n, K, x):
+    band = np.ascontiguousarray(band, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty(n)
+    lib().orc_spmv_banded(n, K, _p(band), _p(x), _p(y))
+    return y
+
+
+def spmv_csr(rp, ci, v, x):
+    rp, ci, v, x = (np.ascontiguousarray(a) for a in (rp, ci, v, x))
+    y = np.empty(rp.size - 1)
+    lib().orc_spmv_csr(rp.size - 1, _p(rp), _p(ci), _p(v), _p(x), _p(y))
+    return y
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()

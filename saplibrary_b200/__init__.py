@@ -1,0 +1,403 @@
+"""saplibrary_b200 — B200-native SPIKE-preconditioned Krylov solver.
+
+Python mirror of the reference's public surface (spikegpu/SaPLibrary):
+``Options`` (sap/solver.h:52-81), ``Stats`` (sap/solver.h:89-140),
+``Solver`` (sap/solver.h:153-225), ``BandedMatrix`` (sap/banded_matrix.h),
+``MVBanded`` / ``SpmvCusp`` (sap/spmv.h) and ``SystemError``
+(sap/exception.h).  Every call goes through the C ABI of libsap_b200.so
+(include/sap_b200.h); there is no CPU fallback: importing the package fails
+when the shared library is missing.
+
+Arrays: numpy float64 arrays are host buffers; torch CUDA tensors (float64)
+are device buffers and are passed by pointer without copies.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libsap_b200.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        f"saplibrary_b200: {_LIB_PATH} is missing; build it with `python -m saplibrary_b200.build`")
+_lib = ctypes.CDLL(_LIB_PATH)
+
+# ---- enums (sap/common.h) ----------------------------------------------------
+BiCGStab_C, GMRES_C, CG_C, CR_C, BiCGStab1, BiCGStab2, BiCGStab, MINRES = range(8)
+LU_UL, LU_only = 0, 1
+Spike, Block, NoPrecond = 0, 1, 2
+HOST, DEVICE = 0, 1
+
+
+class SystemError(RuntimeError):  # noqa: A001 - mirrors sap::system_error
+    """sap::system_error (sap/exception.h:13-45); `reason` is the Reason code."""
+    Zero_pivoting = -1
+    Negative_DB_weight = -2
+    Illegal_update = -3
+    Illegal_solve = -4
+    Matrix_singular = -5
+
+    def __init__(self, reason: int, what: str):
+        super().__init__(what)
+        self.reason = reason
+
+
+class LibraryError(RuntimeError):
+    """A failure with no reference counterpart (CUDA error, bad argument...)."""
+
+    def __init__(self, code: int, what: str):
+        super().__init__(f"[{code}] {what}")
+        self.code = code
+
+
+class _COptions(ctypes.Structure):
+    _fields_ = [("solverType", ctypes.c_int), ("maxNumIterations", ctypes.c_int), ("relTol", ctypes.c_double),
+                ("absTol", ctypes.c_double), ("testDB", ctypes.c_int), ("isSPD", ctypes.c_int),
+                ("saveMem", ctypes.c_int), ("performReorder", ctypes.c_int), ("performDB", ctypes.c_int),
+                ("dbFirstStageOnly", ctypes.c_int), ("applyScaling", ctypes.c_int), ("maxBandwidth", ctypes.c_int),
+                ("gpuCount", ctypes.c_int), ("dropOffFraction", ctypes.c_double), ("factMethod", ctypes.c_int),
+                ("precondType", ctypes.c_int), ("safeFactorization", ctypes.c_int),
+                ("variableBandwidth", ctypes.c_int), ("trackReordering", ctypes.c_int), ("useBCR", ctypes.c_int),
+                ("ilu_level", ctypes.c_int)]
+
+
+_STAT_FIELDS = (["timeSetup", "timeUpdate", "timeSolve", "time_DB", "time_DB_pre", "time_DB_first",
+                 "time_DB_second", "time_DB_post", "d_p1", "d_p1_ori", "diag_dom", "diag_dom_ori",
+                 "time_reorder", "time_dropOff", "time_cpu_assemble", "time_transfer", "time_toBanded",
+                 "time_offDiags", "time_bandLU", "time_bandUL", "time_fullLU", "time_assembly", "time_shuffle"],
+                ["bandwidthReorder", "bandwidthDB", "bandwidth"], ["nuKf", "flops_LU"], ["numPartitions"],
+                ["actualDropOff"], ["numIterations"], ["rhsNorm", "residualNorm", "relResidualNorm"],
+                ["actual_nnz"])
+_STAT_TYPES = (ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_float,
+               ctypes.c_double, ctypes.c_int)
+
+
+class _CStats(ctypes.Structure):
+    _fields_ = [(name, t) for group, t in zip(_STAT_FIELDS, _STAT_TYPES) for name in group]
+
+
+_vp, _i, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+_pp = ctypes.POINTER(ctypes.c_void_p)
+_sig = {
+    "sap_last_error": (ctypes.c_char_p, []),
+    "sap_kernel_launch_count": (ctypes.c_int64, []),
+    "sap_options_default": (_i, [ctypes.POINTER(_COptions)]),
+    "sap_banded_create": (_i, [_i, _i, _vp, _i, _pp]),
+    "sap_banded_generate": (_i, [_i, _i, _d, _i, ctypes.c_uint64, _pp]),
+    "sap_generate_band_host": (_i, [_i, _i, _d, _i, ctypes.c_uint64, _vp]),
+    "sap_banded_copy_out": (_i, [_vp, _vp, _i]),
+    "sap_banded_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "sap_banded_destroy": (_i, [_vp]),
+    "sap_csr_create": (_i, [_i, _i, _vp, _vp, _vp, _i, _pp]),
+    "sap_csr_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "sap_csr_destroy": (_i, [_vp]),
+    "sap_spmv_banded_create": (_i, [_vp, _pp]),
+    "sap_spmv_csr_create": (_i, [_vp, _pp]),
+    "sap_spmv_callback_create": (_i, [_i, _vp, _vp, _pp]),
+    "sap_spmv_apply": (_i, [_vp, _vp, _vp]),
+    "sap_spmv_destroy": (_i, [_vp]),
+    "sap_solver_create": (_i, [_i, ctypes.POINTER(_COptions), _i, _pp]),
+    "sap_solver_destroy": (_i, [_vp]),
+    "sap_solver_setup_banded": (_i, [_vp, _vp]),
+    "sap_solver_setup_csr": (_i, [_vp, _vp]),
+    "sap_solver_update": (_i, [_vp, _vp, ctypes.c_int64, _i, ctypes.POINTER(_i)]),
+    "sap_solver_solve": (_i, [_vp, _vp, _vp, _vp, _i, ctypes.POINTER(_i)]),
+    "sap_precond_apply": (_i, [_vp, _vp, _vp]),
+    "sap_solver_get_stats": (_i, [_vp, ctypes.POINTER(_CStats)]),
+    "sap_solver_get_monitor": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_char_p)]),
+    "sap_solver_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "sap_solver_stream": (_vp, [_vp]),
+    "sap_profile_select": (_i, [ctypes.c_char_p]),
+    "sap_profile_read": (_i, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
+}
+for _name, (_res, _args) in _sig.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED_SYMBOLS = tuple(_sig)
+
+
+def _check(code: int) -> None:
+    if code == 0:
+        return
+    msg = (_lib.sap_last_error() or b"").decode()
+    if -5 <= code <= -1:
+        raise SystemError(code, msg)
+    raise LibraryError(code, msg)
+
+
+def _ptr(a):
+    """(pointer, memspace) of a numpy array or a torch CUDA tensor (float64/int32)."""
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return ctypes.c_void_p(a.ctypes.data), HOST
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr()), DEVICE
+    raise TypeError("expected a numpy array or a CUDA tensor")
+
+
+def kernel_launch_count() -> int:
+    """Number of kernels this library has enqueued since it was loaded."""
+    return int(_lib.sap_kernel_launch_count())
+
+
+def profile_select(kernel_name: str | None) -> None:
+    """Bracket every launch of `kernel_name` with CUDA events on its stream."""
+    _check(_lib.sap_profile_select((kernel_name or "").encode()))
+
+
+def profile_read() -> tuple[float, int]:
+    """(total milliseconds, launches) of the selected kernel since selection."""
+    ms, cnt = ctypes.c_double(), ctypes.c_int64()
+    _check(_lib.sap_profile_read(ctypes.byref(ms), ctypes.byref(cnt)))
+    return ms.value, cnt.value
+
+
+def generate_band_host(n: int, k: int, d: float, dist: int = 1, seed: int = 0) -> np.ndarray:
+    """Row-major band of BandedMatrix(n, k, d) generated on the host (no GPU)."""
+    out = np.zeros(n * (2 * k + 1), dtype=np.float64)
+    _check(_lib.sap_generate_band_host(n, k, float(d), dist, seed, ctypes.c_void_p(out.ctypes.data)))
+    return out
+
+
+# ---- Options / Stats ------------------------------------------------------------
+@dataclass
+class Options:
+    """sap::Options (sap/solver.h:52-81), defaults of sap/solver.h:233-256."""
+    solverType: int = BiCGStab2
+    maxNumIterations: int = 100
+    relTol: float = 1e-6
+    absTol: float = 0.0
+    testDB: bool = False
+    isSPD: bool = False
+    saveMem: bool = False
+    performReorder: bool = True
+    performDB: bool = True
+    dbFirstStageOnly: bool = False
+    applyScaling: bool = True
+    maxBandwidth: int = 2**31 - 1
+    gpuCount: int = 1
+    dropOffFraction: float = 0.0
+    factMethod: int = LU_only
+    precondType: int = Spike
+    safeFactorization: bool = False
+    variableBandwidth: bool = True
+    trackReordering: bool = False
+    useBCR: bool = False
+    ilu_level: int = -1
+
+    def _c(self) -> _COptions:
+        c = _COptions()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            setattr(c, f.name, float(v) if isinstance(v, float) else int(v))
+        return c
+
+
+class Stats:
+    """sap::Stats (sap/solver.h:89-140); times in milliseconds."""
+
+    def __init__(self, c: _CStats):
+        for name, _ in _CStats._fields_:
+            setattr(self, name, getattr(c, name))
+
+    def __repr__(self):
+        keys = ("timeSetup", "timeSolve", "numIterations", "relResidualNorm", "bandwidth", "numPartitions")
+        return "Stats(" + ", ".join(f"{k}={getattr(self, k)!r}" for k in keys) + ")"
+
+
+# ---- matrices -------------------------------------------------------------------
+class BandedMatrix:
+    """sap::BandedMatrix (sap/banded_matrix.h:25-95): a device-resident
+    row-major FP64 band.  `BandedMatrix(n, k, d)` generates it like the
+    reference (dist 0: rand() in [-10,10]); `BandedMatrix.from_array`
+    wraps caller data."""
+
+    def __init__(self, n: int, k: int, d: float, dist: int = 0, seed: int = 1, _handle=None):
+        self.m_n = self.num_rows = self.num_cols = int(n)
+        self.m_k = int(k)
+        self.m_d = float(d)
+        if _handle is None:
+            h = ctypes.c_void_p()
+            _check(_lib.sap_banded_generate(n, k, float(d), dist, seed, ctypes.byref(h)))
+            _handle = h
+        self._h = _handle
+        self.num_entries = n * (2 * k + 1) - k * (k + 1)
+
+    @classmethod
+    def from_array(cls, band, n: int, k: int) -> "BandedMatrix":
+        p, ms = _ptr(band)
+        h = ctypes.c_void_p()
+        _check(_lib.sap_banded_create(n, k, p, ms, ctypes.byref(h)))
+        return cls(n, k, 0.0, _handle=h)
+
+    def getBandedMatrix(self) -> np.ndarray:
+        out = np.empty(self.m_n * (2 * self.m_k + 1), dtype=np.float64)
+        _check(_lib.sap_banded_copy_out(self._h, ctypes.c_void_p(out.ctypes.data), HOST))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.sap_banded_destroy(h)
+            self._h = None
+
+
+class CsrMatrix:
+    """Device CSR matrix, int32 indices and FP64 values (the reference's
+    cusp::csr_matrix<int, double, device_memory>)."""
+
+    def __init__(self, row_offsets, column_indices, values):
+        rp = np.ascontiguousarray(row_offsets, dtype=np.int32)
+        ci = np.ascontiguousarray(column_indices, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.num_rows = self.num_cols = rp.size - 1
+        self.num_entries = ci.size
+        h = ctypes.c_void_p()
+        _check(_lib.sap_csr_create(self.num_rows, self.num_entries, ctypes.c_void_p(rp.ctypes.data),
+                                   ctypes.c_void_p(ci.ctypes.data), ctypes.c_void_p(v.ctypes.data), HOST,
+                                   ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.sap_csr_destroy(h)
+            self._h = None
+
+
+# ---- SpMV functors (sap/spmv.h) ---------------------------------------------------
+class _Spmv:
+    def __call__(self, v, Av):
+        pv, msv = _ptr(v)
+        pa, msa = _ptr(Av)
+        if msv != DEVICE or msa != DEVICE:
+            raise TypeError("SpMV operands must be CUDA tensors")
+        _check(_lib.sap_spmv_apply(self._h, pv, pa))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.sap_spmv_destroy(h)
+            self._h = None
+
+
+class MVBanded(_Spmv):
+    """MVBanded<Matrix> (sap/spmv.h:27-74)."""
+
+    def __init__(self, A: BandedMatrix):
+        self._A = A
+        h = ctypes.c_void_p()
+        _check(_lib.sap_spmv_banded_create(A._h, ctypes.byref(h)))
+        self._h = h
+
+
+class SpmvCusp(_Spmv):
+    """SpmvCusp<Matrix> (sap/spmv.h:83-129): FP64 CSR product."""
+
+    def __init__(self, A: CsrMatrix):
+        self._A = A
+        h = ctypes.c_void_p()
+        _check(_lib.sap_spmv_csr_create(A._h, ctypes.byref(h)))
+        self._h = h
+
+    def getTime(self) -> float:
+        return 0.0
+
+    def getCount(self) -> float:
+        return 0.0
+
+    def getGFlops(self) -> float:
+        return 0.0
+
+
+# ---- Solver ------------------------------------------------------------------------
+class Solver:
+    """sap::Solver<Array, PrecValueType> (sap/solver.h:153-225)."""
+
+    def __init__(self, numPartitions: int, opts: Options, prec: str = "float"):
+        self._opts = opts
+        h = ctypes.c_void_p()
+        copts = opts._c()
+        _check(_lib.sap_solver_create(int(numPartitions), ctypes.byref(copts), 0 if prec == "float" else 1,
+                                      ctypes.byref(h)))
+        self._h = h
+
+    def setup(self, A) -> bool:
+        """Solver::setup(A) (sap/solver.h:339-404)."""
+        self._A = A
+        if isinstance(A, BandedMatrix):
+            _check(_lib.sap_solver_setup_banded(self._h, A._h))
+        elif isinstance(A, CsrMatrix):
+            _check(_lib.sap_solver_setup_csr(self._h, A._h))
+        else:
+            raise TypeError("setup expects a BandedMatrix or a CsrMatrix")
+        return True
+
+    def update(self, entries) -> bool:
+        """Solver::update(entries) (sap/solver.h:421-462)."""
+        p, ms = _ptr(entries)
+        acc = ctypes.c_int(1)
+        n = entries.size if isinstance(entries, np.ndarray) else entries.numel()
+        _check(_lib.sap_solver_update(self._h, p, n, ms, ctypes.byref(acc)))
+        return bool(acc.value)
+
+    def solve(self, spmv: _Spmv, b, x) -> bool:
+        """Solver::solve(spmv, b, x) (sap/solver.h:477-562); x is the initial
+        guess on entry and the solution on exit (numpy or CUDA tensor)."""
+        pb, msb = _ptr(b)
+        px, msx = _ptr(x)
+        if msb != msx:
+            raise TypeError("b and x must live in the same memory space")
+        conv = ctypes.c_int(0)
+        _check(_lib.sap_solver_solve(self._h, spmv._h, pb, px, msb, ctypes.byref(conv)))
+        return bool(conv.value)
+
+    def precond(self, v, z) -> None:
+        """Precond::operator()(v, z) (sap/precond.h:1370-1386), CUDA tensors."""
+        pv, _ = _ptr(v)
+        pz, _ = _ptr(z)
+        _check(_lib.sap_precond_apply(self._h, pv, pz))
+
+    def getStats(self) -> Stats:
+        c = _CStats()
+        _check(_lib.sap_solver_get_stats(self._h, ctypes.byref(c)))
+        return Stats(c)
+
+    def getMonitorCode(self) -> int:
+        code = ctypes.c_int()
+        _check(_lib.sap_solver_get_monitor(self._h, ctypes.byref(code), None))
+        return code.value
+
+    def getMonitorMessage(self) -> str:
+        msg = ctypes.c_char_p()
+        _check(_lib.sap_solver_get_monitor(self._h, None, ctypes.byref(msg)))
+        return (msg.value or b"").decode()
+
+    def info(self):
+        n, k, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.sap_solver_info(self._h, ctypes.byref(n), ctypes.byref(k), ctypes.byref(p)))
+        return n.value, k.value, p.value
+
+    def stream(self) -> int:
+        return _lib.sap_solver_stream(self._h) or 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            _lib.sap_solver_destroy(h)
+            self._h = None
+
+
+__all__ = ["Options", "Stats", "Solver", "BandedMatrix", "CsrMatrix", "MVBanded", "SpmvCusp", "SystemError",
+           "LibraryError", "generate_band_host", "kernel_launch_count", "BiCGStab1", "BiCGStab2", "LU_UL",
+           "LU_only", "Spike", "Block", "NoPrecond", "EXPORTED_SYMBOLS"]

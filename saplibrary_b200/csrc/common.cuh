@@ -1,0 +1,120 @@
+// Shared utilities of the sap_b200 library: error plumbing, device buffers,
+// launch accounting and the asynchronous-copy PTX wrappers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sap_b200.h"
+
+namespace sapb {
+
+// Library failure carrying a C-ABI status code.  Reference failures use the
+// sap::system_error::Reason values (sap/exception.h:16-23).
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int code = (e == cudaErrorMemoryAllocation) ? SAP_ERR_OUT_OF_MEMORY : SAP_ERR_CUDA;
+    throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+#define SAPB_CUDA(x) ::sapb::cuda_check((x), #x)
+
+// Number of kernels enqueued by this library (reported by the bench).
+extern std::atomic<int64_t> g_launches;
+inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+#define SAPB_LAUNCHED() do { ::sapb::count_launch(); SAPB_CUDA(cudaGetLastError()); } while (0)
+
+// Event bracketing of the launches of one selected kernel (sap_profile_*).
+struct ProfScope {
+  bool on = false;
+  cudaStream_t s = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(const char* name, cudaStream_t st);
+  ~ProfScope();
+};
+#define SAPB_PROF(name, stream) ::sapb::ProfScope _sapb_prof_scope(name, stream)
+
+// Owning device buffer (stream-ordered allocation on the solver's stream).
+template <typename T>
+class DBuf {
+ public:
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept { swap(o); }
+  DBuf& operator=(DBuf&& o) noexcept { release(); swap(o); return *this; }
+  ~DBuf() { release(); }
+
+  void alloc(size_t n) {
+    if (n == n_ && p_) return;
+    release();
+    n_ = n;
+    if (n) SAPB_CUDA(cudaMalloc(&p_, n * sizeof(T)));
+  }
+  void zero(cudaStream_t s) {
+    if (n_) SAPB_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+  }
+  void upload(const T* h, size_t n, cudaStream_t s) {
+    alloc(n);
+    if (n) SAPB_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& h, cudaStream_t s) { upload(h.data(), h.size(), s); }
+  void download(std::vector<T>& h, cudaStream_t s) const {
+    h.resize(n_);
+    if (n_) SAPB_CUDA(cudaMemcpyAsync(h.data(), p_, n_ * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  void swap(DBuf& o) { std::swap(p_, o.p_); std::swap(n_, o.n_); }
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// --- asynchronous global->shared copies (sm_80+ cp.async) ---------------------
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_val(T* smem, const T* gmem) {
+  if constexpr (sizeof(T) == 8) cp_async8(smem, gmem);
+  else cp_async4(smem, gmem);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// boostValue (sap/device/factor_band_const.cuh:29-40): pivots with
+// |p| <= BURST_VALUE are replaced by +-BURST_NEW_VALUE.
+template <typename T>
+__device__ __forceinline__ T boost_pivot(T v) {
+  const T thr = (T)1e-7, nv = (T)1e-4;
+  if (v > thr || v < -thr) return v;
+  return v < (T)0 ? -nv : nv;
+}
+
+}  // namespace sapb

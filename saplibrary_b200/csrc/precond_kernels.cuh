@@ -1,0 +1,646 @@
+// Device kernels of the SPIKE preconditioner (setup and apply).
+//
+// Storage (kept from the reference because the factor, spike and sweep
+// index arithmetic depends on it): each partition's band is column-major
+// with 2K+1 entries per column, element (i,j) at (j-start)*(2K+1)+K+(i-j)
+// from the partition's base offset (sap/device/data_transfer.cuh:423-495).
+// For a constant-bandwidth matrix the partition bases coincide with the
+// global layout of the reference.
+#pragma once
+
+#include "common.cuh"
+
+namespace sapb {
+
+struct PartDev {
+  int start, size, K, ul;  // ul: partition holds UL factors (last one under LU_UL)
+  long long boff;          // offset of the partition's first band column
+};
+
+struct ChunkDev {
+  int part, a, b, pad;     // rows [a, b) of partition `part`
+};
+
+struct FactorJob {
+  int s, e, K, mirror;     // rows [s, e); mirror = UL factorisation
+  int target, pad;         // 0: factors into B, 1: into B2
+  long long boff;          // band offset of column s in the target buffer
+};
+
+enum { DIR_DOWN = 1, DIR_UP = -1 };
+
+// ---------------------------------------------------------------------------
+// Row-major FP64 band (sap/banded_matrix.h layout) -> column-major FP32 band
+// (bandedMatrixTranspose, sap/device/data_transfer.cuh:733-770).
+template <typename T>
+__global__ void k_band_from_rowmajor(const double* __restrict__ A, T* __restrict__ B, int n, int K) {
+  const long long SW = 2LL * K + 1;
+  const long long total = SW * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long c = e / SW;
+    int pos = (int)(e - c * SW);
+    long long r = c + pos - K;
+    T v = 0.f;
+    if (r >= 0 && r < n) v = (T)A[r * SW + (2 * K - pos)];
+    B[e] = v;
+  }
+}
+
+// COO/CSR scatter into the column-major band (copyFromCOOMatrixToBandedMatrix,
+// sap/device/data_transfer.cuh:423-448): one thread per row.
+template <typename T>
+__global__ void k_band_from_csr(const int* __restrict__ rp, const int* __restrict__ ci,
+                                const double* __restrict__ v, T* __restrict__ B, int n, int K) {
+  const long long SW = 2LL * K + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int p = rp[i]; p < rp[i + 1]; p++) {
+      int j = ci[p];
+      B[(long long)j * SW + K + (i - j)] = (T)v[p];
+    }
+  }
+}
+
+// Off-diagonal coupling blocks of each interface (copydWV*,
+// sap/device/data_transfer.cuh:129-199): B_i[c][r] = A(s-K+c, s+r) for
+// r <= c, C_{i+1}[c][r] = A(s+c, s-K+r) for c <= r, both row-major.
+template <typename T>
+__global__ void k_extract_offdiag(const PartDev* __restrict__ parts, const T* __restrict__ B,
+                                  T* __restrict__ offd, int K) {
+  const int i = blockIdx.y;
+  const int s = parts[i + 1].start;
+  const long long SW = 2LL * K + 1;
+  const long long KK = (long long)K * K;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K * K; e += gridDim.x * blockDim.x) {
+    int c = e / K, r = e % K;
+    T bv = 0.f, cv = 0.f;
+    if (r <= c) { long long row = s - K + c, col = s + r; bv = B[col * SW + K + (row - col)]; }
+    if (c <= r) { long long row = s + c, col = s - K + r; cv = B[col * SW + K + (row - col)]; }
+    offd[(2 * i) * KK + e] = bv;
+    offd[(2 * i + 1) * KK + e] = cv;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Banded LU (or, mirrored, UL) of one partition per CTA, without pivoting,
+// with the reference's boosting rule and the row post-divide of the factor
+// holding the pivots fused into the write-back
+// (bandLU_g32 / blockedBandLU_critical_const_*, bandUL_g32 /
+// blockedBandUL_critical_const_*, bandLUUL_post_divide:
+// sap/device/factor_band_const.cuh:229-400, 1423-1779).
+//
+// The active window (columns j..j+K of the pivot j, full 2K+1 band
+// positions) lives in shared memory as a ring of W = K+1+D column slots;
+// column j+K+D is fetched with cp.async D pivots before it is needed and
+// column j-1 is written back (post-divided) while pivot j runs.  Mirrored
+// jobs (UL) see the partition with reversed rows and columns, which turns
+// the UL elimination into an LU elimination of the mirrored band.
+template <typename T, int D>
+__global__ void __launch_bounds__(1024)
+k_factor_smem(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restrict__ B2,
+              int do_boost, int* __restrict__ zero_flag, int G) {
+  const FactorJob jb = jobs[blockIdx.x];
+  const int K = jb.K, SW = 2 * K + 1, np = jb.e - jb.s, W = K + 1 + D;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* sm = reinterpret_cast<T*>(sm_raw);
+  T* win = sm;
+  T* piv = sm + (size_t)W * SW;
+  T* band = (jb.target ? B2 : B) + jb.boff;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const bool mir = jb.mirror != 0;
+  auto gidx = [&](int i, int p) -> long long {
+    int col = mir ? (np - 1 - i) : i;
+    int pos = mir ? (2 * K - p) : p;
+    return (long long)col * SW + pos;
+  };
+  for (int i = 0; i < K + D; i++) {
+    if (i < np)
+      for (int p = tid; p < SW; p += NT) cp_async_val<T>(&win[(i % W) * SW + p], band + gidx(i, p));
+    cp_async_commit();
+  }
+  const int rB = tid % K + 1, gB = tid / K;
+  for (int j = 0; j < np; j++) {
+    cp_async_wait<D - 1>();
+    __syncthreads();
+    {
+      const int nc = j + K + D;
+      const int sl = nc % W;  // == (j-1) % W for j >= 1
+      for (int p = tid; p < SW; p += NT) {
+        if (j >= 1) {
+          T v = win[sl * SW + p];
+          if (p < K) {
+            int i = j - 1 - K + p;
+            if (i >= 0) v /= piv[i % W];
+          }
+          band[gidx(j - 1, p)] = v;
+        }
+        if (nc < np) cp_async_val<T>(&win[sl * SW + p], band + gidx(nc, p));
+      }
+      cp_async_commit();
+    }
+    const int w = min(K, np - 1 - j);
+    const int sj = j % W;
+    T p = win[sj * SW + K];
+    if (do_boost) p = boost_pivot(p);
+    else if (tid == 0 && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
+    for (int r = tid + 1; r <= w; r += NT) win[sj * SW + K + r] /= p;
+    if (tid == 0) piv[sj] = p;
+    __syncthreads();
+    if (tid == 0) win[sj * SW + K] = p;
+    if (gB < G && rB <= w) {
+      const T l = win[sj * SW + K + rB];
+      int sc = (j + gB + 1) % W;
+      for (int c = gB + 1; c <= w; c += G) {
+        win[sc * SW + K + rB - c] -= l * win[sc * SW + K - c];
+        sc += G;
+        if (sc >= W) sc -= W;
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  {
+    const int j = np;
+    const int sl = (j - 1) % W;
+    for (int p = tid; p < SW; p += NT) {
+      T v = win[sl * SW + p];
+      if (p < K) {
+        int i = j - 1 - K + p;
+        if (i >= 0) v /= piv[i % W];
+      }
+      band[gidx(j - 1, p)] = v;
+    }
+  }
+}
+
+// Same factorisation operating directly on the band in global memory, for
+// half-bandwidths whose window does not fit in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_factor_global(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restrict__ B2,
+                int do_boost, int* __restrict__ zero_flag, int G) {
+  const FactorJob jb = jobs[blockIdx.x];
+  const int K = jb.K, SW = 2 * K + 1, np = jb.e - jb.s;
+  T* band = (jb.target ? B2 : B) + jb.boff;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const bool mir = jb.mirror != 0;
+  auto A = [&](int i, int p) -> T& {
+    int col = mir ? (np - 1 - i) : i;
+    int pos = mir ? (2 * K - p) : p;
+    return band[(long long)col * SW + pos];
+  };
+  __shared__ T spiv;
+  const int rB = tid % K + 1, gB = tid / K;
+  for (int j = 0; j < np; j++) {
+    __syncthreads();
+    if (j >= 1) {  // post-divide the U part of column j-1 (final)
+      for (int p = tid; p < K; p += NT) {
+        int i = j - 1 - K + p;
+        if (i >= 0) A(j - 1, p) /= A(i, K);
+      }
+    }
+    const int w = min(K, np - 1 - j);
+    T pv = A(j, K);
+    if (do_boost) pv = boost_pivot(pv);
+    else if (tid == 0 && fabs((double)pv) < 1e-7) atomicOr(zero_flag, 1);
+    for (int r = tid + 1; r <= w; r += NT) A(j, K + r) /= pv;
+    if (tid == 0) spiv = pv;
+    __syncthreads();
+    if (tid == 0) A(j, K) = spiv;
+    if (gB < G && rB <= w) {
+      const T l = A(j, K + rB);
+      for (int c = gB + 1; c <= w; c += G) A(j + c, K + rB - c) -= l * A(j + c, K - c);
+    }
+  }
+  __syncthreads();
+  for (int p = tid; p < K; p += NT) {
+    int i = np - 1 - K + p;
+    if (i >= 0) A(np - 1, p) /= A(i, K);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spike tips of the LU_UL method, one CTA per (interface, tip), one thread
+// per right-hand-side column (calculateSpikes(B2, WV) and the
+// forwardElimLdWV / backwardElimUdWV kernels, sap/precond.h:6232-6287,
+// sap/device/sweep_band_const.cuh:585-706), on post-divided factors:
+//   V_i = Ut_bb^-1 D_bb^-1 L_bb^-1 B_i   (LU corner of partition i)
+//   W_i = Lt_tt^-1 D_tt^-1 U'_tt^-1 C_{i+1}  (UL corner of partition i+1)
+template <typename T>
+__global__ void k_spikes_luul(const PartDev* __restrict__ parts, int P, const T* __restrict__ B,
+                              const T* __restrict__ B2, const T* __restrict__ offd,
+                              T* __restrict__ V, T* __restrict__ Wm, int K) {
+  const int i = blockIdx.x, which = blockIdx.y, col = threadIdx.x;
+  if (col >= K) return;
+  const long long SW = 2LL * K + 1, KK = (long long)K * K;
+  const int s = parts[i + 1].start;
+  auto val = [&](const T* band, long long r, long long c) { return band[c * SW + K + (r - c)]; };
+  if (which == 0) {
+    T* X = V + i * KK;
+    const T* Bm = offd + (2 * i) * KK;
+    const long long base = s - K;
+    for (int r = 0; r < K; r++) X[r * K + col] = Bm[r * K + col];
+    for (int j = 0; j < K - 1; j++) {
+      T xj = X[j * K + col];
+      for (int t = 1; t < K - j; t++) X[(j + t) * K + col] -= val(B, base + j + t, base + j) * xj;
+    }
+    for (int j = 0; j < K; j++) X[j * K + col] /= val(B, base + j, base + j);
+    for (int j = K - 1; j >= 1; j--) {
+      T xj = X[j * K + col];
+      for (int t = 1; t <= j; t++) X[(j - t) * K + col] -= val(B, base + j - t, base + j) * xj;
+    }
+  } else {
+    T* X = Wm + i * KK;
+    const T* Cm = offd + (2 * i + 1) * KK;
+    const T* src = (i + 1 == P - 1) ? B : B2;
+    const long long base = s;
+    for (int r = 0; r < K; r++) X[r * K + col] = Cm[r * K + col];
+    for (int j = K - 1; j >= 1; j--) {
+      T xj = X[j * K + col];
+      for (int t = 1; t <= j; t++) X[(j - t) * K + col] -= val(src, base + j - t, base + j) * xj;
+    }
+    for (int j = 0; j < K; j++) X[j * K + col] /= val(src, base + j, base + j);
+    for (int j = 0; j < K - 1; j++) {
+      T xj = X[j * K + col];
+      for (int t = 1; t < K - j; t++) X[(j + t) * K + col] -= val(src, base + j + t, base + j) * xj;
+    }
+  }
+}
+
+// Spike tips of the constant-band LU_only method: V as above; W from full
+// sweeps of partition i+1 with K right-hand sides (calculateSpikes_const,
+// sap/precond.h:5785-5949), one thread per column, the column kept in a
+// global scratch vector of the partition's length.
+template <typename T>
+__global__ void k_spikes_luonly(const PartDev* __restrict__ parts, const T* __restrict__ B,
+                                const T* __restrict__ offd, T* __restrict__ V,
+                                T* __restrict__ Wm, T* __restrict__ scratch,
+                                long long scratch_stride, int K) {
+  const int i = blockIdx.x, which = blockIdx.y, col = threadIdx.x;
+  if (col >= K) return;
+  const long long SW = 2LL * K + 1, KK = (long long)K * K;
+  const int s = parts[i + 1].start;
+  auto val = [&](long long r, long long c) { return B[c * SW + K + (r - c)]; };
+  if (which == 0) {
+    T* X = V + i * KK;
+    const T* Bm = offd + (2 * i) * KK;
+    const long long base = s - K;
+    for (int r = 0; r < K; r++) X[r * K + col] = Bm[r * K + col];
+    for (int j = 0; j < K - 1; j++) {
+      T xj = X[j * K + col];
+      for (int t = 1; t < K - j; t++) X[(j + t) * K + col] -= val(base + j + t, base + j) * xj;
+    }
+    for (int j = 0; j < K; j++) X[j * K + col] /= val(base + j, base + j);
+    for (int j = K - 1; j >= 1; j--) {
+      T xj = X[j * K + col];
+      for (int t = 1; t <= j; t++) X[(j - t) * K + col] -= val(base + j - t, base + j) * xj;
+    }
+  } else {
+    const int np = parts[i + 1].size;
+    T* y = scratch + ((long long)i * K + col) * scratch_stride;
+    const T* Cm = offd + (2 * i + 1) * KK;
+    for (int r = 0; r < np; r++) y[r] = (r < K) ? Cm[r * K + col] : 0.f;
+    for (int j = 0; j < np - 1; j++) {
+      T yj = y[j];
+      if (yj == 0.f) continue;
+      int w = min(K, np - 1 - j);
+      for (int t = 1; t <= w; t++) y[j + t] -= val(s + j + t, s + j) * yj;
+    }
+    for (int j = 0; j < np; j++) y[j] /= val(s + j, s + j);
+    for (int j = np - 1; j >= 1; j--) {
+      T yj = y[j];
+      int w = min(K, j);
+      for (int t = 1; t <= w; t++) y[j - t] -= val(s + j - t, s + j) * yj;
+    }
+    T* X = Wm + i * KK;
+    for (int r = 0; r < K; r++) X[r * K + col] = y[r];
+  }
+}
+
+// Reduced system of each interface: R_i = [[I, V_i], [W_i, I]] has unit
+// leading pivots, so its LU reduces to the LU of S_i = I - W_i V_i
+// (fullLU_sub_spec + blockedFullLU_phase1..3 + fullLU_post_divide,
+// sap/device/factor_band_var.cuh:736-800, 964-1107).  S is row-major, its
+// unit-lower L and the post-divided U share the storage, D on the diagonal.
+template <typename T>
+__global__ void __launch_bounds__(512)
+k_reduced_factor(const T* __restrict__ V, const T* __restrict__ Wm, T* __restrict__ S,
+                 int K, int do_boost) {
+  const int i = blockIdx.x, tid = threadIdx.x, NT = blockDim.x;
+  const long long KK = (long long)K * K;
+  const T* Vi = V + i * KK;
+  const T* Wi = Wm + i * KK;
+  T* Si = S + i * KK;
+  for (int e = tid; e < K * K; e += NT) {
+    int r = e / K, c = e % K;
+    T acc = (r == c) ? 1.f : 0.f;
+    for (int k = 0; k < K; k++) acc -= Wi[r * K + k] * Vi[k * K + c];
+    Si[e] = acc;
+  }
+  __shared__ T sp;
+  for (int j = 0; j < K; j++) {
+    __syncthreads();
+    T p = Si[j * K + j];
+    if (do_boost) p = boost_pivot(p);
+    for (int r = j + 1 + tid; r < K; r += NT) Si[r * K + j] /= p;
+    if (tid == 0) sp = p;
+    __syncthreads();
+    if (tid == 0) Si[j * K + j] = sp;
+    const int w = K - 1 - j;
+    for (int e = tid; e < w * w; e += NT) {
+      int r = j + 1 + e / w, c = j + 1 + e % w;
+      Si[r * K + c] -= Si[r * K + j] * Si[j * K + c];
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < K * K; e += NT) {
+    int r = e / K, c = e % K;
+    if (c > r) Si[e] /= Si[r * K + r];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Chunked partition sweeps.
+//
+// Every triangular solve of a partition (L or U, unit diagonal) is cut into
+// chunks of >= K rows processed in parallel.  The solve of a chunk is an
+// affine function of the K "carry" values entering it from the previous
+// chunk (in the direction of the solve): tail = T_c * carry + tail0.  A
+// setup kernel computes T_c; per apply, pass 1 solves each chunk with a
+// zero carry (tail0), a per-partition scan chains the carries, and pass 2/3
+// re-solve the chunks with their exact carries.  The result equals the
+// serial partition sweep of the reference up to rounding.
+//
+// Processing-order indexing inside a chunk: xs[0..K) holds the carry rows,
+// xs[K..K+m) the chunk rows in the order the solve visits them; the row of
+// index u is o + dir*(u-K), with o = a (down) or b-1 (up).  The coefficient
+// that propagates row(u) to row(u+t) sits in band column row(u) at position
+// K + dir*t.
+template <typename T, int PF>
+__device__ __forceinline__ void chunk_solve(T* xs, int m, int K, int dir, int o, const T* col0,
+                                            int start, int SW, bool carry) {
+  const int tid = threadIdx.x, t = tid + 1;
+  const int u0 = carry ? 0 : K;
+  const int uend = K + m - 1;  // last source index with a target
+  T cur[PF], nxt[PF];
+  auto ld = [&](int u) -> T {
+    int v = u + t;
+    if (u < uend && t <= K && v < K + m && v >= K) {
+      int row = o + dir * (u - K);
+      return __ldg(col0 + (long long)(row - start) * SW + K + dir * t);
+    }
+    return 0.f;
+  };
+#pragma unroll
+  for (int q = 0; q < PF; q++) cur[q] = ld(u0 + q);
+  for (int ub = u0; ub < uend; ub += PF) {
+#pragma unroll
+    for (int q = 0; q < PF; q++) nxt[q] = ld(ub + PF + q);
+#pragma unroll
+    for (int q = 0; q < PF; q++) {
+      const int u = ub + q;
+      __syncthreads();
+      if (u < uend) {
+        const T xu = xs[u];
+        const int v = u + t;
+        if (t <= K && v < K + m && v >= K) xs[v] -= cur[q] * xu;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < PF; q++) cur[q] = nxt[q];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int dir1_of(const PartDev& p) { return p.ul ? DIR_UP : DIR_DOWN; }
+
+// pass 1: first solve of the partition (L for LU partitions, U' for the UL
+// partition) with a zero carry; records the chunk's tail.  With vin given,
+// the right-hand side is converted from FP64 and stored to F.
+template <typename T, int PF>
+__global__ void k_pass1(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
+                        const long long* __restrict__ koff, const T* __restrict__ B,
+                        const double* __restrict__ vin, T* __restrict__ F, T* __restrict__ tails) {
+  extern __shared__ __align__(16) unsigned char xs_raw[];
+  T* xs = reinterpret_cast<T*>(xs_raw);
+  const ChunkDev ch = chunks[blockIdx.x];
+  const PartDev p = parts[ch.part];
+  const int K = p.K, m = ch.b - ch.a, dir = dir1_of(p), o = dir > 0 ? ch.a : ch.b - 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int row = o + dir * i;
+    T v;
+    if (vin) { v = (T)vin[row]; F[row] = v; }
+    else v = F[row];
+    xs[K + i] = v;
+  }
+  chunk_solve<T, PF>(xs, m, K, dir, o, B + p.boff, p.start, 2 * K + 1, false);
+  for (int i = threadIdx.x; i < K; i += blockDim.x) tails[koff[blockIdx.x] + i] = xs[m + i];
+}
+
+// pass 2: first solve with the exact carry, divide by the pivots, store Y,
+// then the second solve (opposite direction) of the chunk with a zero carry,
+// recording its tail.
+template <typename T, int PF>
+__global__ void k_pass2(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
+                        const int* __restrict__ first1, const long long* __restrict__ koff,
+                        const T* __restrict__ B, const T* __restrict__ F,
+                        const T* __restrict__ carry1, T* __restrict__ Y, T* __restrict__ tails2) {
+  extern __shared__ __align__(16) unsigned char xs_raw[];
+  T* xs = reinterpret_cast<T*>(xs_raw);
+  const int c = blockIdx.x;
+  const ChunkDev ch = chunks[c];
+  const PartDev p = parts[ch.part];
+  const int K = p.K, SW = 2 * K + 1, m = ch.b - ch.a, dir = dir1_of(p), o = dir > 0 ? ch.a : ch.b - 1;
+  const bool has_carry = !first1[c];
+  const T* col0 = B + p.boff;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) xs[K + i] = F[o + dir * i];
+  if (has_carry)
+    for (int i = threadIdx.x; i < K; i += blockDim.x) xs[i] = carry1[koff[c] + i];
+  chunk_solve<T, PF>(xs, m, K, dir, o, col0, p.start, SW, has_carry);
+  // divide by the pivots and reverse into the second solve's order
+  T* ys = xs + K + m;  // second half of the shared buffer
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int row = o + dir * i;
+    T v = xs[K + i] / col0[(long long)(row - p.start) * SW + K];
+    Y[row] = v;
+    ys[K + (m - 1 - i)] = v;
+  }
+  __syncthreads();
+  const int dir2 = -dir, o2 = dir2 > 0 ? ch.a : ch.b - 1;
+  chunk_solve<T, PF>(ys, m, K, dir2, o2, col0, p.start, SW, false);
+  for (int i = threadIdx.x; i < K; i += blockDim.x) tails2[koff[c] + i] = ys[m + i];
+}
+
+// pass 3: second solve with the exact carry; writes FP64 (zout) or FP32
+// (gout) results in natural row order.
+template <typename T, int PF>
+__global__ void k_pass3(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
+                        const int* __restrict__ first2, const long long* __restrict__ koff,
+                        const T* __restrict__ B, const T* __restrict__ Y,
+                        const T* __restrict__ carry2, double* __restrict__ zout, T* __restrict__ gout) {
+  extern __shared__ __align__(16) unsigned char xs_raw[];
+  T* xs = reinterpret_cast<T*>(xs_raw);
+  const int c = blockIdx.x;
+  const ChunkDev ch = chunks[c];
+  const PartDev p = parts[ch.part];
+  const int K = p.K, SW = 2 * K + 1, m = ch.b - ch.a;
+  const int dir2 = -dir1_of(p), o2 = dir2 > 0 ? ch.a : ch.b - 1;
+  const bool has_carry = !first2[c];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) xs[K + i] = Y[o2 + dir2 * i];
+  if (has_carry)
+    for (int i = threadIdx.x; i < K; i += blockDim.x) xs[i] = carry2[koff[c] + i];
+  chunk_solve<T, PF>(xs, m, K, dir2, o2, B + p.boff, p.start, SW, has_carry);
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    int row = o2 + dir2 * i;
+    if (zout) zout[row] = (double)xs[K + i];
+    else gout[row] = xs[K + i];
+  }
+}
+
+// Carry scan of one partition per CTA: carry_{next} = T_c carry_c + tail_c
+// along the chunks in the direction of the solve (which = 1: first solve,
+// 2: second solve).  T_c is stored column-major (T[k*K + u]).
+template <typename T>
+__global__ void __launch_bounds__(512)
+k_scan(const PartDev* __restrict__ parts, const int* __restrict__ pchunk0, const int* __restrict__ pnchunk,
+       const long long* __restrict__ koff, const long long* __restrict__ toff, const T* __restrict__ Tm,
+       const T* __restrict__ tails, T* __restrict__ carry, int which, int G) {
+  const PartDev p = parts[blockIdx.x];
+  const int K = p.K, c0 = pchunk0[blockIdx.x], nc = pnchunk[blockIdx.x];
+  if (nc <= 1) return;
+  const int dir = (which == 1) ? dir1_of(p) : -dir1_of(p);
+  extern __shared__ __align__(16) unsigned char sh_raw[];
+  T* sh = reinterpret_cast<T*>(sh_raw);
+  T* sig = sh;        // K
+  T* red = sh + K;    // G*K
+  const int tid = threadIdx.x, u = tid % K, g = tid / K;
+  const bool act = g < G;
+  for (int step = 0; step < nc - 1; step++) {
+    const int c = dir > 0 ? c0 + step : c0 + nc - 1 - step;
+    const int cn = dir > 0 ? c + 1 : c - 1;
+    T part = 0.f;
+    if (act && step > 0) {
+      const T* Tc = Tm + toff[c];
+      for (int k = g; k < K; k += G) part += Tc[(long long)k * K + u] * sig[k];
+    }
+    if (act) red[g * K + u] = part;
+    __syncthreads();
+    if (tid < K) {
+      T acc = tails[koff[c] + tid];
+      for (int q = 0; q < G; q++) acc += red[q * K + tid];
+      carry[koff[cn] + tid] = acc;
+      sig[tid] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Transfer matrices of every chunk for one of the two solves (setup):
+// thread k follows a unit carry e_k through the chunk with a zero
+// right-hand side and records the chunk's tail, T[k*K + u] = d tail_u / d
+// carry_k.  The last K values live in a shared ring of K slots per thread.
+template <typename T>
+__global__ void k_transfer(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
+                           const long long* __restrict__ toff, const T* __restrict__ B,
+                           T* __restrict__ Tm, int which, T* __restrict__ gring,
+                           const int* __restrict__ first) {
+  extern __shared__ __align__(16) unsigned char ring_raw[];
+  // a chunk that starts its partition in this direction has no carry: its
+  // transfer matrix is never read, and its carry rows lie outside the partition
+  if (first[blockIdx.x]) return;
+  const ChunkDev ch = chunks[blockIdx.x];
+  const PartDev p = parts[ch.part];
+  const int K = p.K, SW = 2 * K + 1, m = ch.b - ch.a;
+  const int NT = blockDim.x;
+  // the ring lives in shared memory, or in a per-block global slice when
+  // K x blockDim values do not fit
+  T* ring = gring ? gring + (long long)blockIdx.x * K * NT : reinterpret_cast<T*>(ring_raw);
+  const int dir = (which == 1) ? dir1_of(p) : -dir1_of(p);
+  const int o = dir > 0 ? ch.a : ch.b - 1;
+  const int k = threadIdx.x;
+  if (k < K) {
+    for (int u = 0; u < K; u++) ring[u * NT + k] = (u == k) ? T(1) : T(0);
+    const T* col0 = B + p.boff;
+    for (int v = K; v < K + m; v++) {
+      T acc = T(0);
+      int slot = (v - 1) % K;
+      int row = o + dir * (v - 1 - K);
+      for (int t = 1; t <= K; t++) {
+        acc -= __ldg(col0 + (long long)(row - p.start) * SW + K + dir * t) * ring[slot * NT + k];
+        slot = (slot == 0) ? K - 1 : slot - 1;
+        row -= dir;
+      }
+      ring[(v % K) * NT + k] = acc;
+    }
+    T* Tc = Tm + toff[blockIdx.x];
+    for (int u = 0; u < K; u++) Tc[(long long)k * K + u] = ring[((m + u) % K) * NT + k];
+  }
+}
+
+// Reduced solve of each interface followed by the purification of the
+// interface right-hand sides (partFullFwdSweep/BckSweep + purifyRHS,
+// sap/precond.h:5418-5530).  G holds D^-1 f from the first sweep pair;
+// F is the FP32 right-hand side the second sweep pair will read.
+template <typename T>
+__global__ void __launch_bounds__(1024)
+k_reduced_apply(const PartDev* __restrict__ parts, const T* __restrict__ V, const T* __restrict__ Wm,
+                const T* __restrict__ S, const T* __restrict__ offd, const T* __restrict__ Gv,
+                T* __restrict__ F, int K) {
+  extern __shared__ __align__(16) unsigned char sh_raw[];
+  T* sh = reinterpret_cast<T*>(sh_raw);
+  T* xb = sh;
+  T* z = sh + K;
+  T* x1 = sh + 2 * K;
+  const int i = blockIdx.x, r = threadIdx.x;
+  const long long KK = (long long)K * K;
+  const int s = parts[i + 1].start;
+  const T* Vi = V + i * KK;
+  const T* Wi = Wm + i * KK;
+  const T* Si = S + i * KK;
+  const T* Bm = offd + (2 * i) * KK;
+  const T* Cm = offd + (2 * i + 1) * KK;
+  if (r < K) xb[r] = Gv[s - K + r];
+  __syncthreads();
+  if (r < K) {
+    T acc = Gv[s + r];
+    for (int c = 0; c < K; c++) acc -= Wi[r * K + c] * xb[c];
+    z[r] = acc;
+  }
+  for (int j = 0; j < K - 1; j++) {
+    __syncthreads();
+    T zj = z[j];
+    if (r > j && r < K) z[r] -= Si[r * K + j] * zj;
+  }
+  __syncthreads();
+  if (r < K) z[r] /= Si[r * K + r];
+  for (int j = K - 1; j >= 1; j--) {
+    __syncthreads();
+    T zj = z[j];
+    if (r < j) z[r] -= Si[r * K + j] * zj;
+  }
+  __syncthreads();
+  if (r < K) {
+    T acc = xb[r];
+    for (int c = 0; c < K; c++) acc -= Vi[r * K + c] * z[c];
+    x1[r] = acc;
+  }
+  __syncthreads();
+  if (r < K) {
+    T t1 = 0.f, t2 = 0.f;
+    for (int c = 0; c < K; c++) {
+      t1 += Bm[r * K + c] * z[c];
+      t2 += Cm[r * K + c] * x1[c];
+    }
+    F[s - K + r] -= t1;
+    F[s + r] -= t2;
+  }
+}
+
+// K == 0: the band is the diagonal (getSRev, sap/precond.h:1416-1419).
+template <typename T>
+__global__ void k_diag_apply(const T* __restrict__ B, const double* __restrict__ v, double* __restrict__ z, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    z[i] = (double)((T)v[i] / B[i]);
+}
+
+}  // namespace sapb

@@ -1,0 +1,1079 @@
+// Host orchestration of the B200 SPIKE solver and its C ABI (include/sap_b200.h).
+//
+// One solver = one CUDA stream.  Setup builds the partitioned band on the
+// device, factors it, computes the spike tips, the reduced system and the
+// chunk transfer matrices of the parallel sweeps; solve runs the
+// reference's BiCGStab(L) (sap/bicgstab2.h:32-360) with its monitor
+// (sap/monitor.h:154-339) over FP64 device vectors.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "krylov_kernels.cuh"
+#include "precond_kernels.cuh"
+#include "reorder.h"
+
+namespace sapb {
+
+std::atomic<int64_t> g_launches{0};
+static thread_local std::string g_last_error;
+
+// --- live kernel profiling -----------------------------------------------------
+struct ProfState {
+  std::mutex mu;
+  std::string name;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pairs;
+};
+static ProfState g_prof;
+
+ProfScope::ProfScope(const char* name, cudaStream_t st) {
+  std::lock_guard<std::mutex> lk(g_prof.mu);
+  if (g_prof.name.empty() || g_prof.name != name) return;
+  on = true;
+  s = st;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, s);
+}
+ProfScope::~ProfScope() {
+  if (!on) return;
+  cudaEventRecord(b, s);
+  std::lock_guard<std::mutex> lk(g_prof.mu);
+  g_prof.pairs.emplace_back(a, b);
+}
+
+static int grid_for(long long n, int threads, int cap = 148 * 16) {
+  long long g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+using Clock = std::chrono::steady_clock;
+static double ms_since(Clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+// ---------------------------------------------------------------------------
+struct Banded {
+  int n = 0, K = 0;
+  DBuf<double> A;  // row-major band on the device
+};
+
+struct Csr {
+  int n = 0, nnz = 0;
+  DBuf<int> rp, ci;
+  DBuf<double> v;
+  std::vector<int> rp_h, ci_h;  // host copies of the pattern (reordering runs on the host)
+  std::vector<double> v_h;
+};
+
+struct Spmv {
+  int kind = 0;  // 0 banded, 1 csr, 2 callback
+  const Banded* band = nullptr;
+  const Csr* csr = nullptr;
+  sap_spmv_fn fn = nullptr;
+  void* ctx = nullptr;
+  int n = 0;
+  void apply(const double* x, double* y, cudaStream_t s) const {
+    if (kind == 0) {
+      SAPB_PROF("spmv_banded", s);
+      k_spmv_banded<<<grid_for((long long)band->n * 32, 256, 148 * 32), 256, 0, s>>>(band->A.get(), x, y, band->n, band->K);
+      SAPB_LAUNCHED();
+    } else if (kind == 1) {
+      SAPB_PROF("spmv_csr", s);
+      double avg = csr->n ? (double)csr->nnz / csr->n : 0;
+      if (avg <= 12) {
+        k_spmv_csr<4><<<grid_for((long long)csr->n * 4, 256, 148 * 64), 256, 0, s>>>(csr->rp.get(), csr->ci.get(), csr->v.get(), x, y, csr->n);
+      } else {
+        k_spmv_csr<32><<<grid_for((long long)csr->n * 32, 256, 148 * 64), 256, 0, s>>>(csr->rp.get(), csr->ci.get(), csr->v.get(), x, y, csr->n);
+      }
+      SAPB_LAUNCHED();
+    } else {
+      fn(ctx, x, y, (void*)s);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Preconditioner (sap::Precond, sap/precond.h).  PrecBase holds what does not
+// depend on the value type; PrecondT<T> is the Precond<PrecVector> of a
+// float or double PrecValueType (sap/solver.h:153).
+class PrecBase {
+ public:
+  sap_options o{};
+  int P_req = 1;
+  cudaStream_t st = nullptr;
+
+  int n = 0, K = 0, P = 1;
+  bool spike = false, lu_ul = false;
+  int ptype = SAP_PRECOND_SPIKE;
+  std::vector<PartDev> parts_h;
+  DBuf<PartDev> parts_d;
+
+  // reordering (sparse path): row/column permutations and scalings
+  bool reordered = false;
+  Reorder ro;
+  DBuf<int> perm_in_d, perm_out_d;
+  DBuf<double> scale_in_d, scale_out_d;
+  DBuf<double> vtmp, ztmp;
+
+  // statistics
+  double t_toBanded = 0, t_offDiags = 0, t_bandLU = 0, t_assembly = 0, t_fullLU = 0, t_transfer = 0;
+  double t_reorder = 0, t_dropOff = 0, t_cpu_assemble = 0;
+  int k_reorder = 0, k_db = 0;
+  double drop_actual = 0;
+
+  virtual ~PrecBase() {}
+  // Band setups: the row-major FP64 band of a BandedMatrix, or a CSR matrix
+  // used without reordering.
+  virtual void setup_rowmajor(const double* A_dev, int n_, int K_) = 0;
+  virtual void setup_csr_direct(const Csr& A, int K_) = 0;
+  virtual void apply_band(const double* v, double* z) = 0;
+  void apply(const double* v, double* z);
+
+  void clamp_partitions_banded() {
+    // convertToBandedMatrix (sap/precond.h:2116-2117, 2258-2259)
+    int maxP = std::max(1, n / std::max(K + 1, 2 * K));
+    P = std::min(P_req, maxP);
+  }
+  void init_parts_const() {
+    parts_h.resize(P);
+    int q = n / P, r = n % P;
+    for (int p = 0; p < P; p++) {
+      PartDev d{};
+      d.start = p * q + std::min(p, r);
+      d.size = q + (p < r ? 1 : 0);
+      d.K = K;
+      d.ul = (lu_ul && p == P - 1) ? 1 : 0;
+      d.boff = (long long)d.start * (2 * K + 1);
+      parts_h[p] = d;
+    }
+    parts_d.upload(parts_h, st);
+  }
+  int parts_maxK() const {
+    int m = 0;
+    for (auto& p : parts_h) m = std::max(m, p.K);
+    return m;
+  }
+};
+
+template <typename T>
+class PrecondT : public PrecBase {
+ public:
+  DBuf<T> B, B2, offd, V, W, S, scratch;
+  // chunked sweeps
+  std::vector<ChunkDev> chunks_h;
+  DBuf<ChunkDev> chunks_d;
+  DBuf<long long> koff_d, toff_d;
+  DBuf<int> first1_d, first2_d, pchunk0_d, pnchunk_d;
+  DBuf<T> T1, T2, tails1, tails2, carry1, carry2;
+  DBuf<T> F, Gv, Y;
+  DBuf<int> flag;
+  int maxChunk = 0, sweepThreads = 32, scanG = 1;
+
+  void setup_rowmajor(const double* A_dev, int n_, int K_) override {
+    n = n_;
+    K = K_;
+    clamp_partitions_banded();
+    B.alloc((size_t)(2 * K + 1) * n);
+    auto t1 = Clock::now();
+    k_band_from_rowmajor<T><<<grid_for((long long)(2 * K + 1) * n, 256, 148 * 32), 256, 0, st>>>(A_dev, B.get(), n, K);
+    SAPB_LAUNCHED();
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_toBanded = ms_since(t1);
+    setup_from_band();
+  }
+
+  void setup_csr_direct(const Csr& A, int K_) override {
+    n = A.n;
+    K = K_;
+    clamp_partitions_banded();
+    B.alloc((size_t)(2 * K + 1) * n);
+    B.zero(st);
+    auto t1 = Clock::now();
+    k_band_from_csr<T><<<grid_for(n, 256), 256, 0, st>>>(A.rp.get(), A.ci.get(), A.v.get(), B.get(), n, K);
+    SAPB_LAUNCHED();
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_toBanded = ms_since(t1);
+    setup_from_band();
+  }
+
+  void setup_from_band() {
+    ptype = o.precondType;
+    spike = (ptype == SAP_PRECOND_SPIKE && P > 1);
+    lu_ul = spike && o.factMethod == SAP_LU_UL;
+    if (ptype == SAP_PRECOND_NONE) return;
+    init_parts_const();
+    if (K == 0) return;
+    auto t0 = Clock::now();
+    if (spike) {
+      offd.alloc((size_t)2 * (P - 1) * K * K);
+      dim3 g(grid_for((long long)K * K, 256, 64), P - 1);
+      k_extract_offdiag<T><<<g, 256, 0, st>>>(parts_d.get(), B.get(), offd.get(), K);
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_offDiags = ms_since(t0);
+    t0 = Clock::now();
+    factor();
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_bandLU = ms_since(t0);
+    t0 = Clock::now();
+    if (spike) {
+      V.alloc((size_t)(P - 1) * K * K);
+      W.alloc((size_t)(P - 1) * K * K);
+      S.alloc((size_t)(P - 1) * K * K);
+      if (lu_ul) {
+        k_spikes_luul<T><<<dim3(P - 1, 2), ((K + 31) / 32) * 32, 0, st>>>(parts_d.get(), P, B.get(),
+                                                                        B2.get() ? B2.get() : B.get(), offd.get(),
+                                                                        V.get(), W.get(), K);
+        SAPB_LAUNCHED();
+      } else {
+        int maxsz = 0;
+        for (auto& p : parts_h) maxsz = std::max(maxsz, p.size);
+        scratch.alloc((size_t)(P - 1) * K * maxsz);
+        k_spikes_luonly<T><<<dim3(P - 1, 2), ((K + 31) / 32) * 32, 0, st>>>(parts_d.get(), B.get(), offd.get(),
+                                                                          V.get(), W.get(), scratch.get(),
+                                                                          (long long)maxsz, K);
+        SAPB_LAUNCHED();
+      }
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      B2.release();
+      scratch.release();
+      t_assembly = ms_since(t0);
+      t0 = Clock::now();
+      k_reduced_factor<T><<<P - 1, 512, 0, st>>>(V.get(), W.get(), S.get(), K, o.safeFactorization ? 1 : 0);
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      t_fullLU = ms_since(t0);
+    }
+    build_sweeps();
+  }
+
+  // partBandedLU / partBlockedBandedUL (sap/precond.h:3882-3983, 4336-4418, 4780-4846).
+  void factor() {
+    std::vector<FactorJob> jobs;
+    bool boost;
+    if (!spike) {
+      boost = o.safeFactorization || (P > 1 && K >= 70);
+      for (int p = 0; p < P; p++) {
+        const auto& d = parts_h[p];
+        jobs.push_back(FactorJob{d.start, d.start + d.size, K, 0, 0, 0, d.boff});
+      }
+    } else {
+      boost = o.safeFactorization || K >= 70;
+      int nlu = lu_ul ? P - 1 : P;
+      for (int p = 0; p < nlu; p++) {
+        const auto& d = parts_h[p];
+        jobs.push_back(FactorJob{d.start, d.start + d.size, K, 0, 0, 0, d.boff});
+      }
+      if (lu_ul) {
+        if (P > 2) {
+          B2.alloc(B.size());
+          SAPB_CUDA(cudaMemcpyAsync(B2.get(), B.get(), B.size() * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        for (int p = 1; p < P; p++) {
+          const auto& d = parts_h[p];
+          int target = (p == P - 1) ? 0 : 1;
+          jobs.push_back(FactorJob{d.start, d.start + d.size, K, 1, target, 0, d.boff});
+        }
+      }
+    }
+    DBuf<FactorJob> jobs_d;
+    jobs_d.upload(jobs, st);
+    flag.alloc(1);
+    flag.zero(st);
+    int G = std::max(1, std::min(K, 512 / std::max(K, 1)));
+    int NT = ((K * G + 31) / 32) * 32;
+    NT = std::max(NT, 64);
+    constexpr int D = 8;
+    size_t smem = ((size_t)(K + 1 + D) * (2 * K + 1) + (K + 1 + D)) * sizeof(T);
+    if (smem <= 200 * 1024) {
+      SAPB_CUDA(cudaFuncSetAttribute(k_factor_smem<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      SAPB_PROF("factor", st);
+      k_factor_smem<T, D><<<(int)jobs.size(), NT, smem, st>>>(jobs_d.get(), B.get(), B2.get(), boost ? 1 : 0,
+                                                             flag.get(), G);
+    } else {
+      SAPB_PROF("factor", st);
+      k_factor_global<T><<<(int)jobs.size(), NT, 0, st>>>(jobs_d.get(), B.get(), B2.get(), boost ? 1 : 0, flag.get(), G);
+    }
+    SAPB_LAUNCHED();
+    int hflag = 0;
+    SAPB_CUDA(cudaMemcpyAsync(&hflag, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    if (hflag && !o.safeFactorization) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
+  }
+
+  void build_sweeps() {
+    int maxK = parts_maxK();
+    if (maxK > 1024) throw Error(SAP_ERR_UNSUPPORTED, "half-bandwidth above 1024 is not supported by the sweep kernels");
+    chunks_h.clear();
+    std::vector<long long> koff, toff;
+    std::vector<int> first1, first2, pc0, pnc;
+    long long ko = 0, to = 0;
+    maxChunk = 0;
+    for (int p = 0; p < (int)parts_h.size(); p++) {
+      const auto& d = parts_h[p];
+      int Kp = d.K;
+      int m = std::min(4096, std::max(256, 8 * Kp));
+      int nc = std::max(1, d.size / m);
+      pc0.push_back((int)chunks_h.size());
+      pnc.push_back(nc);
+      int base = d.size / nc, rem = d.size % nc, a = d.start;
+      for (int c = 0; c < nc; c++) {
+        int len = base + (c < rem ? 1 : 0);
+        chunks_h.push_back(ChunkDev{p, a, a + len, 0});
+        maxChunk = std::max(maxChunk, len);
+        koff.push_back(ko);
+        toff.push_back(to);
+        ko += Kp;
+        to += (long long)Kp * Kp;
+        bool down1 = !d.ul;
+        first1.push_back(down1 ? (c == 0) : (c == nc - 1));
+        first2.push_back(down1 ? (c == nc - 1) : (c == 0));
+        a += len;
+      }
+    }
+    chunks_d.upload(chunks_h, st);
+    koff_d.upload(koff, st);
+    toff_d.upload(toff, st);
+    first1_d.upload(first1, st);
+    first2_d.upload(first2, st);
+    pchunk0_d.upload(pc0, st);
+    pnchunk_d.upload(pnc, st);
+    T1.alloc(std::max<long long>(to, 1));
+    T2.alloc(std::max<long long>(to, 1));
+    tails1.alloc(std::max<long long>(ko, 1));
+    tails2.alloc(std::max<long long>(ko, 1));
+    carry1.alloc(std::max<long long>(ko, 1));
+    carry2.alloc(std::max<long long>(ko, 1));
+    F.alloc(n);
+    Gv.alloc(n);
+    Y.alloc(n);
+    sweepThreads = std::max(32, ((maxK + 31) / 32) * 32);
+    scanG = std::max(1, std::min(maxK, 512 / std::max(1, maxK)));
+    const int nch = (int)chunks_h.size();
+    const int tthreads = sweepThreads;
+    size_t tsmem = (size_t)maxK * tthreads * sizeof(T);
+    DBuf<T> gring;
+    auto t0 = Clock::now();
+    if (tsmem > 200 * 1024) {
+      gring.alloc((size_t)nch * maxK * tthreads);
+      tsmem = 0;
+    } else {
+      SAPB_CUDA(cudaFuncSetAttribute(k_transfer<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(tsmem, 1024)));
+    }
+    SAPB_PROF("transfer", st);
+    k_transfer<T><<<nch, tthreads, tsmem, st>>>(parts_d.get(), chunks_d.get(), toff_d.get(), B.get(), T1.get(), 1, gring.get(), first1_d.get());
+    SAPB_LAUNCHED();
+    k_transfer<T><<<nch, tthreads, tsmem, st>>>(parts_d.get(), chunks_d.get(), toff_d.get(), B.get(), T2.get(), 2, gring.get(), first2_d.get());
+    SAPB_LAUNCHED();
+    size_t s1 = (size_t)(maxK + maxChunk) * sizeof(T);
+    if (2 * s1 > 220 * 1024) throw Error(SAP_ERR_UNSUPPORTED, "sweep chunk does not fit in shared memory");
+    SAPB_CUDA(cudaFuncSetAttribute(k_pass2<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * s1)));
+    SAPB_CUDA(cudaFuncSetAttribute(k_pass1<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+    SAPB_CUDA(cudaFuncSetAttribute(k_pass3<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s1));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_assembly += ms_since(t0);
+  }
+
+  // One partitioned sweep pair: out = D^-1 rhs, rhs = vin (FP64) or F.
+  void sweep_pair(const double* vin, double* zout, T* gout) {
+    const int nch = (int)chunks_h.size();
+    const int maxK = parts_maxK();
+    const size_t s1 = (size_t)(maxK + maxChunk) * sizeof(T);
+    const int NT = sweepThreads;
+    const int scanNT = ((maxK * scanG + 31) / 32) * 32;
+    const size_t ssm = (size_t)(maxK + scanG * maxK) * sizeof(T);
+    {
+      SAPB_PROF("pass1", st);
+      k_pass1<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), koff_d.get(), B.get(), vin, F.get(), tails1.get());
+      SAPB_LAUNCHED();
+    }
+    {
+      SAPB_PROF("scan", st);
+      k_scan<T><<<(int)parts_h.size(), scanNT, ssm, st>>>(parts_d.get(), pchunk0_d.get(), pnchunk_d.get(), koff_d.get(),
+                                                          toff_d.get(), T1.get(), tails1.get(), carry1.get(), 1, scanG);
+      SAPB_LAUNCHED();
+    }
+    {
+      SAPB_PROF("pass2", st);
+      k_pass2<T, 16><<<nch, NT, 2 * s1, st>>>(parts_d.get(), chunks_d.get(), first1_d.get(), koff_d.get(), B.get(),
+                                              F.get(), carry1.get(), Y.get(), tails2.get());
+      SAPB_LAUNCHED();
+    }
+    {
+      SAPB_PROF("scan", st);
+      k_scan<T><<<(int)parts_h.size(), scanNT, ssm, st>>>(parts_d.get(), pchunk0_d.get(), pnchunk_d.get(), koff_d.get(),
+                                                          toff_d.get(), T2.get(), tails2.get(), carry2.get(), 2, scanG);
+      SAPB_LAUNCHED();
+    }
+    {
+      SAPB_PROF("pass3", st);
+      k_pass3<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), first2_d.get(), koff_d.get(), B.get(), Y.get(),
+                                          carry2.get(), zout, gout);
+      SAPB_LAUNCHED();
+    }
+  }
+
+  // Precond::operator() + solve + getSRev (sap/precond.h:1370-1528) in the
+  // band's row order.
+  void apply_band(const double* v, double* z) override {
+    if (ptype == SAP_PRECOND_NONE) {
+      SAPB_CUDA(cudaMemcpyAsync(z, v, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      return;
+    }
+    if (K == 0) {
+      k_diag_apply<T><<<grid_for(n, 256), 256, 0, st>>>(B.get(), v, z, n);
+      SAPB_LAUNCHED();
+      return;
+    }
+    if (spike) {
+      sweep_pair(v, nullptr, Gv.get());
+      SAPB_PROF("reduced_apply", st);
+      k_reduced_apply<T><<<P - 1, ((K + 31) / 32) * 32, 3 * K * sizeof(T), st>>>(parts_d.get(), V.get(), W.get(), S.get(),
+                                                                            offd.get(), Gv.get(), F.get(), K);
+      SAPB_LAUNCHED();
+      sweep_pair(nullptr, z, nullptr);
+    } else {
+      sweep_pair(v, z, nullptr);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// BiCGStabLMonitor (sap/monitor.h:154-339).
+struct Monitor {
+  int maxIt = 100, maxm = 8, stag = 0, more = 0, maxStag = 3;
+  double relTol = 1e-6, absTol = 0, rhsNorm = 0, rNorm = std::numeric_limits<double>::max();
+  float it = 0;
+  int code = 0;
+  std::string msg;
+  void init(double rhs) { rhsNorm = rhs; it = 0; code = 0; msg = ""; stag = 0; more = 0; }
+  double tol() const { return absTol + relTol * rhsNorm; }
+  void stop(int c, const char* m) { code = c; msg = m; }
+  bool finished(double r) {
+    rNorm = r;
+    if (code != 0) return true;
+    if (std::isnan(rNorm)) stop(-2, "Residual norm is NaN");
+    else if (rNorm <= tol()) stop(1, "Converged");
+    else if (it > maxIt) stop(-1, "Maximum number of iterations was reached");
+    else {
+      if (stag >= maxStag && more == 0) stag = 0;
+      more++;
+      if (more >= maxm) stop(-3, "Stagnation encountered");
+    }
+    return code != 0;
+  }
+  bool finished() {
+    if (code != 0) return true;
+    if (it > maxIt) stop(-1, "Maximum number of iterations was reached");
+    return code != 0;
+  }
+  bool needCheck(double r) {
+    rNorm = r;
+    if (code != 0) return false;
+    if (std::isnan(rNorm)) stop(-2, "Residual norm is NaN");
+    return code == 0 && (rNorm <= tol() || stag >= maxStag || more);
+  }
+};
+
+// ---------------------------------------------------------------------------
+class Solver {
+ public:
+  sap_options opts{};
+  int P_req = 1;
+  int prec_dtype = SAP_PREC_FLOAT;
+  cudaStream_t st = nullptr;
+  std::unique_ptr<PrecBase> pcp;
+  PrecBase& pc() { return *pcp; }
+  Monitor mon;
+  sap_stats stats{};
+  bool setup_done = false;
+  int n = 0;
+  long long nnz = 0;
+  // Krylov workspace
+  DBuf<double> dots_part, dots_out;
+  DBuf<unsigned int> dots_ctr;
+  double* pinned = nullptr;
+  DBuf<double> bvec, xvec;
+
+  Solver(int P, const sap_options& o, int dtype) : opts(o), P_req(P), prec_dtype(dtype) {
+    SAPB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (dtype == SAP_PREC_DOUBLE) pcp = std::make_unique<PrecondT<double>>();
+    else pcp = std::make_unique<PrecondT<float>>();
+    pcp->o = o;
+    pcp->P_req = P;
+    pcp->st = st;
+    mon.maxIt = o.maxNumIterations;
+    mon.relTol = o.relTol;
+    mon.absTol = o.absTol;
+    dots_part.alloc(4 * kDotBlocks);
+    dots_out.alloc(4);
+    dots_ctr.alloc(1);
+    dots_ctr.zero(st);
+    SAPB_CUDA(cudaMallocHost(&pinned, 8 * sizeof(double)));
+    init_stats();
+  }
+  ~Solver() {
+    if (pinned) cudaFreeHost(pinned);
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  }
+  void init_stats() {
+    std::memset(&stats, 0, sizeof(stats));
+    stats.rhsNorm = stats.residualNorm = stats.relResidualNorm = std::numeric_limits<double>::max();
+  }
+
+  // -- BLAS-1 on the solver stream ------------------------------------------
+  void axpby(const double* x, const double* y, double* z, double a, double b) {
+    k_axpby<<<grid_for(n, 256), 256, 0, st>>>(n, a, x, b, y, z);
+    SAPB_LAUNCHED();
+  }
+  void axpy(const double* x, double* y, double a) {
+    k_axpy<<<grid_for(n, 256), 256, 0, st>>>(n, a, x, y);
+    SAPB_LAUNCHED();
+  }
+  void copy(const double* x, double* y) {
+    SAPB_CUDA(cudaMemcpyAsync(y, x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
+  // up to four dot products, returned on the host
+  void dots(int nq, const double* const* xs, const double* const* ys, double* out) {
+    DotArgs a{};
+    a.nq = nq;
+    for (int q = 0; q < nq; q++) { a.x[q] = xs[q]; a.y[q] = ys[q]; }
+    {
+      SAPB_PROF("dots", st);
+      k_dots<<<kDotBlocks, kDotThreads, 0, st>>>(n, a, dots_part.get(), dots_ctr.get(), dots_out.get());
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaMemcpyAsync(pinned, dots_out.get(), nq * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < nq; q++) out[q] = pinned[q];
+  }
+  double dot(const double* x, const double* y) {
+    double r;
+    dots(1, &x, &y, &r);
+    return r;
+  }
+  double nrm2(const double* x) { return std::sqrt(dot(x, x)); }
+
+  // bicgstabl<..., L> (sap/bicgstab2.h:32-360)
+  void bicgstabl(const Spmv& A, double* x, const double* b, int L);
+};
+
+void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
+  const double eps = 1e-20;
+  double rho0 = 1, alpha = 0, omega = 1, rho1;
+  std::vector<DBuf<double>> rr(L + 1), uu(L + 1);
+  DBuf<double> r0, xx, Pv, x_min, Pxx, APxx;
+  for (int k = 0; k <= L; k++) {
+    rr[k].alloc(n); rr[k].zero(st);
+    uu[k].alloc(n); uu[k].zero(st);
+  }
+  r0.alloc(n); xx.alloc(n); Pv.alloc(n); x_min.alloc(n); Pxx.alloc(n); APxx.alloc(n);
+  x_min.zero(st);
+  std::vector<std::vector<double>> tao(L + 1, std::vector<double>(L + 1, 0.0));
+  std::vector<double> gamma(L + 2), gp(L + 2), gpp(L + 2), sigma(L + 2);
+  auto Pm = [&](const double* in, double* out) { pcp->apply(in, out); };
+  auto Am = [&](const double* in, double* out) { A.apply(in, out, st); };
+
+  // r0 <- b - A x ; r <- r0 ; uu0 <- 0 ; xx <- x ; rr0 <- r
+  Am(x, r0.get());
+  axpby(b, r0.get(), r0.get(), 1.0, -1.0);
+  copy(x, xx.get());
+  copy(r0.get(), rr[0].get());
+  double r_norm_min = nrm2(rr[0].get()), r_norm = r_norm_min, r_norm_act = r_norm;
+  auto recheck = [&]() {
+    Pm(xx.get(), Pxx.get());
+    Am(Pxx.get(), APxx.get());
+    axpby(b, APxx.get(), rr[0].get(), 1.0, -1.0);
+    r_norm_act = nrm2(rr[0].get());
+  };
+  auto stag_check = [&](double coef, const double* v) {
+    const double* xs[2] = {v, xx.get()};
+    double d[2];
+    dots(2, xs, xs, d);
+    if (std::fabs(coef) * std::sqrt(d[0]) < eps * std::sqrt(d[1])) mon.stag++;
+    else mon.stag = 0;
+  };
+  while (true) {
+    rho0 = -omega * rho0;
+    mon.it += 0.25f;
+    for (int j = 0; j < L; j++) {
+      rho1 = dot(rr[j].get(), r0.get());
+      if (rho0 == 0) { mon.stop(-10, "rho0 is zero"); break; }
+      double beta = alpha * rho1 / rho0;
+      rho0 = rho1;
+      for (int i = 0; i <= j; i++) axpby(rr[i].get(), uu[i].get(), uu[i].get(), 1.0, -beta);
+      Pm(uu[j].get(), Pv.get());
+      Am(Pv.get(), uu[j + 1].get());
+      double gam = dot(uu[j + 1].get(), r0.get());
+      if (gam == 0) { mon.stop(-11, "gamma is zero"); break; }
+      alpha = rho0 / gam;
+      for (int i = 0; i <= j; i++) axpy(uu[i + 1].get(), rr[i].get(), -alpha);
+      r_norm_act = r_norm = nrm2(rr[0].get());
+      Pm(rr[j].get(), Pv.get());
+      Am(Pv.get(), rr[j + 1].get());
+      stag_check(alpha, uu[0].get());
+      axpy(uu[0].get(), xx.get(), alpha);
+      if (mon.needCheck(r_norm)) {
+        recheck();
+        if (mon.finished(r_norm_act)) break;
+      }
+      if (r_norm_act < r_norm_min) { r_norm_min = r_norm_act; copy(xx.get(), x_min.get()); }
+      if (mon.finished()) break;
+    }
+    if (mon.finished()) break;
+    for (int j = 1; j <= L; j++) {
+      for (int i = 1; i < j; i++) {
+        tao[i][j] = dot(rr[j].get(), rr[i].get()) / sigma[i];
+        axpy(rr[i].get(), rr[j].get(), -tao[i][j]);
+      }
+      const double* xs[2] = {rr[j].get(), rr[j].get()};
+      const double* ys[2] = {rr[j].get(), rr[0].get()};
+      double d[2];
+      dots(2, xs, ys, d);
+      sigma[j] = d[0];
+      if (sigma[j] == 0) { mon.stop(-12, "a sigma value is zero"); break; }
+      gp[j] = d[1] / sigma[j];
+    }
+    if (mon.finished()) break;
+    gamma[L] = gp[L];
+    omega = gamma[L];
+    for (int j = L - 1; j > 0; j--) {
+      gamma[j] = gp[j];
+      for (int i = j + 1; i <= L; i++) gamma[j] -= tao[j][i] * gamma[i];
+    }
+    for (int j = 1; j < L; j++) {
+      gpp[j] = gamma[j + 1];
+      for (int i = j + 1; i < L; i++) gpp[j] += tao[j][i] * gamma[i + 1];
+    }
+    stag_check(gamma[1], rr[0].get());
+    axpy(rr[0].get(), xx.get(), gamma[1]);
+    axpy(rr[L].get(), rr[0].get(), -gp[L]);
+    axpy(uu[L].get(), uu[0].get(), -gamma[L]);
+    r_norm_act = r_norm = nrm2(rr[0].get());
+    mon.it += 0.25f;
+    if (mon.needCheck(r_norm)) {
+      recheck();
+      if (mon.finished(r_norm_act)) break;
+    }
+    if (r_norm_act < r_norm_min) { r_norm_min = r_norm_act; copy(xx.get(), x_min.get()); }
+    if (mon.finished()) break;
+    mon.it += 0.25f;
+    for (int j = 1; j < L; j++) {
+      axpy(uu[j].get(), uu[0].get(), -gamma[j]);
+      stag_check(gpp[j], rr[j].get());
+      axpy(rr[j].get(), xx.get(), gpp[j]);
+      axpy(rr[j].get(), rr[0].get(), -gp[j]);
+      r_norm_act = r_norm = nrm2(rr[0].get());
+      if (mon.needCheck(r_norm)) {
+        recheck();
+        if (mon.finished(r_norm_act)) break;
+      }
+      if (r_norm_act < r_norm_min) { r_norm_min = r_norm_act; copy(xx.get(), x_min.get()); }
+      if (mon.finished()) break;
+    }
+    if (mon.finished()) break;
+    mon.it += 0.25f;
+  }
+  if (mon.code > 0) {
+    Pm(xx.get(), x);
+  } else {
+    DBuf<double> Pxmin, APxmin, rc, rcm;
+    Pxmin.alloc(n); APxmin.alloc(n); rc.alloc(n); rcm.alloc(n);
+    Pm(xx.get(), Pxx.get());
+    Am(Pxx.get(), APxx.get());
+    axpby(b, APxx.get(), rc.get(), 1.0, -1.0);
+    Pm(x_min.get(), Pxmin.get());
+    Am(Pxmin.get(), APxmin.get());
+    axpby(b, APxmin.get(), rcm.get(), 1.0, -1.0);
+    double a = nrm2(rc.get()), c = nrm2(rcm.get());
+    if (a < c) { copy(Pxx.get(), x); mon.rNorm = a; }
+    else { copy(Pxmin.get(), x); mon.rNorm = c; }
+  }
+  SAPB_CUDA(cudaStreamSynchronize(st));
+}
+
+// Precond::operator() with the reordering transforms (leftTrans / rightTrans,
+// sap/precond.h:1535-1559) around the band apply.
+void PrecBase::apply(const double* v, double* z) {
+  if (!reordered) { apply_band(v, z); return; }
+  reorder_apply_in(*this, v, vtmp.get());
+  apply_band(vtmp.get(), ztmp.get());
+  reorder_apply_out(*this, ztmp.get(), z);
+}
+
+void reorder_setup(PrecBase&, const Csr&) {
+  throw Error(SAP_ERR_UNSUPPORTED, "reordering is not available yet");
+}
+void reorder_apply_in(PrecBase&, const double*, double*) {}
+void reorder_apply_out(PrecBase&, const double*, double*) {}
+
+}  // namespace sapb
+
+// ===========================================================================
+// C ABI
+using namespace sapb;
+
+struct sap_solver { std::unique_ptr<Solver> s; };
+struct sap_banded { Banded b; };
+struct sap_csr { Csr c; };
+struct sap_spmv { Spmv op; cudaStream_t st = nullptr; };
+
+#define SAP_TRY(...)                                     \
+  try {                                                  \
+    __VA_ARGS__;                                         \
+    return SAP_OK;                                       \
+  } catch (const sapb::Error& e) {                       \
+    g_last_error = e.what();                             \
+    return e.code;                                       \
+  } catch (const std::bad_alloc&) {                      \
+    g_last_error = "host allocation failed";             \
+    return SAP_ERR_OUT_OF_MEMORY;                        \
+  } catch (const std::exception& e) {                    \
+    g_last_error = e.what();                             \
+    return SAP_ERR_CUDA;                                 \
+  }
+
+#define SAP_REQUIRE(cond, msg) \
+  do { if (!(cond)) throw sapb::Error(SAP_ERR_INVALID_ARGUMENT, msg); } while (0)
+
+extern "C" {
+
+const char* sap_last_error(void) { return g_last_error.c_str(); }
+int64_t sap_kernel_launch_count(void) { return g_launches.load(); }
+
+int sap_profile_select(const char* name) {
+  SAP_TRY({
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    for (auto& pr : g_prof.pairs) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    g_prof.pairs.clear();
+    g_prof.name = name ? name : "";
+  });
+}
+
+int sap_profile_read(double* total_ms, int64_t* launches) {
+  SAP_TRY({
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    double tot = 0;
+    for (auto& pr : g_prof.pairs) {
+      SAPB_CUDA(cudaEventSynchronize(pr.second));
+      float ms = 0;
+      SAPB_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = (int64_t)g_prof.pairs.size();
+  });
+}
+
+int sap_options_default(sap_options* o) {
+  SAP_TRY({
+    SAP_REQUIRE(o, "null options");
+    std::memset(o, 0, sizeof(*o));
+    o->solverType = SAP_BICGSTAB2;
+    o->maxNumIterations = 100;
+    o->relTol = 1e-6;
+    o->absTol = 0;
+    o->performReorder = 1;
+    o->performDB = 1;
+    o->applyScaling = 1;
+    o->maxBandwidth = std::numeric_limits<int>::max();
+    o->gpuCount = 1;
+    o->dropOffFraction = 0;
+    o->factMethod = SAP_LU_ONLY;
+    o->precondType = SAP_PRECOND_SPIKE;
+    o->variableBandwidth = 1;
+    o->ilu_level = -1;
+  });
+}
+
+int sap_banded_create(int n, int k, const double* data, int memspace, sap_banded** out) {
+  SAP_TRY({
+    SAP_REQUIRE(out && data && n > 0 && k >= 0 && k < n, "invalid banded matrix arguments");
+    auto h = std::make_unique<sap_banded>();
+    h->b.n = n; h->b.K = k;
+    size_t cnt = (size_t)n * (2 * k + 1);
+    h->b.A.alloc(cnt);
+    SAPB_CUDA(cudaMemcpy(h->b.A.get(), data, cnt * sizeof(double),
+                         memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    *out = h.release();
+  });
+}
+
+int sap_banded_generate(int n, int k, double d, int dist, uint64_t seed, sap_banded** out) {
+  SAP_TRY({
+    SAP_REQUIRE(out && n > 0 && k >= 0 && k < n && dist >= 0 && dist <= 2, "invalid generator arguments");
+    std::vector<double> h((size_t)n * (2 * k + 1), 0.0);
+    sapb::generate_band(n, k, d, dist, seed, h.data());
+    auto m = std::make_unique<sap_banded>();
+    m->b.n = n; m->b.K = k;
+    m->b.A.alloc(h.size());
+    SAPB_CUDA(cudaMemcpy(m->b.A.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    *out = m.release();
+  });
+}
+
+int sap_generate_band_host(int n, int k, double d, int dist, uint64_t seed, double* out) {
+  SAP_TRY({
+    SAP_REQUIRE(out && n > 0 && k >= 0 && k < n && dist >= 0 && dist <= 2, "invalid generator arguments");
+    std::memset(out, 0, sizeof(double) * (size_t)n * (2 * k + 1));
+    sapb::generate_band(n, k, d, dist, seed, out);
+  });
+}
+
+int sap_banded_copy_out(const sap_banded* A, double* dst, int memspace) {
+  SAP_TRY({
+    SAP_REQUIRE(A && dst, "null argument");
+    SAPB_CUDA(cudaMemcpy(dst, A->b.A.get(), A->b.A.size() * sizeof(double),
+                         memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+  });
+}
+
+int sap_banded_info(const sap_banded* A, int* n, int* k) {
+  SAP_TRY({
+    SAP_REQUIRE(A, "null matrix");
+    if (n) *n = A->b.n;
+    if (k) *k = A->b.K;
+  });
+}
+
+int sap_banded_destroy(sap_banded* A) { delete A; return SAP_OK; }
+
+int sap_csr_create(int n, int nnz, const int* rp, const int* ci, const double* v, int memspace, sap_csr** out) {
+  SAP_TRY({
+    SAP_REQUIRE(out && rp && ci && v && n > 0 && nnz >= 0, "invalid CSR arguments");
+    auto h = std::make_unique<sap_csr>();
+    h->c.n = n; h->c.nnz = nnz;
+    h->c.rp_h.resize(n + 1); h->c.ci_h.resize(nnz); h->c.v_h.resize(nnz);
+    cudaMemcpyKind kind = memspace == SAP_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+    SAPB_CUDA(cudaMemcpy(h->c.rp_h.data(), rp, (n + 1) * sizeof(int), kind));
+    SAPB_CUDA(cudaMemcpy(h->c.ci_h.data(), ci, (size_t)nnz * sizeof(int), kind));
+    SAPB_CUDA(cudaMemcpy(h->c.v_h.data(), v, (size_t)nnz * sizeof(double), kind));
+    SAP_REQUIRE(h->c.rp_h[0] == 0 && h->c.rp_h[n] == nnz, "row offsets inconsistent with nnz");
+    for (int i = 0; i < n; i++) SAP_REQUIRE(h->c.rp_h[i] <= h->c.rp_h[i + 1], "row offsets not monotone");
+    for (int p = 0; p < nnz; p++) SAP_REQUIRE(h->c.ci_h[p] >= 0 && h->c.ci_h[p] < n, "column index out of range");
+    h->c.rp.upload(h->c.rp_h, nullptr);
+    h->c.ci.upload(h->c.ci_h, nullptr);
+    h->c.v.upload(h->c.v_h, nullptr);
+    SAPB_CUDA(cudaDeviceSynchronize());
+    *out = h.release();
+  });
+}
+
+int sap_csr_info(const sap_csr* A, int* n, int* nnz) {
+  SAP_TRY({
+    SAP_REQUIRE(A, "null matrix");
+    if (n) *n = A->c.n;
+    if (nnz) *nnz = A->c.nnz;
+  });
+}
+
+int sap_csr_destroy(sap_csr* A) { delete A; return SAP_OK; }
+
+int sap_spmv_banded_create(const sap_banded* A, sap_spmv** out) {
+  SAP_TRY({
+    SAP_REQUIRE(A && out, "null argument");
+    auto h = std::make_unique<sap_spmv>();
+    h->op.kind = 0; h->op.band = &A->b; h->op.n = A->b.n;
+    *out = h.release();
+  });
+}
+
+int sap_spmv_csr_create(const sap_csr* A, sap_spmv** out) {
+  SAP_TRY({
+    SAP_REQUIRE(A && out, "null argument");
+    auto h = std::make_unique<sap_spmv>();
+    h->op.kind = 1; h->op.csr = &A->c; h->op.n = A->c.n;
+    *out = h.release();
+  });
+}
+
+int sap_spmv_callback_create(int n, sap_spmv_fn fn, void* ctx, sap_spmv** out) {
+  SAP_TRY({
+    SAP_REQUIRE(fn && out && n > 0, "invalid callback operator");
+    auto h = std::make_unique<sap_spmv>();
+    h->op.kind = 2; h->op.fn = fn; h->op.ctx = ctx; h->op.n = n;
+    *out = h.release();
+  });
+}
+
+int sap_spmv_apply(sap_spmv* op, const double* x, double* y) {
+  SAP_TRY({
+    SAP_REQUIRE(op && x && y, "null argument");
+    op->op.apply(x, y, nullptr);
+    SAPB_CUDA(cudaStreamSynchronize(nullptr));
+  });
+}
+
+int sap_spmv_destroy(sap_spmv* op) { delete op; return SAP_OK; }
+
+int sap_solver_create(int P, const sap_options* opts, int prec_dtype, sap_solver** out) {
+  SAP_TRY({
+    SAP_REQUIRE(out && opts && P >= 1, "invalid solver arguments");
+    SAP_REQUIRE(prec_dtype == SAP_PREC_FLOAT || prec_dtype == SAP_PREC_DOUBLE, "invalid preconditioner type");
+    auto h = std::make_unique<sap_solver>();
+    h->s = std::make_unique<Solver>(P, *opts, prec_dtype);
+    *out = h.release();
+  });
+}
+
+int sap_solver_destroy(sap_solver* s) { delete s; return SAP_OK; }
+
+static void finish_setup_stats(Solver& S, double t_setup) {
+  auto& st = S.stats;
+  auto& pc = S.pc();
+  st.timeSetup = t_setup;
+  st.bandwidthReorder = pc.k_reorder;
+  st.bandwidthDB = pc.k_db;
+  st.bandwidth = pc.K;
+  st.numPartitions = pc.P;
+  st.actualDropOff = pc.drop_actual;
+  st.time_toBanded = pc.t_toBanded;
+  st.time_offDiags = pc.t_offDiags;
+  st.time_bandLU = pc.t_bandLU;
+  st.time_assembly = pc.t_assembly;
+  st.time_fullLU = pc.t_fullLU;
+  st.time_reorder = pc.t_reorder;
+  st.time_dropOff = pc.t_dropOff;
+  st.time_cpu_assemble = pc.t_cpu_assemble;
+  st.time_transfer = pc.t_transfer;
+}
+
+int sap_solver_setup_banded(sap_solver* h, const sap_banded* A) {
+  SAP_TRY({
+    SAP_REQUIRE(h && A, "null argument");
+    Solver& S = *h->s;
+    auto t0 = Clock::now();
+    PrecBase& pc = S.pc();
+    pc.reordered = false;
+    pc.setup_rowmajor(A->b.A.get(), A->b.n, A->b.K);
+    SAPB_CUDA(cudaStreamSynchronize(pc.st));
+    S.n = pc.n;
+    S.nnz = (long long)A->b.n * (2 * A->b.K + 1);
+    S.setup_done = true;
+    finish_setup_stats(S, ms_since(t0));
+  });
+}
+
+int sap_solver_setup_csr(sap_solver* h, const sap_csr* A) {
+  SAP_TRY({
+    SAP_REQUIRE(h && A, "null argument");
+    Solver& S = *h->s;
+    auto t0 = Clock::now();
+    PrecBase& pc = S.pc();
+    if (!S.opts.performReorder) {
+      // convertToBandedMatrix(CSR) (sap/precond.h:2240-2368)
+      pc.reordered = false;
+      int K = 0;
+      for (int i = 0; i < A->c.n; i++)
+        for (int p = A->c.rp_h[i]; p < A->c.rp_h[i + 1]; p++) K = std::max(K, std::abs(i - A->c.ci_h[p]));
+      pc.setup_csr_direct(A->c, K);
+    } else {
+      reorder_setup(pc, A->c);
+    }
+    SAPB_CUDA(cudaStreamSynchronize(pc.st));
+    S.n = pc.n;
+    S.nnz = A->c.nnz;
+    S.setup_done = true;
+    finish_setup_stats(S, ms_since(t0));
+  });
+}
+
+int sap_solver_update(sap_solver* h, const double* entries, int64_t nnz, int memspace, int* accepted) {
+  SAP_TRY({
+    SAP_REQUIRE(h && entries, "null argument");
+    Solver& S = *h->s;
+    if (!S.setup_done) throw Error(SAP_ILLEGAL_UPDATE, "Illegal call to update() before setup().");
+    if (!S.opts.trackReordering)
+      throw Error(SAP_ILLEGAL_UPDATE, "Illegal call to update() with reordering tracking disabled.");
+    if (nnz != S.nnz) {
+      if (accepted) *accepted = 0;
+      return SAP_OK;
+    }
+    (void)memspace;
+    throw Error(SAP_ERR_UNSUPPORTED, "update() is not available yet");
+  });
+}
+
+int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, int memspace, int* converged) {
+  SAP_TRY({
+    SAP_REQUIRE(h && spmv && b && x, "null argument");
+    Solver& S = *h->s;
+    if (!S.setup_done) throw Error(SAP_ILLEGAL_SOLVE, "Illegal call to solve() before setup().");
+    SAP_REQUIRE(spmv->op.n == S.n, "operator size differs from the preconditioner's");
+    int L = 0;
+    if (S.opts.solverType == SAP_BICGSTAB2) L = 2;
+    else if (S.opts.solverType == SAP_BICGSTAB1) L = 1;
+    else throw Error(SAP_ERR_UNSUPPORTED, "only BiCGStab1 / BiCGStab2 are provided");
+    auto t0 = Clock::now();
+    const size_t bytes = (size_t)S.n * sizeof(double);
+    S.bvec.alloc(S.n);
+    S.xvec.alloc(S.n);
+    cudaMemcpyKind kin = memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    SAPB_CUDA(cudaMemcpyAsync(S.bvec.get(), b, bytes, kin, S.st));
+    SAPB_CUDA(cudaMemcpyAsync(S.xvec.get(), x, bytes, kin, S.st));
+    S.mon.init(S.nrm2(S.bvec.get()));
+    S.bicgstabl(spmv->op, S.xvec.get(), S.bvec.get(), L);
+    cudaMemcpyKind kout = memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    SAPB_CUDA(cudaMemcpyAsync(x, S.xvec.get(), bytes, kout, S.st));
+    SAPB_CUDA(cudaStreamSynchronize(S.st));
+    S.stats.timeSolve = ms_since(t0);
+    S.stats.rhsNorm = S.mon.rhsNorm;
+    S.stats.residualNorm = S.mon.rNorm;
+    S.stats.relResidualNorm = S.mon.rNorm / S.mon.rhsNorm;
+    S.stats.numIterations = S.mon.it;
+    if (converged) *converged = S.mon.code > 0 ? 1 : 0;
+  });
+}
+
+int sap_precond_apply(sap_solver* h, const double* v, double* z) {
+  SAP_TRY({
+    SAP_REQUIRE(h && v && z, "null argument");
+    Solver& S = *h->s;
+    if (!S.setup_done) throw Error(SAP_ILLEGAL_SOLVE, "preconditioner used before setup().");
+    S.pc().apply(v, z);
+    SAPB_CUDA(cudaStreamSynchronize(S.st));
+  });
+}
+
+int sap_solver_get_stats(const sap_solver* h, sap_stats* out) {
+  SAP_TRY({
+    SAP_REQUIRE(h && out, "null argument");
+    *out = h->s->stats;
+  });
+}
+
+int sap_solver_get_monitor(const sap_solver* h, int* code, const char** message) {
+  SAP_TRY({
+    SAP_REQUIRE(h, "null argument");
+    if (code) *code = h->s->mon.code;
+    if (message) *message = h->s->mon.msg.c_str();
+  });
+}
+
+int sap_solver_info(const sap_solver* h, int* n, int* k, int* P) {
+  SAP_TRY({
+    SAP_REQUIRE(h, "null argument");
+    if (n) *n = h->s->pcp->n;
+    if (k) *k = h->s->pcp->K;
+    if (P) *P = h->s->pcp->P;
+  });
+}
+
+void* sap_solver_stream(const sap_solver* h) { return h ? (void*)h->s->st : nullptr; }
+
+}  // extern "C"
