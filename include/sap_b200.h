@@ -159,6 +159,15 @@ int sap_spmv_callback_create(int n, sap_spmv_fn fn, void* ctx, sap_spmv** out);
 int sap_spmv_apply(sap_spmv* op, const double* x, double* y);
 int sap_spmv_destroy(sap_spmv* op);
 
+/* ---- BLAS-1 ------------------------------------------------------------------ */
+/* nq <= 4 dot products out[q] = sum_i x[q][i] * y[q][i] of FP64 device
+ * vectors in one pass: the fused form of the cusp::blas::dotc calls of the
+ * Krylov monitor (sap/bicgstab2.h:98-300).  `out` is a device array of nq
+ * doubles; the work is enqueued on `stream` (a cudaStream_t, NULL for the
+ * legacy default stream) and the call returns without waiting.  Block partial
+ * sums live in scratch allocated and freed on the stream by each call. */
+int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y, double* out, void* stream);
+
 /* ---- solver --------------------------------------------------------------- */
 /* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297). */
 int sap_solver_create(int num_partitions, const sap_options* opts, int prec_dtype,

@@ -24,7 +24,7 @@ _LIB_PATH = os.path.join(_HERE, "libsap_b200.so")
 
 if not os.path.exists(_LIB_PATH):
     raise ImportError(
-        f"saplibrary_b200: {_LIB_PATH} is missing; build it with `python -m saplibrary_b200.build`")
+        f"saplibrary_b200: {_LIB_PATH} is missing; build it with `python saplibrary_b200/build.py`")
 _lib = ctypes.CDLL(_LIB_PATH)
 
 # ---- enums (sap/common.h) ----------------------------------------------------
@@ -112,6 +112,7 @@ _sig = {
     "sap_solver_get_monitor": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_char_p)]),
     "sap_solver_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_solver_stream": (_vp, [_vp]),
+    "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_profile_select": (_i, [ctypes.c_char_p]),
     "sap_profile_read": (_i, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
 }
@@ -160,6 +161,16 @@ def profile_read() -> tuple[float, int]:
     ms, cnt = ctypes.c_double(), ctypes.c_int64()
     _check(_lib.sap_profile_read(ctypes.byref(ms), ctypes.byref(cnt)))
     return ms.value, cnt.value
+
+
+def blas_dots(xs, ys, out, stream: int = 0) -> None:
+    """Fused FP64 dot products out[q] = xs[q] . ys[q] (q < 4) of CUDA tensors,
+    through sap_blas_dots; `out` is a CUDA float64 tensor of len(xs)."""
+    nq = len(xs)
+    n = xs[0].numel()
+    xa = (ctypes.c_void_p * nq)(*[t.data_ptr() for t in xs])
+    ya = (ctypes.c_void_p * nq)(*[t.data_ptr() for t in ys])
+    _check(_lib.sap_blas_dots(n, nq, xa, ya, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream)))
 
 
 def generate_band_host(n: int, k: int, d: float, dist: int = 1, seed: int = 0) -> np.ndarray:

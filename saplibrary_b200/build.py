@@ -1,6 +1,6 @@
 """Build recipe of the sap_b200 CUDA library (sm_100a) and its CPU oracle.
 
-`python -m saplibrary_b200.build` compiles every CUDA/C++ source of
+`python saplibrary_b200/build.py` compiles every CUDA/C++ source of
 saplibrary_b200/csrc into saplibrary_b200/libsap_b200.so with nvcc, in tree,
 so the shared object travels with the repository snapshot.
 """

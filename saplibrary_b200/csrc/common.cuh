@@ -30,6 +30,9 @@ inline void cuda_check(cudaError_t e, const char* what) {
 }
 #define SAPB_CUDA(x) ::sapb::cuda_check((x), #x)
 
+// Message returned by sap_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
+
 // Number of kernels enqueued by this library (reported by the bench).
 extern std::atomic<int64_t> g_launches;
 inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }

@@ -9,7 +9,7 @@ namespace sapb {
 // y = A x for the row-major FP64 band of MVBanded (sap/spmv.h:27-74,
 // sap/device/matrix_multiply.cuh:301-350): one warp per row, coalesced
 // reads of the row's 2K+1 values.
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 k_spmv_banded(const double* __restrict__ A, const double* __restrict__ x, double* __restrict__ y, int n, int K) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -43,23 +43,24 @@ k_spmv_csr(const int* __restrict__ rp, const int* __restrict__ ci, const double*
 }
 
 // z = a*x + b*y (cusp::blas::axpby)
-__global__ void k_axpby(int n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
+static __global__ void k_axpby(int n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
                         double* __restrict__ z) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     z[i] = a * x[i] + b * y[i];
 }
 // y += a*x (cusp::blas::axpy)
-__global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
+static __global__ void k_axpy(int n, double a, const double* __restrict__ x, double* __restrict__ y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += a * x[i];
 }
 // z = b - y  (the true-residual recheck, axpby(b, APxx, rr0, 1, -1))
-__global__ void k_sub(int n, const double* __restrict__ b, const double* __restrict__ y, double* __restrict__ z) {
+static __global__ void k_sub(int n, const double* __restrict__ b, const double* __restrict__ y, double* __restrict__ z) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = b[i] - y[i];
 }
 
 // Up to 4 dot products sum_i x_q[i]*y_q[i] in one pass.  Block partials go to
-// `part`; the last block to finish reduces them in a fixed order, so the
-// result is deterministic for a given grid.
+// `part` (4 * gridDim.x doubles); the last block to finish reduces them in a
+// fixed order, so the result is deterministic for a given grid.  `counter`
+// must be zero on entry and is zero again on exit.
 struct DotArgs {
   const double* x[4];
   const double* y[4];
@@ -68,8 +69,14 @@ struct DotArgs {
 
 constexpr int kDotBlocks = 296;
 constexpr int kDotThreads = 512;
+// rows per thread of the size-proportional grid of the standalone dot entry point
+constexpr int kDotItems = 16;
+inline int dot_grid_for(long long n) {
+  long long g = (n + (long long)kDotThreads * kDotItems - 1) / ((long long)kDotThreads * kDotItems);
+  return (int)(g < 1 ? 1 : g);
+}
 
-__global__ void __launch_bounds__(kDotThreads)
+static __global__ void __launch_bounds__(kDotThreads)
 k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ counter,
        double* __restrict__ out) {
   __shared__ double red[4][kDotThreads / 32];
@@ -92,7 +99,7 @@ k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ c
     int q = threadIdx.x;
     double v = 0;
     for (int w = 0; w < kDotThreads / 32; w++) v += red[q][w];
-    part[q * kDotBlocks + blockIdx.x] = v;
+    part[q * gridDim.x + blockIdx.x] = v;
   }
   __threadfence();
   __syncthreads();
@@ -104,7 +111,7 @@ k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ c
       int q = threadIdx.x;
       volatile double* pp = part;
       double v = 0;
-      for (int b = 0; b < (int)gridDim.x; b++) v += pp[q * kDotBlocks + b];
+      for (int b = 0; b < (int)gridDim.x; b++) v += pp[q * gridDim.x + b];
       out[q] = v;
     }
     if (threadIdx.x == 0) *counter = 0u;

@@ -25,6 +25,7 @@ namespace sapb {
 
 std::atomic<int64_t> g_launches{0};
 static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 // --- live kernel profiling -----------------------------------------------------
 struct ProfState {
@@ -439,10 +440,12 @@ class PrecondT : public PrecBase {
     }
     if (spike) {
       sweep_pair(v, nullptr, Gv.get());
+      {
       SAPB_PROF("reduced_apply", st);
       k_reduced_apply<T><<<P - 1, ((K + 31) / 32) * 32, 3 * K * sizeof(T), st>>>(parts_d.get(), V.get(), W.get(), S.get(),
                                                                             offd.get(), Gv.get(), F.get(), K);
       SAPB_LAUNCHED();
+      }
       sweep_pair(nullptr, z, nullptr);
     } else {
       sweep_pair(v, z, nullptr);
@@ -920,6 +923,30 @@ int sap_spmv_apply(sap_spmv* op, const double* x, double* y) {
 }
 
 int sap_spmv_destroy(sap_spmv* op) { delete op; return SAP_OK; }
+
+int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y, double* out, void* stream) {
+  SAP_TRY({
+    SAP_REQUIRE(n >= 0 && nq >= 1 && nq <= 4 && x && y && out, "invalid dot-product arguments");
+    DotArgs a{};
+    a.nq = nq;
+    for (int q = 0; q < nq; q++) {
+      SAP_REQUIRE(x[q] && y[q], "null vector");
+      a.x[q] = x[q];
+      a.y[q] = y[q];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int grid = dot_grid_for(n);
+    double* part = nullptr;
+    unsigned int* ctr = nullptr;
+    SAPB_CUDA(cudaMallocAsync((void**)&part, sizeof(double) * 4 * (size_t)grid, st));
+    SAPB_CUDA(cudaMallocAsync((void**)&ctr, sizeof(unsigned int), st));
+    SAPB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned int), st));
+    k_dots<<<grid, kDotThreads, 0, st>>>(n, a, part, ctr, out);
+    SAPB_LAUNCHED();
+    SAPB_CUDA(cudaFreeAsync(part, st));
+    SAPB_CUDA(cudaFreeAsync(ctr, st));
+  });
+}
 
 int sap_solver_create(int P, const sap_options* opts, int prec_dtype, sap_solver** out) {
   SAP_TRY({

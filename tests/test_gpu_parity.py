@@ -209,3 +209,15 @@ def test_kernels_were_launched():
     A, s, o = setup_pair(band, n, K, 3, "double")
     apply_gpu(s, np.ones(n))
     assert sap.kernel_launch_count() > before + 10
+
+
+@pytest.mark.parametrize("n", [1, 1000, 3_000_001])
+def test_blas_dots_match_numpy(n):
+    rng = np.random.default_rng(n)
+    xs = [torch.tensor(rng.standard_normal(n), device="cuda") for _ in range(3)]
+    ys = [torch.tensor(rng.standard_normal(n), device="cuda") for _ in range(3)]
+    out = torch.empty(3, device="cuda", dtype=torch.float64)
+    sap.blas_dots(xs, ys, out)
+    torch.cuda.synchronize()
+    ref = [float(np.dot(x.cpu().numpy(), y.cpu().numpy())) for x, y in zip(xs, ys)]
+    assert np.allclose(out.cpu().numpy(), ref, rtol=1e-12, atol=1e-12)
