@@ -167,6 +167,22 @@ int sap_spmv_destroy(sap_spmv* op);
  * legacy default stream) and the call returns without waiting.  Block partial
  * sums live in scratch allocated and freed on the stream by each call. */
 int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y, double* out, void* stream);
+/* The same dot products with no allocation of any kind, for callers that
+ * cannot allocate device memory where they need the reduction (code running
+ * under another framework's caching allocator that owns the free memory,
+ * applications that budget GPU memory once at start-up, loops in which a
+ * cudaMalloc/cudaFree pair would synchronise the device).  No counterpart in
+ * the reference.  The block partial sums live in a fixed 64 KB scratch array
+ * compiled into the library, held by every GPU that loads it until exit;
+ * n is limited to 16,777,216 (larger n returns SAP_ERR_INVALID_ARGUMENT).
+ * The first call on a device looks up the scratch's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls on one device share its scratch,
+ * which keeps the last call's contents (the completion counter is cleared by
+ * each call): calls that overlap on the same GPU, for example on two
+ * streams, race on it and must be serialised by the caller. */
+int sap_blas_dots_noalloc(int n, int nq, const double* const* x, const double* const* y, double* out,
+                          void* stream);
 
 /* ---- solver --------------------------------------------------------------- */
 /* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297). */

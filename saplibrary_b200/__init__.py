@@ -113,6 +113,7 @@ _sig = {
     "sap_solver_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_solver_stream": (_vp, [_vp]),
     "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
+    "sap_blas_dots_noalloc": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_profile_select": (_i, [ctypes.c_char_p]),
     "sap_profile_read": (_i, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
 }
