@@ -218,6 +218,15 @@ int sap_solver_get_monitor(const sap_solver* s, int* code, const char** message)
 /* Number of rows, the effective half-bandwidth and partition count after
  * setup (Precond::getBandwidth / getNumPartitions, sap/precond.h:152-157). */
 int sap_solver_info(const sap_solver* s, int* n, int* k, int* num_partitions);
+/* Reordering results of a CSR setup with reordering, as int arrays:
+ * which = 0: DB row permutation (row i of A goes to row out[i]);
+ * 1: composed row permutation, input row -> band row (Precond::m_optPerm
+ *    after composition, sap/precond.h:2071-2097);
+ * 2: composed column order, band column -> input column (m_optReordering);
+ * 3: first_rows of the second-level reordering (graph.h:991-1007);
+ * 4: per-partition half-bandwidths K_p (m_ks_host).
+ * With out == NULL only *count is set. */
+int sap_solver_get_reorder(const sap_solver* s, int which, int* out, int64_t* count);
 /* The cudaStream_t all device work of this solver is enqueued on. */
 void* sap_solver_stream(const sap_solver* s);
 /* Number of kernels this library has enqueued since load (all handles). */

@@ -19,8 +19,12 @@ LIB = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "sap_oracle.cpp")
 
 
+SRC2 = os.path.join(HERE, "reorder_oracle.cpp")
+
+
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
+    newest = max(os.path.getmtime(SRC), os.path.getmtime(SRC2))
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         subprocess.run(["g++", "-O2", "-std=c++17", "-fopenmp", "-fPIC", "-shared", SRC, "-o", LIB], check=True)
     return LIB
 
@@ -134,3 +138,96 @@ def spmv_csr(rp, ci, v, x):
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+class SparseInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("nnz", ctypes.c_int), ("K", ctypes.c_int), ("P", ctypes.c_int),
+                ("k_db", ctypes.c_int), ("k_reorder", ctypes.c_int), ("varBand", ctypes.c_int),
+                ("status", ctypes.c_int), ("drop_actual", ctypes.c_double)]
+
+
+_sparse_sigs = False
+
+
+def _sparse_lib():
+    global _sparse_sigs
+    L = lib()
+    if not _sparse_sigs:
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.orc_sparse_create.restype = vp
+        L.orc_sparse_create.argtypes = [i, i, i, i, d, i, i, i]
+        L.orc_sparse_destroy.argtypes = [vp]
+        L.orc_sparse_setup.argtypes = [vp, i, vp, vp, vp, i, ctypes.c_char_p, i]
+        L.orc_sparse_info_get.argtypes = [vp, ctypes.POINTER(SparseInfo)]
+        L.orc_sparse_ints.restype = ctypes.c_longlong
+        L.orc_sparse_ints.argtypes = [vp, i, vp]
+        L.orc_sparse_reals.restype = ctypes.c_longlong
+        L.orc_sparse_reals.argtypes = [vp, i, vp]
+        L.orc_sparse_apply.argtypes = [vp, vp, vp]
+        L.orc_sparse_solve.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, d, d, ctypes.POINTER(OrcResult)]
+        _sparse_sigs = True
+    return L
+
+
+INT_NAMES = ["dbRowPerm", "optReordering", "optPerm", "secondReorder", "secondPerm", "first_rows", "ks",
+             "finalPerm", "finalReordering", "offDiagWidths_left", "offDiagWidths_right", "offDiagPerms_left",
+             "offDiagPerms_right", "ks_col", "ks_row"]
+
+
+class SparsePrecond:
+    """The oracle's sparse setup: DB + RCM + drop-off + (variable) band
+    assembly of sap/graph.h, then the variable-band SPIKE preconditioner."""
+
+    def __init__(self, P, dtype="float", doDB=True, scale=True, dropFrac=0.0, maxBandwidth=2**31 - 1,
+                 varBand=True, safe=False):
+        self.h = _sparse_lib().orc_sparse_create(int(P), 0 if dtype == "float" else 1, int(doDB), int(scale),
+                                                 float(dropFrac), int(maxBandwidth), int(varBand), int(safe))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _sparse_lib().orc_sparse_destroy(self.h)
+            self.h = None
+
+    def setup(self, rp, ci, v, factor=True):
+        self._csr = [np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
+                     np.ascontiguousarray(v, np.float64)]
+        msg = ctypes.create_string_buffer(256)
+        rc = _sparse_lib().orc_sparse_setup(self.h, self._csr[0].size - 1, *[_p(a) for a in self._csr],
+                                            int(factor), msg, 256)
+        self.message = msg.value.decode()
+        return rc
+
+    def info(self) -> SparseInfo:
+        s = SparseInfo()
+        _sparse_lib().orc_sparse_info_get(self.h, ctypes.byref(s))
+        return s
+
+    def ints(self, name: str) -> np.ndarray:
+        w = INT_NAMES.index(name)
+        cnt = _sparse_lib().orc_sparse_ints(self.h, w, None)
+        out = np.empty(cnt, np.int32)
+        if cnt:
+            _sparse_lib().orc_sparse_ints(self.h, w, _p(out))
+        return out
+
+    def reals(self, which: int) -> np.ndarray:
+        cnt = _sparse_lib().orc_sparse_reals(self.h, which, None)
+        out = np.empty(cnt, np.float64)
+        if cnt:
+            _sparse_lib().orc_sparse_reals(self.h, which, _p(out))
+        return out
+
+    def apply(self, v):
+        v = np.ascontiguousarray(v, np.float64)
+        z = np.empty_like(v)
+        _sparse_lib().orc_sparse_apply(self.h, _p(v), _p(z))
+        return z
+
+    def solve(self, b, x0=None, L=2, maxit=100, reltol=1e-6, abstol=0.0):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        res = OrcResult()
+        rp, ci, v = self._csr
+        _sparse_lib().orc_sparse_solve(self.h, b.size, _p(rp), _p(ci), _p(v), _p(b), _p(x), L, maxit, reltol,
+                                       abstol, ctypes.byref(res))
+        return x, res

@@ -1,0 +1,1150 @@
+// ORACLE — test infrastructure, NOT product code.
+//
+// CPU restatement of the reordering pipeline of SaP's sparse setup
+// (sap/graph.h; the Graph class): DB matching and scaling, RCM, drop-off,
+// off-diagonal assembly, second-level (per-partition) RCM and the
+// variable-band assembly, in the reference's operation order, so that
+// permutations, bandwidths and partition data come out bit-identical.
+// Heaps are std::priority_queue with the reference's comparator, which
+// replays its tie order.  Used only by tests/ and bench.py's CPU leg.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdio>
+#include <cstdlib>
+#include <ctime>
+#include <limits>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace orc {
+
+static const double LOC_INF = 1e37;  // Graph<T>::LOC_INFINITY (graph.h:287-288)
+
+struct DBError : std::runtime_error {
+  int code;
+  DBError(int c, const char* m) : std::runtime_error(m), code(c) {}
+};
+
+// Graph<T> state (sap/graph.h:227-276)
+template <typename T>
+struct Graph {
+  int n = 0, nnz = 0;
+  std::vector<int> rp, ci;  // m_matrix (CSR)
+  std::vector<T> val;
+  std::vector<int> drp, dci;  // m_matrix_diagonal (CSR)
+  std::vector<T> dval;
+  std::vector<char> exists;  // m_exists
+  // DB persistent work arrays (graph.h:500-503)
+  std::vector<int> DB_B;
+  std::vector<char> DB_inB, DB_visited;
+  std::vector<double> DB_d;
+  std::vector<int> buffer_reordering;
+};
+
+struct DijkstraCmp {  // CompareValue<double> (graph.h:385-389)
+  bool operator()(const std::pair<int, double>& a, const std::pair<int, double>& b) const {
+    return a.second > b.second;
+  }
+};
+struct DegreeCmp {  // CompareValue<int>
+  bool operator()(const std::pair<int, int>& a, const std::pair<int, int>& b) const { return a.second > b.second; }
+};
+
+// find_shortest_aug_path (graph.h:2043-2173)
+template <typename T>
+static bool find_shortest_aug_path(Graph<T>& g, int init_node, std::vector<char>& matched,
+                                   std::vector<char>& rev_matched, std::vector<int>& match_nodes,
+                                   std::vector<int>& rev_match_nodes, const std::vector<int>& row_ptr,
+                                   const std::vector<int>& rows, std::vector<int>& prev, std::vector<double>& u_val,
+                                   std::vector<double>& v_val, const std::vector<double>& c_val,
+                                   std::vector<int>& irn) {
+  bool success = false;
+  int b_cnt = 0;
+  std::priority_queue<std::pair<int, double>, std::vector<std::pair<int, double>>, DijkstraCmp> Q;
+  double lsp = 0.0, lsap = LOC_INF;
+  int cur_node = init_node;
+  int isap = -1, ksap = -1;
+  prev[init_node] = -1;
+  while (true) {
+    int start_cur = row_ptr[cur_node], end_cur = row_ptr[cur_node + 1];
+    for (int i = start_cur; i < end_cur; i++) {
+      int cur_row = rows[i];
+      if (g.DB_inB[cur_row]) continue;
+      if (c_val[i] > LOC_INF / 2.0) continue;
+      double reduced_cval = c_val[i] - u_val[cur_row] - v_val[cur_node];
+      if (reduced_cval + 1e-10 < 0) throw DBError(-2, "Negative reduced weight in DB.");
+      double d_new = lsp + reduced_cval;
+      if (d_new < lsap) {
+        if (!matched[cur_row]) {
+          lsap = d_new;
+          isap = cur_row;
+          ksap = i;
+          match_nodes[isap] = cur_node;
+        } else if (d_new < g.DB_d[cur_row]) {
+          g.DB_d[cur_row] = d_new;
+          prev[match_nodes[cur_row]] = cur_node;
+          Q.push(std::make_pair(cur_row, d_new));
+          irn[cur_row] = i;
+        }
+      }
+    }
+    std::pair<int, double> min_d;
+    bool found = false;
+    while (!Q.empty()) {
+      min_d = Q.top();
+      Q.pop();
+      if (g.DB_visited[min_d.first]) continue;
+      found = true;
+      break;
+    }
+    if (!found) break;
+    int tmp_idx = min_d.first;
+    g.DB_visited[tmp_idx] = true;
+    lsp = min_d.second;
+    if (lsap <= lsp) {
+      g.DB_visited[tmp_idx] = false;
+      g.DB_d[tmp_idx] = LOC_INF;
+      break;
+    }
+    g.DB_inB[tmp_idx] = true;
+    g.DB_B[b_cnt++] = tmp_idx;
+    cur_node = match_nodes[tmp_idx];
+  }
+  if (lsap < LOC_INF / 2.0) {
+    matched[isap] = true;
+    cur_node = match_nodes[isap];
+    v_val[cur_node] = c_val[ksap];
+    while (prev[cur_node] >= 0) {
+      match_nodes[isap] = cur_node;
+      int next_ksap = rev_match_nodes[cur_node];
+      int next_isap = rows[next_ksap];
+      next_ksap = irn[next_isap];
+      rev_match_nodes[cur_node] = ksap;
+      cur_node = prev[cur_node];
+      isap = next_isap;
+      ksap = next_ksap;
+    }
+    match_nodes[isap] = cur_node;
+    rev_match_nodes[cur_node] = ksap;
+    rev_matched[cur_node] = true;
+    success = true;
+    for (int i = 0; i < b_cnt; i++) {
+      int tmp_row = g.DB_B[i];
+      int j_val = match_nodes[tmp_row];
+      int tmp_k = rev_match_nodes[j_val];
+      u_val[tmp_row] += g.DB_d[tmp_row] - lsap;
+      v_val[j_val] = c_val[tmp_k] - u_val[tmp_row];
+      g.DB_d[tmp_row] = LOC_INF;
+      g.DB_visited[tmp_row] = false;
+      g.DB_inB[tmp_row] = false;
+    }
+    while (!Q.empty()) {
+      auto t = Q.top();
+      Q.pop();
+      g.DB_d[t.first] = LOC_INF;
+    }
+  }
+  return success;
+}
+
+// DB (graph.h:1214-1361) with get_csc_matrix (1827-1857) and the full
+// (not first-stage-only) init_reduced_cval (1875-2035).  `A*` is the input
+// CSR in PrecValueType (the reference converts to it first, precond.h:1667).
+// Outputs: dbRowPerm (row i of A goes to row dbRowPerm[i]), row/column
+// scales (double), and the permuted, scaled matrix in g.rp/ci/val.
+template <typename T>
+static void DB(Graph<T>& g, const std::vector<int>& Arp, const std::vector<int>& Aci, const std::vector<T>& Aval,
+               bool scale, std::vector<int>& dbRowPerm, std::vector<double>& rowScale, std::vector<double>& colScale) {
+  const int n = g.n, nnz = g.nnz;
+  g.DB_inB.assign(n, 0);
+  g.DB_B.assign(n, 0);
+  g.DB_d.assign(n, LOC_INF);
+  g.DB_visited.assign(n, 0);
+  // get_csc_matrix: c = |a|, row maxima, c = log(max / |a|)
+  std::vector<double> c_val(nnz), max_val(n, 0.0);
+  for (int i = 0; i < n; i++) {
+    double m = 0;
+    bool first = true;
+    for (int l = Arp[i]; l < Arp[i + 1]; l++) {
+      double a = std::fabs((double)Aval[l]);
+      c_val[l] = a;
+      m = first ? a : std::max(m, a);
+      first = false;
+    }
+    max_val[i] = m;
+  }
+  for (int i = 0; i < n; i++)
+    for (int l = Arp[i]; l < Arp[i + 1]; l++) c_val[l] = std::log(max_val[i] / c_val[l]);
+  // init_reduced_cval
+  std::vector<double>& u_val = colScale;
+  std::vector<double>& v_val = rowScale;
+  u_val.assign(n, 0.0);
+  v_val.assign(n, LOC_INF);
+  std::vector<int> match_nodes(n, 0), rev_match_nodes(nnz, 0);
+  std::vector<char> matched(n, 0), rev_matched(n, 0);
+  for (int i = 0; i < n; i++) {  // reduce_by_key(min) over the CSR rows
+    double m = 0;
+    bool first = true;
+    for (int l = Arp[i]; l < Arp[i + 1]; l++) {
+      m = first ? c_val[l] : std::min(m, c_val[l]);
+      first = false;
+    }
+    u_val[i] = m;
+  }
+  for (int i = 0; i < n; i++) {
+    int min_idx = -1;
+    for (int j = Arp[i]; j < Arp[i + 1]; j++) {
+      if (c_val[j] > LOC_INF / 2.0) continue;
+      int row = Aci[j];
+      double tmp_val = c_val[j] - u_val[row];
+      if (v_val[i] > tmp_val) {
+        v_val[i] = tmp_val;
+        min_idx = j;
+      }
+    }
+    if (min_idx >= 0) {
+      int tmp_row = Aci[min_idx];
+      if (!matched[tmp_row]) {
+        rev_matched[i] = true;
+        matched[tmp_row] = true;
+        match_nodes[tmp_row] = i;
+        rev_match_nodes[i] = min_idx;
+      }
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    if (!matched[i]) u_val[i] = 0.0;
+    if (!rev_matched[i]) v_val[i] = 0.0;
+  }
+  // augmenting paths
+  std::vector<int> irn(n), prev(n);
+  for (int i = 0; i < n; i++) {
+    if (rev_matched[i]) continue;
+    find_shortest_aug_path(g, i, matched, rev_matched, match_nodes, rev_match_nodes, Arp, Aci, prev, u_val, v_val,
+                           c_val, irn);
+  }
+  for (int i = 0; i < n; i++)
+    if (!matched[i]) throw DBError(-5, "Singular matrix found");
+  for (int i = 0; i < n; i++) colScale[i] = std::exp(u_val[i]);
+  for (int i = 0; i < n; i++) rowScale[i] = std::exp(v_val[i]) / max_val[i];
+  dbRowPerm.assign(n, 0);
+  for (int k = 0; k < n; k++) dbRowPerm[match_nodes[k]] = k;
+  // permute and scale rows, stable counting sort by the new row
+  std::vector<int> row_idx(nnz);
+  std::vector<T> sv(nnz);
+  for (int i = 0; i < n; i++) {
+    int nr = dbRowPerm[i];
+    for (int l = Arp[i]; l < Arp[i + 1]; l++) {
+      row_idx[l] = nr;
+      if (scale) {
+        T f = (T)(rowScale[i] * colScale[Aci[l]]);
+        sv[l] = f * Aval[l];
+      } else {
+        sv[l] = Aval[l];
+      }
+    }
+  }
+  g.rp.assign(n + 1, 0);
+  g.ci.assign(nnz, 0);
+  g.val.assign(nnz, T(0));
+  for (int l = 0; l < nnz; l++) g.rp[row_idx[l]]++;
+  for (int i = 1; i <= n; i++) g.rp[i] += g.rp[i - 1];  // inclusive scan (rp[n] stays 0 + ...)
+  for (int l = nnz - 1; l >= 0; l--) {
+    int idx = --g.rp[row_idx[l]];
+    g.ci[idx] = Aci[l];
+    g.val[idx] = sv[l];
+  }
+  g.rp[n] = nnz;
+}
+
+// buildTopology (graph.h:1764-1809): symmetrised adjacency of the edges
+// [e0, e1) without self loops (duplicates kept), rows [nb, ne) counted into
+// the n+1 vector `ro` with a stable counting sort from the end.
+static void build_topology(const std::vector<int>& er, const std::vector<int>& ec, int e0, int e1, int nb, int ne,
+                           int n, std::vector<int>& ro, std::vector<int>& adj) {
+  ro.assign(n + 1, 0);
+  std::vector<int> rows;
+  rows.reserve(2 * (size_t)(e1 - e0));
+  adj.clear();
+  adj.reserve(2 * (size_t)(e1 - e0));
+  for (int e = e0; e < e1; e++) {
+    int from = er[e], to = ec[e];
+    if (from != to) {
+      rows.push_back(from); adj.push_back(to);
+      rows.push_back(to); adj.push_back(from);
+    }
+  }
+  const int cnt = (int)rows.size();
+  for (int i = 0; i < cnt; i++) ro[rows[i]]++;
+  for (int i = nb + 1; i <= ne; i++) ro[i] += ro[i - 1];  // inclusive scan over [nb, ne]
+  std::vector<int> tmp(cnt);
+  for (int i = cnt - 1; i >= 0; i--) tmp[--ro[rows[i]]] = adj[i];
+  adj.swap(tmp);
+}
+
+// RCM (graph.h:1371-1584), including its quirks: `max_level` is never
+// updated, so at most two trials run; the start node of a later trial uses
+// the degrees of vertices 0..count-1 (graph.h:1440-1443); BFS levels of
+// restart nodes are not reset.  Permutes g's CSR symmetrically (stable
+// counting sort) and returns the half-bandwidth.
+template <typename T>
+static int RCM(Graph<T>& g, std::vector<int>& optReordering, std::vector<int>& optPerm) {
+  const int n = g.n, nnz = g.nnz;
+  optReordering.resize(n);
+  optPerm.assign(n, 0);
+  std::vector<int> tmp_reordering(n);
+  for (int i = 0; i < n; i++) optReordering[i] = i;
+  std::vector<int> row_idx(nnz), ori_degrees(n);
+  for (int i = 0; i < n; i++) {
+    for (int l = g.rp[i]; l < g.rp[i + 1]; l++) row_idx[l] = i;
+    ori_degrees[i] = g.rp[i + 1] - g.rp[i];
+  }
+  int bandwidth = 0;
+  for (int l = 0; l < nnz; l++) bandwidth = std::max(bandwidth, std::abs(row_idx[l] - g.ci[l]));
+  std::vector<int> ro, adj;
+  build_topology(row_idx, g.ci, 0, nnz, 0, n, n, ro, adj);
+  const int MAX_NUM_TRIAL = 5, BANDWIDTH_THRESHOLD = 256;
+  std::vector<char> tried(n, 0);
+  std::vector<int> pushed(n, -1), levels(n, 0);
+  int max_level = 0, p_max_level = 0;
+  for (int trial = 0; trial < MAX_NUM_TRIAL; trial++) {
+    std::queue<int> q;
+    std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, DegreeCmp> pq;
+    int tmp_node;
+    int left_cnt = n, j = 0, last = 0;
+    if (trial > 0) {
+      int max_pos = (int)(std::max_element(levels.begin(), levels.end()) - levels.begin());
+      int max_count = (int)std::count(levels.begin(), levels.end(), max_level);
+      if (max_count > 1) {
+        std::vector<int> verts;
+        verts.reserve(max_count);
+        for (int i = 0; i < n; i++)
+          if (levels[i] == max_level) verts.push_back(i);
+        int pos = (int)(std::min_element(ori_degrees.begin(), ori_degrees.begin() + max_count) - ori_degrees.begin());
+        tmp_node = verts[pos];
+      } else {
+        tmp_node = max_pos;
+      }
+      while (tried[tmp_node]) tmp_node = (tmp_node + 1) % n;
+    } else {
+      tmp_node = (int)(std::min_element(ori_degrees.begin(), ori_degrees.end()) - ori_degrees.begin());
+    }
+    tried[tmp_node] = 1;
+    levels[tmp_node] = 0;
+    pushed[tmp_node] = trial;
+    q.push(tmp_node);
+    while (left_cnt--) {
+      if (q.empty()) {
+        left_cnt++;
+        int i;
+        for (i = last; i < n; i++) {
+          if (pushed[i] != trial) {
+            q.push(i);
+            pushed[i] = trial;
+            last = i;
+            break;
+          }
+        }
+        if (i < n) continue;
+        return -1;
+      }
+      tmp_node = q.front();
+      tmp_reordering[j++] = tmp_node;
+      q.pop();
+      int local_level = levels[tmp_node];
+      for (int i = ro[tmp_node]; i < ro[tmp_node + 1]; i++) {
+        int t = adj[i];
+        if (pushed[t] != trial) {
+          pushed[t] = trial;
+          pq.push(std::make_pair(t, ori_degrees[t]));
+          levels[t] = local_level + 1;
+        }
+      }
+      while (!pq.empty()) {
+        q.push(pq.top().first);
+        pq.pop();
+      }
+    }
+    for (int k = 0; k < n; k++) optPerm[tmp_reordering[k]] = k;
+    int tmp_bw = 0;
+    for (int l = 0; l < nnz; l++) tmp_bw = std::max(tmp_bw, std::abs(optPerm[row_idx[l]] - optPerm[g.ci[l]]));
+    if (bandwidth > tmp_bw) {
+      bandwidth = tmp_bw;
+      optReordering = tmp_reordering;
+    }
+    if (trial > 0) {
+      if (p_max_level >= max_level) break;
+      double ratio = 1.0 * (max_level - p_max_level) / p_max_level;
+      if (ratio < 0.01) break;
+      p_max_level = max_level;
+    } else {
+      p_max_level = max_level;
+    }
+    if (bandwidth <= BANDWIDTH_THRESHOLD) break;
+  }
+  for (int k = 0; k < n; k++) optPerm[optReordering[k]] = k;
+  // symmetric permutation and stable CSR rebuild
+  std::vector<int> nr(nnz), nc(nnz);
+  for (int l = 0; l < nnz; l++) { nr[l] = optPerm[row_idx[l]]; nc[l] = optPerm[g.ci[l]]; }
+  std::vector<int> rp(n + 1, 0), ci(nnz);
+  std::vector<T> val(nnz);
+  for (int l = 0; l < nnz; l++) rp[nr[l]]++;
+  for (int i = 1; i <= n; i++) rp[i] += rp[i - 1];
+  for (int l = nnz - 1; l >= 0; l--) {
+    int idx = --rp[nr[l]];
+    ci[idx] = nc[l];
+    val[idx] = g.val[l];
+  }
+  rp[n] = nnz;
+  g.rp.swap(rp);
+  g.ci.swap(ci);
+  g.val.swap(val);
+  return bandwidth;
+}
+
+// dropOff (graph.h:598-747): entries bucketed by |i-j| (stable), bands
+// removed from the outside while the remaining sum of squares (in T, summed
+// sequentially) stays >= (1-frac) * total.  Returns the reference's K: the
+// distance of the last band removed (or of the outermost band if none is).
+template <typename T>
+static int dropOff(Graph<T>& g, T frac, int maxBandwidth, T& frac_actual) {
+  const int n = g.n;
+  int nnz = g.nnz;
+  std::vector<int> bucket(n, 0);
+  for (int i = 0; i < n; i++)
+    for (int l = g.rp[i]; l < g.rp[i + 1]; l++) bucket[std::abs(i - g.ci[l])]++;
+  {
+    int acc = 0;
+    for (int d = 0; d < n; d++) { int c = bucket[d]; bucket[d] = acc; acc += c; }
+  }
+  std::vector<int> cr(nnz), cc(nnz);
+  std::vector<T> cv(nnz);
+  for (int i = 0; i < n; i++)
+    for (int l = g.rp[i]; l < g.rp[i + 1]; l++) {
+      int idx = bucket[std::abs(i - g.ci[l])]++;
+      cr[idx] = i; cc[idx] = g.ci[l]; cv[idx] = g.val[l];
+    }
+  T norm_in = T(0);
+  for (int l = 0; l < nnz; l++) norm_in = norm_in + g.val[l] * g.val[l];
+  T min_norm_out = (T(1) - frac) * norm_in;
+  T norm_out = norm_in;
+  auto band = [&](int rev_pos) { int idx = nnz - 1 - rev_pos; return std::abs(cr[idx] - cc[idx]); };
+  auto sq = [&](int rev_pos) { int idx = nnz - 1 - rev_pos; return cv[idx] * cv[idx]; };
+  int first = 0, last = 0;
+  int final_k = band(0);
+  {
+    int bw;
+    while ((bw = band(last)) > maxBandwidth) last++;
+    T s = T(0);
+    for (int p = first; p < last; p++) s = s + sq(p);
+    norm_out -= s;
+    first = last;
+    final_k = bw;
+  }
+  if (norm_out >= min_norm_out) {
+    while (true) {
+      int bw = band(first);
+      if (bw == 0) { final_k = 0; break; }
+      do { last++; } while (band(last) == bw);
+      T band_norm = T(0);
+      for (int p = first; p < last; p++) band_norm = band_norm + sq(p);
+      if (norm_out - band_norm < min_norm_out) break;
+      norm_out -= band_norm;
+      first = last;
+      final_k = bw;
+    }
+  }
+  frac_actual = T(1) - norm_out / norm_in;
+  nnz -= first;
+  // rebuild: stable counting sort by column, then (stable, from the end) by row
+  std::fill(bucket.begin(), bucket.end(), 0);
+  for (int l = 0; l < nnz; l++) bucket[cc[l]]++;
+  {
+    int acc = 0;
+    for (int d = 0; d < n; d++) { int c = bucket[d]; bucket[d] = acc; acc += c; }
+  }
+  std::vector<int> tr(nnz), tc(nnz);
+  std::vector<T> tv(nnz);
+  for (int l = 0; l < nnz; l++) {
+    int idx = bucket[cc[l]]++;
+    tr[idx] = cr[l]; tc[idx] = cc[l]; tv[idx] = cv[l];
+  }
+  std::fill(bucket.begin(), bucket.end(), 0);
+  for (int l = 0; l < nnz; l++) bucket[tr[l]]++;
+  for (int d = 1; d < n; d++) bucket[d] += bucket[d - 1];
+  std::vector<int> rr(nnz), rc(nnz);
+  std::vector<T> rv(nnz);
+  for (int l = nnz - 1; l >= 0; l--) {
+    int idx = --bucket[tr[l]];
+    rr[idx] = tr[l]; rc[idx] = tc[l]; rv[idx] = tv[l];
+  }
+  g.rp.assign(n + 1, 0);
+  for (int l = 0; l < nnz; l++) g.rp[rr[l] + 1]++;
+  for (int i = 0; i < n; i++) g.rp[i + 1] += g.rp[i];
+  g.ci.swap(rc);
+  g.val.swap(rv);
+  g.nnz = nnz;
+  return final_k;
+}
+
+// Partition of a row (graph.h:780-786): the first n%P partitions hold n/P+1 rows.
+static inline int part_of(int r, int q, int rem) {
+  int p = r / (q + 1);
+  if (p >= rem) p = rem + (r - rem * (q + 1)) / q;
+  return p;
+}
+
+// assembleOffDiagMatrices (graph.h:756-898): diagonal-block entries go to the
+// diagonal matrix (CSR order kept); coupling entries to offDiags (row-major
+// K x K per block) and WV (column-major, columns compressed in first-seen
+// order: offDiagPerms / offDiagWidths).
+template <typename T>
+static void assembleOffDiag(Graph<T>& g, int K, int P, std::vector<T>& WV, std::vector<T>& offd,
+                            std::vector<int>& wl, std::vector<int>& wr, std::vector<int>& permL,
+                            std::vector<int>& permR) {
+  const int n = g.n;
+  const size_t KK = (size_t)K * K;
+  WV.assign(2 * KK * (P - 1), T(0));
+  offd.assign(2 * KK * (P - 1), T(0));
+  wl.assign(P - 1, 0);
+  wr.assign(P - 1, 0);
+  permL.assign((size_t)(P - 1) * K, -1);
+  permR.assign((size_t)(P - 1) * K, -1);
+  std::vector<int> reordL((size_t)(P - 1) * K, -1), reordR((size_t)(P - 1) * K, -1);
+  const int q = n / P, rem = n % P;
+  g.exists.assign(n, 0);
+  std::vector<int> dr, dc;
+  std::vector<T> dv;
+  dr.reserve(g.nnz); dc.reserve(g.nnz); dv.reserve(g.nnz);
+  for (int j = 0; j < n; j++) {
+    for (int it = g.rp[j]; it < g.rp[j + 1]; it++) {
+      int l = g.ci[it];
+      int pc = part_of(l, q, rem), pr = part_of(j, q, rem);
+      if (pc == pr) {
+        dr.push_back(j); dc.push_back(l); dv.push_back(g.val[it]);
+      } else if (pc > pr) {  // V/B block
+        g.exists[j] = 1;
+        int partEndRow = q * pr + (pr < rem ? pr + q + 1 : rem + q);
+        int partStartCol = q * pc + (pc < rem ? pc : rem);
+        size_t key = (size_t)pr * K + (l - partStartCol);
+        if (reordR[key] < 0) {
+          reordR[key] = wr[pr];
+          permR[(size_t)pr * K + wr[pr]] = l - partStartCol;
+          wr[pr]++;
+        }
+        offd[pr * 2 * KK + (size_t)(j + K - partEndRow) * K + (l - partStartCol)] = g.val[it];
+        WV[pr * 2 * KK + (j + K - partEndRow) + (size_t)reordR[key] * K] = g.val[it];
+      } else {  // W/C block
+        int partStartRow = q * pr + (pr < rem ? pr : rem);
+        int partEndCol = q * pc + (pc < rem ? pc + q + 1 : rem + q);
+        size_t key = (size_t)(pr - 1) * K + (l - partEndCol + K);
+        if (reordL[key] < 0) {
+          reordL[key] = K - 1 - wl[pr - 1];
+          permL[(size_t)(pr - 1) * K + K - 1 - wl[pr - 1]] = l - partEndCol + K;
+          wl[pr - 1]++;
+        }
+        offd[(pc * 2 + 1) * KK + (size_t)(j - partStartRow) * K + (l - partEndCol + K)] = g.val[it];
+        WV[(pc * 2 + 1) * KK + (j - partStartRow) + (size_t)reordL[key] * K] = g.val[it];
+      }
+    }
+  }
+  // COO (row-sorted) -> CSR
+  g.drp.assign(n + 1, 0);
+  for (int r : dr) g.drp[r + 1]++;
+  for (int i = 0; i < n; i++) g.drp[i + 1] += g.drp[i];
+  g.dci.swap(dc);
+  g.dval.swap(dv);
+}
+
+// partitionedRCM (graph.h:1593-1757) on the diagonal matrix's edges
+// [e0, e1) and nodes [nb, ne).  Quirks kept: BFS priority is the symmetrised
+// topology degree, the start node uses the CSR row lengths, a later trial's
+// start uses the degrees of the partition's first `count` nodes, and
+// max_level is the level of the last node assigned.
+template <typename T>
+static void partitionedRCM(Graph<T>& g, int e0, int e1, int nb, int ne, std::vector<int>& optReordering,
+                           std::vector<int>& optPerm, const std::vector<int>& row_idx) {
+  const int n = g.n;
+  for (int i = nb; i < ne; i++) optReordering[i] = i;
+  int opt_bw = 0;
+  for (int e = e0; e < e1; e++) opt_bw = std::max(opt_bw, std::abs(row_idx[e] - g.dci[e]));
+  std::vector<int> ro, adj;
+  build_topology(row_idx, g.dci, e0, e1, nb, ne, n, ro, adj);
+  const int MAX_NUM_TRIAL = 5, BANDWIDTH_THRESHOLD = 128;
+  std::vector<char> tried(n, 0);
+  std::vector<int> pushed(ne, -1), levels(n, 0);
+  std::vector<int> ori_degrees(ne - nb);
+  for (int i = nb; i < ne; i++) ori_degrees[i - nb] = g.drp[i + 1] - g.drp[i];
+  int max_level = 0, p_max_level = 0;  // the reference leaves these uninitialised
+  std::vector<int>& buf = g.buffer_reordering;
+  for (int trial = 0; trial < MAX_NUM_TRIAL; trial++) {
+    std::queue<int> q;
+    std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, DegreeCmp> pq;
+    int tmp_node;
+    if (trial > 0) {
+      int max_pos = (int)(std::max_element(levels.begin() + nb, levels.begin() + ne) - levels.begin());
+      int max_count = (int)std::count(levels.begin() + nb, levels.begin() + ne, max_level);
+      if (max_count > 1) {
+        std::vector<int> verts;
+        for (int i = nb; i < ne; i++)
+          if (levels[i] == max_level) verts.push_back(i);
+        int pos = (int)(std::min_element(ori_degrees.begin(), ori_degrees.begin() + max_count) - ori_degrees.begin());
+        tmp_node = verts[pos];
+      } else {
+        tmp_node = max_pos;
+      }
+      while (tried[tmp_node]) tmp_node = (tmp_node + 1) % n;
+    } else {
+      tmp_node = (int)(std::min_element(ori_degrees.begin(), ori_degrees.end()) - ori_degrees.begin()) + nb;
+    }
+    tried[tmp_node] = 1;
+    levels[tmp_node] = 0;
+    pushed[tmp_node] = trial;
+    q.push(tmp_node);
+    int left_cnt = ne - nb, j = nb, last = nb;
+    while (left_cnt--) {
+      if (q.empty()) {
+        left_cnt++;
+        int i;
+        for (i = last; i < ne; i++) {
+          if (pushed[i] != trial) {
+            q.push(i);
+            pushed[i] = trial;
+            last = i;
+            break;
+          }
+        }
+        if (i < ne) continue;
+        return;
+      }
+      tmp_node = q.front();
+      buf[j++] = tmp_node;
+      q.pop();
+      for (int i = ro[tmp_node]; i < ro[tmp_node + 1]; i++) {
+        int t = adj[i];
+        if (pushed[t] != trial) {
+          pushed[t] = trial;
+          pq.push(std::make_pair(t, ro[t + 1] - ro[t]));
+          max_level = levels[t] = levels[tmp_node] + 1;
+        }
+      }
+      while (!pq.empty()) {
+        q.push(pq.top().first);
+        pq.pop();
+      }
+    }
+    for (int k = nb; k < ne; k++) optPerm[buf[k]] = k;
+    int tmp_bw = 0;
+    for (int e = e0; e < e1; e++) tmp_bw = std::max(tmp_bw, std::abs(optPerm[row_idx[e]] - optPerm[g.dci[e]]));
+    if (opt_bw > tmp_bw) {
+      opt_bw = tmp_bw;
+      std::copy(buf.begin() + nb, buf.begin() + ne, optReordering.begin() + nb);
+    }
+    if (trial > 0) {
+      if (p_max_level >= max_level) break;
+      double ratio = 1.0 * (max_level - p_max_level) / p_max_level;
+      if (ratio < 0.01) break;
+      p_max_level = max_level;
+    } else {
+      p_max_level = max_level;
+    }
+    if (opt_bw <= BANDWIDTH_THRESHOLD) break;
+  }
+  for (int k = nb; k < ne; k++) optPerm[optReordering[k]] = k;
+}
+
+// secondLevelReordering (graph.h:908-1008)
+template <typename T>
+static void secondLevelReordering(Graph<T>& g, int K, int P, std::vector<int>& secondReorder,
+                                  std::vector<int>& secondPerm, std::vector<int>& first_rows) {
+  const int n = g.n, q = n / P, rem = n % P;
+  secondReorder.assign(n, 0);
+  secondPerm.assign(n, 0);
+  g.buffer_reordering.assign(n, 0);
+  const int dnnz = (int)g.dci.size();
+  std::vector<int> row_idx(dnnz);
+  for (int i = 0; i < n; i++)
+    for (int l = g.drp[i]; l < g.drp[i + 1]; l++) row_idx[l] = i;
+  int nb = 0, e0 = 0;
+  for (int p = 0; p < P; p++) {
+    int ne = nb + q + (p < rem ? 1 : 0);
+    int e1 = g.drp[ne];
+    partitionedRCM(g, e0, e1, nb, ne, secondReorder, secondPerm, row_idx);
+    nb = ne;
+    e0 = e1;
+  }
+  // permute the diagonal matrix, stable CSR rebuild
+  std::vector<int> nr(dnnz), nc(dnnz);
+  for (int l = 0; l < dnnz; l++) { nr[l] = secondPerm[row_idx[l]]; nc[l] = secondPerm[g.dci[l]]; }
+  std::vector<int> rp(n + 1, 0), ci(dnnz);
+  std::vector<T> val(dnnz);
+  for (int l = 0; l < dnnz; l++) rp[nr[l]]++;
+  for (int i = 1; i <= n; i++) rp[i] += rp[i - 1];
+  for (int l = dnnz - 1; l >= 0; l--) {
+    int idx = --rp[nr[l]];
+    ci[idx] = nc[l];
+    val[idx] = g.dval[l];
+  }
+  rp[n] = dnnz;
+  g.drp.swap(rp);
+  g.dci.swap(ci);
+  g.dval.swap(val);
+  first_rows.assign(std::max(P - 1, 0), 0);
+  int last_row = 0;
+  for (int i = 0; i < P - 1; i++) {
+    last_row += q + (i < rem ? 1 : 0);
+    first_rows[i] = last_row;
+    for (int j = last_row - K; j < last_row; j++)
+      if (g.exists[j] && first_rows[i] > secondPerm[j]) first_rows[i] = secondPerm[j];
+  }
+}
+
+// assembleBandedMatrix, variable bandwidth (graph.h:1093-1206): K_p per
+// partition, band offsets, and the diagonal-block COO entries.
+template <typename T>
+static void assembleBandedVar(const Graph<T>& g, int P, std::vector<int>& ks, std::vector<long long>& boff,
+                              std::vector<int>& ks_col, std::vector<int>& ks_row) {
+  const int n = g.n, q = n / P, rem = n % P;
+  ks.assign(P, 0);
+  boff.assign(P + 1, 0);
+  for (int j = 0; j < n; j++)
+    for (int it = g.drp[j]; it < g.drp[j + 1]; it++) {
+      int l = g.dci[it];
+      int p = part_of(l, q, rem);
+      ks[p] = std::max(ks[p], std::abs(l - j));
+    }
+  for (int p = 0; p < P; p++) boff[p + 1] = boff[p] + (long long)(q + (p < rem ? 1 : 0)) * (2 * ks[p] + 1);
+  ks_col.assign(n, 0);
+  ks_row.assign(n, 0);
+  for (int j = 0; j < n; j++)
+    for (int it = g.drp[j]; it < g.drp[j + 1]; it++) {
+      int l = g.dci[it];
+      ks_col[l] = std::max(ks_col[l], j - l);
+      ks_row[j] = std::max(ks_row[j], l - j);
+    }
+  int pb = 0, pe = q;
+  for (int i = 0; i < P; i++) {
+    if (i < rem) pe++;
+    for (int j = pb + 1; j < pe; j++) {
+      if (ks_col[j] < ks_col[j - 1] - 1) ks_col[j] = ks_col[j - 1] - 1;
+      if (ks_col[j] > pe - j - 1) ks_col[j] = pe - j - 1;
+      if (ks_row[j] < ks_row[j - 1] - 1) ks_row[j] = ks_row[j - 1] - 1;
+      if (ks_row[j] > pe - j - 1) ks_row[j] = pe - j - 1;
+    }
+    pb = pe;
+    pe = pb + q;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse setup (transformToBandedMatrix, sap/precond.h:1656-2101) and the
+// variable-band preconditioner built on it (LU_only is forced with a
+// variable band, driver_test.cu:832-833).
+template <typename T>
+struct SparsePrecond {
+  // options
+  int P_req = 1;
+  bool doDB = true, scale = true, varBand = true, safe = false;
+  double dropFrac = 0;
+  int maxBandwidth = std::numeric_limits<int>::max();
+  // results of the reorder pipeline
+  int n = 0, nnz = 0, K = 0, P = 1, k_db = 0, k_reorder = 0;
+  T drop_actual = T(0);
+  std::vector<int> dbRowPerm, optReordering, optPerm, secondReorder, secondPerm, first_rows;
+  std::vector<double> rowScaleD, colScaleD;
+  std::vector<T> rowScale, colScale;             // stored in PrecValueType (precond.h:1737)
+  std::vector<int> finalPerm, finalReordering;   // m_optPerm / m_optReordering after composition
+  std::vector<int> wl, wr, permL, permR, ks, ks_col, ks_row;
+  std::vector<long long> boff;
+  std::vector<T> WV, offd, B;                    // B: variable band (second-level order), factors after setup
+  std::vector<T> V, W, S;
+  std::vector<int> pstart, psize;
+  int status = 0;
+  std::string msg;
+
+  T& at(int p, int i, int j) {  // element (i, j) of partition p's band, global row/col indices
+    return B[boff[p] + (long long)(j - pstart[p]) * (2 * ks[p] + 1) + ks[p] + (i - j)];
+  }
+};
+
+static double wall() { timespec t; clock_gettime(CLOCK_MONOTONIC, &t); return t.tv_sec + 1e-9 * t.tv_nsec; }
+#define ORC_STAGE(name) do { if (getenv("ORC_TIMING")) fprintf(stderr, "[oracle] %-24s %8.3f s\n", name, wall() - t_stage); t_stage = wall(); } while (0)
+
+template <typename T>
+static void sparse_reorder(SparsePrecond<T>& sp, int n, const int* rp, const int* ci, const double* v) {
+  double t_stage = wall();
+  // CSR in PrecValueType with explicit zeros dropped (precond.h:1667-1713)
+  std::vector<int> Arp(n + 1, 0), Aci;
+  std::vector<T> Aval;
+  Aci.reserve(rp[n]);
+  Aval.reserve(rp[n]);
+  for (int i = 0; i < n; i++) {
+    for (int p = rp[i]; p < rp[i + 1]; p++) {
+      T a = (T)v[p];
+      if (a != T(0)) { Aci.push_back(ci[p]); Aval.push_back(a); }
+    }
+    Arp[i + 1] = (int)Aci.size();
+  }
+  Graph<T> g;
+  g.n = n;
+  g.nnz = (int)Aci.size();
+  sp.n = n;
+  if (sp.doDB) {
+    DB(g, Arp, Aci, Aval, sp.scale, sp.dbRowPerm, sp.rowScaleD, sp.colScaleD);
+  } else {
+    g.rp = Arp; g.ci = Aci; g.val = Aval;
+    sp.dbRowPerm.resize(n);
+    for (int i = 0; i < n; i++) sp.dbRowPerm[i] = i;
+    sp.rowScaleD.assign(n, 1.0);
+    sp.colScaleD.assign(n, 1.0);
+  }
+  ORC_STAGE("DB");
+  sp.k_db = 0;
+  for (int i = 0; i < n; i++)
+    for (int l = g.rp[i]; l < g.rp[i + 1]; l++) sp.k_db = std::max(sp.k_db, std::abs(i - g.ci[l]));
+  const bool doRCM = sp.maxBandwidth > 64;  // BANDWIDTH_THRESHOLD (precond.h:1735-1738)
+  if (doRCM) {
+    sp.k_reorder = RCM(g, sp.optReordering, sp.optPerm);
+  } else {
+    sp.k_reorder = sp.k_db;
+    sp.optReordering.resize(n);
+    sp.optPerm.resize(n);
+    for (int i = 0; i < n; i++) sp.optReordering[i] = sp.optPerm[i] = i;
+  }
+  ORC_STAGE("RCM");
+  if (sp.k_reorder > sp.maxBandwidth || sp.dropFrac > 0) {
+    sp.K = dropOff(g, (T)sp.dropFrac, sp.maxBandwidth, sp.drop_actual);
+  } else {
+    sp.K = sp.k_reorder;
+    sp.drop_actual = T(0);
+  }
+  ORC_STAGE("dropOff");
+  const int K = sp.K;
+  sp.P = std::min(sp.P_req, std::max(n / (K + 1), 1));
+  if (sp.P == 1 || K == 0) sp.varBand = false;
+  const int P = sp.P, q = n / P, rem = n % P;
+  sp.pstart.resize(P);
+  sp.psize.resize(P);
+  for (int p = 0; p < P; p++) { sp.pstart[p] = p * q + std::min(p, rem); sp.psize[p] = q + (p < rem ? 1 : 0); }
+  if (sp.varBand) {
+    assembleOffDiag(g, K, P, sp.WV, sp.offd, sp.wl, sp.wr, sp.permL, sp.permR);
+    ORC_STAGE("assembleOffDiag");
+    secondLevelReordering(g, K, P, sp.secondReorder, sp.secondPerm, sp.first_rows);
+    ORC_STAGE("secondLevelReordering");
+    assembleBandedVar(g, P, sp.ks, sp.boff, sp.ks_col, sp.ks_row);
+    sp.B.assign(sp.boff[P], T(0));
+    for (int j = 0; j < n; j++)
+      for (int it = g.drp[j]; it < g.drp[j + 1]; it++) sp.at(part_of(g.dci[it], q, rem), j, g.dci[it]) = g.dval[it];
+  } else {
+    // constant band over the whole reordered matrix (assembleBandedMatrix, graph.h:1019-1091)
+    sp.ks.assign(P, K);
+    sp.boff.assign(P + 1, 0);
+    for (int p = 0; p < P; p++) sp.boff[p + 1] = sp.boff[p] + (long long)sp.psize[p] * (2 * K + 1);
+    sp.B.assign(sp.boff[P], T(0));
+    for (int j = 0; j < n; j++)
+      for (int it = g.rp[j]; it < g.rp[j + 1]; it++) {
+        int l = g.ci[it];
+        sp.B[(long long)l * (2 * K + 1) + K + (j - l)] = g.val[it];
+      }
+    sp.secondReorder.resize(n);
+    sp.secondPerm.resize(n);
+    for (int i = 0; i < n; i++) sp.secondReorder[i] = sp.secondPerm[i] = i;
+  }
+  // permutation composition (precond.h:2071-2097)
+  sp.finalReordering = sp.optReordering;
+  sp.finalPerm = sp.optPerm;
+  if (sp.varBand) {
+    for (int i = 0; i < n; i++) sp.finalReordering[i] = sp.optReordering[sp.secondReorder[i]];
+    for (int i = 0; i < n; i++) sp.finalPerm[i] = sp.secondPerm[sp.optPerm[i]];
+  }
+  {
+    std::vector<int> tmp(n);
+    for (int i = 0; i < n; i++) tmp[i] = sp.finalPerm[sp.dbRowPerm[i]];
+    sp.finalPerm.swap(tmp);
+  }
+  sp.rowScale.resize(n);
+  sp.colScale.resize(n);
+  for (int i = 0; i < n; i++) { sp.rowScale[i] = (T)sp.rowScaleD[i]; sp.colScale[i] = (T)sp.colScaleD[i]; }
+}
+
+// Sparse right-hand-side solve with the LU (unit L, pivots, post-divided U)
+// of partition p in second-level order: forward from the first nonzero,
+// backward down to `low` (the lowest position whose value is needed).
+template <typename T>
+static void var_solve(SparsePrecond<T>& sp, int p, std::vector<T>& x, int first, int low) {
+  const int s = sp.pstart[p], e = s + sp.psize[p], Kp = sp.ks[p];
+  for (int j = first; j < e - 1; j++) {
+    T xj = x[j];
+    if (xj == T(0)) continue;
+    int w = std::min(Kp, e - 1 - j);
+    for (int t = 1; t <= w; t++) x[j + t] -= xj * sp.at(p, j + t, j);
+  }
+  for (int j = first; j < e; j++) x[j] /= sp.at(p, j, j);
+  for (int j = e - 1; j > low; j--) {
+    T xj = x[j];
+    int w = std::min(Kp, j - s);
+    for (int t = 1; t <= w; t++) x[j - t] -= xj * sp.at(p, j - t, j);
+  }
+}
+
+// Variable-band setup after the reorder: partBlockedBandedLU_var (always
+// boosting, precond.h:4546-4631), calculateSpikes_var (5951-6202) computed
+// as the exact tips of A_i^-1 [0; B_i] and A_{i+1}^-1 [C_{i+1}; 0] in
+// first-level order, then the reduced matrix and its LU.
+template <typename T>
+static void sparse_factor(SparsePrecond<T>& sp) {
+  const int P = sp.P, K = sp.K;
+  if (K == 0) return;
+  const bool bst = sp.varBand ? true : sp.safe;
+  for (int p = 0; p < P; p++) {
+    const int s = sp.pstart[p], e = s + sp.psize[p], Kp = sp.ks[p];
+    for (int j = s; j < e; j++) {
+      int w = std::min(Kp, e - 1 - j);
+      T piv = sp.at(p, j, j);
+      if (bst) { piv = boost(piv); sp.at(p, j, j) = piv; }
+      for (int r = 1; r <= w; r++) sp.at(p, j + r, j) /= piv;
+      for (int c = 1; c <= w; c++) {
+        T u = sp.at(p, j, j + c);
+        for (int r = 1; r <= w; r++) sp.at(p, j + r, j + c) -= sp.at(p, j + r, j) * u;
+      }
+    }
+    if (!bst)
+      for (int j = s; j < e; j++)
+        if (std::fabs(sp.at(p, j, j)) < (T)kBurstValue) { sp.status = -1; sp.msg = "Found a pivot equal to zero"; return; }
+    for (int i = s; i < e; i++) {
+      T d = sp.at(p, i, i);
+      for (int j = i + 1; j <= std::min(e - 1, i + Kp); j++) sp.at(p, i, j) /= d;
+    }
+  }
+  if (P == 1 || !sp.varBand) return;
+  const size_t KK = (size_t)K * K;
+  sp.V.assign(KK * (P - 1), T(0));
+  sp.W.assign(KK * (P - 1), T(0));
+  sp.S.assign(KK * (P - 1), T(0));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < P - 1; i++) {
+    const int ei = sp.pstart[i] + sp.psize[i], s1 = sp.pstart[i + 1];
+    const T* Bm = &sp.offd[2 * i * KK];
+    const T* Cm = &sp.offd[(2 * i + 1) * KK];
+    std::vector<T> x(sp.n, T(0));
+    int lowV = sp.n, lowW = sp.n;
+    for (int r = 0; r < K; r++) {
+      lowV = std::min(lowV, sp.secondPerm[ei - K + r]);
+      lowW = std::min(lowW, sp.secondPerm[s1 + r]);
+    }
+    for (int c = 0; c < K; c++) {
+      bool nz = false;
+      for (int r = 0; r < K; r++) nz |= Bm[r * K + c] != T(0);
+      if (nz) {
+        std::fill(x.begin() + sp.pstart[i], x.begin() + ei, T(0));
+        for (int r = 0; r < K; r++) x[sp.secondPerm[ei - K + r]] = Bm[r * K + c];
+        var_solve(sp, i, x, lowV, lowV);
+        for (int r = 0; r < K; r++) sp.V[i * KK + r * K + c] = x[sp.secondPerm[ei - K + r]];
+      }
+      nz = false;
+      for (int r = 0; r < K; r++) nz |= Cm[r * K + c] != T(0);
+      if (nz) {
+        const int e1 = s1 + sp.psize[i + 1];
+        std::fill(x.begin() + s1, x.begin() + e1, T(0));
+        for (int r = 0; r < K; r++) x[sp.secondPerm[s1 + r]] = Cm[r * K + c];
+        var_solve(sp, i + 1, x, lowW, lowW);
+        for (int r = 0; r < K; r++) sp.W[i * KK + r * K + c] = x[sp.secondPerm[s1 + r]];
+      }
+    }
+    T* Si = &sp.S[i * KK];
+    const T* Vi = &sp.V[i * KK];
+    const T* Wi = &sp.W[i * KK];
+    for (int c = 0; c < K; c++)
+      for (int r = 0; r < K; r++) {
+        T t = (c == r) ? T(1) : T(0);
+        for (int cur = 0; cur < K; cur++) t -= Wi[c * K + cur] * Vi[cur * K + r];
+        Si[c * K + r] = t;
+      }
+    dense_lu(Si, K, sp.safe);
+  }
+}
+
+// Precond::solve with reordering (precond.h:1392-1528): leftTrans, the two
+// sweep pairs around the reduced solve on first-level interface rows, and
+// rightTrans.
+template <typename T>
+static void sparse_apply(SparsePrecond<T>& sp, const double* v, double* z) {
+  const int n = sp.n, K = sp.K, P = sp.P;
+  std::vector<T> f(n);
+  for (int i = 0; i < n; i++) {
+    T a = (T)v[i];
+    f[sp.finalPerm[i]] = sp.scale ? a * sp.rowScale[i] : a;
+  }
+  auto sweep_all = [&](std::vector<T>& x) {
+    if (K == 0) {
+      for (int i = 0; i < n; i++) x[i] /= sp.B[i];
+      return;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < P; p++) var_solve(sp, p, x, sp.pstart[p], sp.pstart[p]);
+  };
+  if (P > 1 && sp.varBand) {
+    std::vector<T> g = f;
+    sweep_all(g);
+    const size_t KK = (size_t)K * K;
+    for (int i = 0; i < P - 1; i++) {
+      const int ei = sp.pstart[i] + sp.psize[i], s1 = sp.pstart[i + 1];
+      const T* Vi = &sp.V[i * KK];
+      const T* Wi = &sp.W[i * KK];
+      const T* Si = &sp.S[i * KK];
+      std::vector<T> xb(K), z2(K);
+      for (int r = 0; r < K; r++) xb[r] = g[sp.secondPerm[ei - K + r]];
+      for (int r = 0; r < K; r++) {
+        T t = g[sp.secondPerm[s1 + r]];
+        for (int c = 0; c < K; c++) t -= Wi[r * K + c] * xb[c];
+        z2[r] = t;
+      }
+      for (int r = 0; r < K; r++)
+        for (int c = 0; c < r; c++) z2[r] -= Si[r * K + c] * z2[c];
+      for (int r = 0; r < K; r++) z2[r] /= Si[r * K + r];
+      for (int r = K - 1; r >= 0; r--)
+        for (int c = r + 1; c < K; c++) z2[r] -= Si[r * K + c] * z2[c];
+      std::vector<T> x1(K);
+      for (int r = 0; r < K; r++) {
+        T t = xb[r];
+        for (int c = 0; c < K; c++) t -= Vi[r * K + c] * z2[c];
+        x1[r] = t;
+      }
+      const T* Bm = &sp.offd[2 * i * KK];
+      const T* Cm = &sp.offd[(2 * i + 1) * KK];
+      for (int c = 0; c < K; c++) {
+        T t1 = T(0), t2 = T(0);
+        for (int r = 0; r < K; r++) {
+          t1 += Bm[c * K + r] * z2[r];
+          t2 += Cm[c * K + r] * x1[r];
+        }
+        f[sp.secondPerm[ei - K + c]] -= t1;
+        f[sp.secondPerm[s1 + c]] -= t2;
+      }
+    }
+  }
+  sweep_all(f);
+  for (int i = 0; i < n; i++) {
+    int d = sp.finalReordering[i];
+    z[d] = (double)(sp.scale ? f[i] * sp.colScale[d] : f[i]);
+  }
+}
+
+}  // namespace orc
+
+struct orc_sparse_info {
+  int n, nnz, K, P, k_db, k_reorder, varBand, status;
+  double drop_actual;
+};
+
+struct orc_sparse_handle {
+  int dtype;
+  orc::SparsePrecond<float> f;
+  orc::SparsePrecond<double> d;
+  template <typename Fn> auto visit(Fn fn) { return dtype ? fn(d) : fn(f); }
+};
+
+extern "C" {
+
+void* orc_sparse_create(int P, int dtype, int doDB, int scale, double dropFrac, int maxBandwidth, int varBand,
+                        int safe) {
+  auto* h = new orc_sparse_handle();
+  h->dtype = dtype;
+  h->visit([&](auto& sp) {
+    sp.P_req = P; sp.doDB = doDB != 0; sp.scale = scale != 0; sp.dropFrac = dropFrac;
+    sp.maxBandwidth = maxBandwidth; sp.varBand = varBand != 0; sp.safe = safe != 0;
+    return 0;
+  });
+  return h;
+}
+
+void orc_sparse_destroy(void* h) { delete (orc_sparse_handle*)h; }
+
+// Runs the reorder pipeline only (stage 0) or reorder + factorisation (1).
+int orc_sparse_setup(void* h, int n, const int* rp, const int* ci, const double* v, int factor, char* msg, int msglen) {
+  auto* H = (orc_sparse_handle*)h;
+  return H->visit([&](auto& sp) -> int {
+    try {
+      orc::sparse_reorder(sp, n, rp, ci, v);
+      if (!sp.varBand && sp.P > 1) { sp.status = -103; sp.msg = "constant band with reordering not restated"; }
+      else if (factor) orc::sparse_factor(sp);
+    } catch (const orc::DBError& e) {
+      sp.status = e.code;
+      sp.msg = e.what();
+    }
+    if (msg && msglen > 0) { std::strncpy(msg, sp.msg.c_str(), msglen - 1); msg[msglen - 1] = 0; }
+    return sp.status;
+  });
+}
+
+void orc_sparse_info_get(void* h, orc_sparse_info* out) {
+  ((orc_sparse_handle*)h)->visit([&](auto& sp) {
+    out->n = sp.n; out->nnz = sp.nnz; out->K = sp.K; out->P = sp.P; out->k_db = sp.k_db;
+    out->k_reorder = sp.k_reorder; out->varBand = sp.varBand; out->status = sp.status;
+    out->drop_actual = (double)sp.drop_actual;
+    return 0;
+  });
+}
+
+// Integer outputs: 0 dbRowPerm, 1 optReordering (RCM), 2 optPerm (RCM),
+// 3 secondReorder, 4 secondPerm, 5 first_rows, 6 ks, 7 finalPerm,
+// 8 finalReordering, 9 offDiagWidths_left, 10 offDiagWidths_right,
+// 11 offDiagPerms_left, 12 offDiagPerms_right, 13 ks_col, 14 ks_row.
+long long orc_sparse_ints(void* h, int which, int* out) {
+  return ((orc_sparse_handle*)h)->visit([&](auto& sp) -> long long {
+    const std::vector<int>* vs[] = {&sp.dbRowPerm, &sp.optReordering, &sp.optPerm, &sp.secondReorder,
+                                    &sp.secondPerm, &sp.first_rows, &sp.ks, &sp.finalPerm, &sp.finalReordering,
+                                    &sp.wl, &sp.wr, &sp.permL, &sp.permR, &sp.ks_col, &sp.ks_row};
+    if (which < 0 || which > 14) return -1;
+    const auto& vec = *vs[which];
+    if (out) std::copy(vec.begin(), vec.end(), out);
+    return (long long)vec.size();
+  });
+}
+
+// Real outputs: 0 row scale, 1 column scale (double, before the cast to
+// PrecValueType), 2 band, 3 offDiags, 4 V, 5 W, 6 S.
+long long orc_sparse_reals(void* h, int which, double* out) {
+  return ((orc_sparse_handle*)h)->visit([&](auto& sp) -> long long {
+    if (which == 0) { if (out) std::copy(sp.rowScaleD.begin(), sp.rowScaleD.end(), out); return (long long)sp.rowScaleD.size(); }
+    if (which == 1) { if (out) std::copy(sp.colScaleD.begin(), sp.colScaleD.end(), out); return (long long)sp.colScaleD.size(); }
+    using TT = typename std::decay<decltype(sp.B)>::type;
+    const TT* vs[] = {&sp.B, &sp.offd, &sp.V, &sp.W, &sp.S};
+    if (which < 2 || which > 6) return -1;
+    const auto& vec = *vs[which - 2];
+    if (out)
+      for (size_t i = 0; i < vec.size(); i++) out[i] = (double)vec[i];
+    return (long long)vec.size();
+  });
+}
+
+void orc_sparse_apply(void* h, const double* v, double* z) {
+  ((orc_sparse_handle*)h)->visit([&](auto& sp) { orc::sparse_apply(sp, v, z); return 0; });
+}
+
+// BiCGStab(L) with this preconditioner and the CSR operator (Solver::solve).
+int orc_sparse_solve(void* h, int n, const int* rp, const int* ci, const double* vals, const double* b, double* x,
+                     int L, int maxit, double reltol, double abstol, orc_result* res) {
+  auto* H = (orc_sparse_handle*)h;
+  orc::Op op; op.n = n; op.rp = rp; op.ci = ci; op.vals = vals;
+  orc::Monitor mon; mon.maxIt = maxit; mon.relTol = reltol; mon.absTol = abstol;
+  std::vector<double> bv(b, b + n), xv(x, x + n);
+  mon.rhsNorm = orc::nrm2(bv);
+  orc::Apply A = [&](const std::vector<double>& in, std::vector<double>& out) { op.apply(in.data(), out.data()); };
+  orc::Apply Pm = [&](const std::vector<double>& in, std::vector<double>& out) {
+    H->visit([&](auto& sp) { orc::sparse_apply(sp, in.data(), out.data()); return 0; });
+  };
+  orc::bicgstabl(A, Pm, xv, bv, mon, L);
+  std::copy(xv.begin(), xv.end(), x);
+  res->code = mon.code; res->iterations = mon.it; res->rhs_norm = mon.rhsNorm;
+  res->res_norm = mon.rNorm; res->rel_res_norm = mon.rNorm / mon.rhsNorm;
+  H->visit([&](auto& sp) { res->n = sp.n; res->K = sp.K; res->P = sp.P; res->status = sp.status; return 0; });
+  return mon.code;
+}
+
+}  // extern "C"

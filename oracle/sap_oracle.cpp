@@ -822,3 +822,4 @@ int orc_num_threads(void) {
 }
 
 }  // extern "C"
+#include "reorder_oracle.cpp"

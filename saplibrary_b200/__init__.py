@@ -112,6 +112,7 @@ _sig = {
     "sap_solver_get_monitor": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_char_p)]),
     "sap_solver_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_solver_stream": (_vp, [_vp]),
+    "sap_solver_get_reorder": (_i, [_vp, _i, _vp, ctypes.POINTER(ctypes.c_int64)]),
     "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_blas_dots_noalloc": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_profile_select": (_i, [ctypes.c_char_p]),
@@ -399,6 +400,18 @@ class Solver:
         n, k, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(_lib.sap_solver_info(self._h, ctypes.byref(n), ctypes.byref(k), ctypes.byref(p)))
         return n.value, k.value, p.value
+
+    REORDER_ARRAYS = ("dbRowPerm", "finalPerm", "finalReordering", "first_rows", "ks")
+
+    def getReorder(self, name: str) -> np.ndarray:
+        """Reordering results of a CSR setup (see sap_solver_get_reorder)."""
+        w = self.REORDER_ARRAYS.index(name)
+        cnt = ctypes.c_int64()
+        _check(_lib.sap_solver_get_reorder(self._h, w, None, ctypes.byref(cnt)))
+        out = np.empty(cnt.value, np.int32)
+        if cnt.value:
+            _check(_lib.sap_solver_get_reorder(self._h, w, ctypes.c_void_p(out.ctypes.data), ctypes.byref(cnt)))
+        return out
 
     def stream(self) -> int:
         return _lib.sap_solver_stream(self._h) or 0

@@ -17,10 +17,13 @@ namespace sapb {
 
 // Library failure carrying a C-ABI status code.  Reference failures use the
 // sap::system_error::Reason values (sap/exception.h:16-23).
+#ifndef SAPB_ERROR_DEFINED
+#define SAPB_ERROR_DEFINED
 struct Error : public std::runtime_error {
   int code;
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
+#endif
 
 inline void cuda_check(cudaError_t e, const char* what) {
   if (e != cudaSuccess) {

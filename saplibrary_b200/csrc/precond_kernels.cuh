@@ -420,7 +420,8 @@ __device__ __forceinline__ int dir1_of(const PartDev& p) { return p.ul ? DIR_UP 
 template <typename T, int PF>
 __global__ void k_pass1(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
                         const long long* __restrict__ koff, const T* __restrict__ B,
-                        const double* __restrict__ vin, T* __restrict__ F, T* __restrict__ tails) {
+                        const double* __restrict__ vin, T* __restrict__ F, T* __restrict__ tails,
+                        const int* __restrict__ gin, const T* __restrict__ sin) {
   extern __shared__ __align__(16) unsigned char xs_raw[];
   T* xs = reinterpret_cast<T*>(xs_raw);
   const ChunkDev ch = chunks[blockIdx.x];
@@ -429,7 +430,12 @@ __global__ void k_pass1(const PartDev* __restrict__ parts, const ChunkDev* __res
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     int row = o + dir * i;
     T v;
-    if (vin) { v = (T)vin[row]; F[row] = v; }
+    if (vin) {
+      // leftTrans (precond.h:1535-1544): band row `row` takes input row gin[row], scaled
+      if (gin) v = (T)vin[gin[row]] * sin[row];
+      else v = (T)vin[row];
+      F[row] = v;
+    }
     else v = F[row];
     xs[K + i] = v;
   }
@@ -477,7 +483,8 @@ template <typename T, int PF>
 __global__ void k_pass3(const PartDev* __restrict__ parts, const ChunkDev* __restrict__ chunks,
                         const int* __restrict__ first2, const long long* __restrict__ koff,
                         const T* __restrict__ B, const T* __restrict__ Y,
-                        const T* __restrict__ carry2, double* __restrict__ zout, T* __restrict__ gout) {
+                        const T* __restrict__ carry2, double* __restrict__ zout, T* __restrict__ gout,
+                        const int* __restrict__ sout, const T* __restrict__ cout) {
   extern __shared__ __align__(16) unsigned char xs_raw[];
   T* xs = reinterpret_cast<T*>(xs_raw);
   const int c = blockIdx.x;
@@ -492,8 +499,13 @@ __global__ void k_pass3(const PartDev* __restrict__ parts, const ChunkDev* __res
   chunk_solve<T, PF>(xs, m, K, dir2, o2, B + p.boff, p.start, SW, has_carry);
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     int row = o2 + dir2 * i;
-    if (zout) zout[row] = (double)xs[K + i];
-    else gout[row] = xs[K + i];
+    if (zout) {
+      // rightTrans (precond.h:1550-1559): band column `row` is input column sout[row], scaled
+      if (sout) zout[sout[row]] = (double)(xs[K + i] * cout[row]);
+      else zout[row] = (double)xs[K + i];
+    } else {
+      gout[row] = xs[K + i];
+    }
   }
 }
 
@@ -585,7 +597,7 @@ template <typename T>
 __global__ void __launch_bounds__(1024)
 k_reduced_apply(const PartDev* __restrict__ parts, const T* __restrict__ V, const T* __restrict__ Wm,
                 const T* __restrict__ S, const T* __restrict__ offd, const T* __restrict__ Gv,
-                T* __restrict__ F, int K) {
+                T* __restrict__ F, int K, const int* __restrict__ iface) {
   extern __shared__ __align__(16) unsigned char sh_raw[];
   T* sh = reinterpret_cast<T*>(sh_raw);
   T* xb = sh;
@@ -599,10 +611,15 @@ k_reduced_apply(const PartDev* __restrict__ parts, const T* __restrict__ V, cons
   const T* Si = S + i * KK;
   const T* Bm = offd + (2 * i) * KK;
   const T* Cm = offd + (2 * i + 1) * KK;
-  if (r < K) xb[r] = Gv[s - K + r];
+  // band positions of the interface rows: the bottom K rows of partition i
+  // and the top K rows of partition i+1 in the first-level order
+  const int* map = iface ? iface + (long long)i * 2 * K : nullptr;
+  auto pos_b = [&](int q) { return map ? map[q] : s - K + q; };
+  auto pos_t = [&](int q) { return map ? map[K + q] : s + q; };
+  if (r < K) xb[r] = Gv[pos_b(r)];
   __syncthreads();
   if (r < K) {
-    T acc = Gv[s + r];
+    T acc = Gv[pos_t(r)];
     for (int c = 0; c < K; c++) acc -= Wi[r * K + c] * xb[c];
     z[r] = acc;
   }
@@ -631,9 +648,85 @@ k_reduced_apply(const PartDev* __restrict__ parts, const T* __restrict__ V, cons
       t1 += Bm[r * K + c] * z[c];
       t2 += Cm[r * K + c] * x1[c];
     }
-    F[s - K + r] -= t1;
-    F[s + r] -= t2;
+    F[pos_b(r)] -= t1;
+    F[pos_t(r)] -= t2;
   }
+}
+
+// DB edge weights on the device, as the reference computes them
+// (get_csc_matrix + getResidualValues, graph.h:1827-1857, db.cuh:14-37):
+// w[e] = log(max_row |a| / |a_e|) in double, one warp per row.
+__global__ void k_db_weights(const int* __restrict__ rp, const double* __restrict__ a, double* __restrict__ w,
+                             double* __restrict__ rowmax, int n) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    double m = 0.0;
+    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) m = fmax(m, fabs(a[e]));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) w[e] = log(m / fabs(a[e]));
+    if (lane == 0) rowmax[i] = m;
+  }
+}
+
+// Diagonal-block entries (band row j, band column l) into the variable band
+// (var::copyFromCOOMatrixToBandedMatrix, data_transfer.cuh:454-495).
+template <typename T>
+__global__ void k_band_from_coo_var(const int* __restrict__ rows, const int* __restrict__ cols,
+                                    const T* __restrict__ vals, long long nz, const PartDev* __restrict__ parts,
+                                    const int* __restrict__ part_of_col, T* __restrict__ B) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nz; e += (long long)gridDim.x * blockDim.x) {
+    const int j = rows[e], l = cols[e];
+    const PartDev p = parts[part_of_col[l]];
+    B[p.boff + (long long)(l - p.start) * (2 * p.K + 1) + p.K + (j - l)] = vals[e];
+  }
+}
+
+// Spike tips of the variable-band method (calculateSpikes_var + spikeSweeps,
+// sap/precond.h:5951-6202), computed exactly: V_i = the rows of
+// A_i^-1 [0; B_i] at the bottom K first-level rows of partition i, W_i = the
+// rows of A_{i+1}^-1 [C_{i+1}; 0] at its top K rows.  The partitions' LU
+// factors are in the second-level order, so right-hand sides and tips go
+// through the interface position map.  One thread per right-hand-side
+// column; the column is swept through the partition in a scratch array
+// interleaved by column (coalesced across threads).
+template <typename T>
+__global__ void k_spikes_var(const PartDev* __restrict__ parts, const T* __restrict__ B,
+                             const T* __restrict__ offd, const int* __restrict__ iface, T* __restrict__ V,
+                             T* __restrict__ Wm, T* __restrict__ scratch, long long stride, int K) {
+  const int i = blockIdx.x, which = blockIdx.y, col = threadIdx.x;
+  if (col >= K) return;
+  const long long KK = (long long)K * K;
+  const PartDev p = parts[i + which];
+  const T* M = offd + (2 * i + which) * KK;
+  const int* map = iface + (long long)i * 2 * K + (which ? K : 0);
+  T* out = (which ? Wm : V) + i * KK;
+  bool nz = false;
+  for (int r = 0; r < K; r++) nz |= M[r * K + col] != T(0);
+  if (!nz) {
+    for (int r = 0; r < K; r++) out[r * K + col] = T(0);
+    return;
+  }
+  T* x = scratch + ((long long)(2 * i + which) * stride) * K;  // x[j*K + col], j local to the partition
+  const int s = p.start, np = p.size, Kp = p.K, SW = 2 * Kp + 1;
+  const T* band = B + p.boff;
+  int low = np;
+  for (int r = 0; r < K; r++) low = min(low, map[r] - s);
+  for (int j = low; j < np; j++) x[(long long)j * K + col] = T(0);
+  for (int r = 0; r < K; r++) x[(long long)(map[r] - s) * K + col] = M[r * K + col];
+  for (int j = low; j < np - 1; j++) {
+    const T xj = x[(long long)j * K + col];
+    if (xj == T(0)) continue;
+    const int w = min(Kp, np - 1 - j);
+    for (int t = 1; t <= w; t++) x[(long long)(j + t) * K + col] -= xj * band[(long long)j * SW + Kp + t];
+  }
+  for (int j = low; j < np; j++) x[(long long)j * K + col] /= band[(long long)j * SW + Kp];
+  for (int j = np - 1; j > low; j--) {
+    const T xj = x[(long long)j * K + col];
+    const int w = min(Kp, j);
+    for (int t = 1; t <= w; t++) x[(long long)(j - t) * K + col] -= xj * band[(long long)j * SW + Kp - t];
+  }
+  for (int r = 0; r < K; r++) out[r * K + col] = x[(long long)(map[r] - s) * K + col];
 }
 
 // K == 0: the band is the diagonal (getSRev, sap/precond.h:1416-1419).

@@ -1,0 +1,68 @@
+// Host reordering pipeline of the sparse setup (see reorder.cpp).
+#pragma once
+
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sap_b200.h"
+
+namespace sapb {
+
+#ifndef SAPB_ERROR_DEFINED
+#define SAPB_ERROR_DEFINED
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+#endif
+
+namespace rp {
+
+// T is the preconditioner value type: the reference runs the whole
+// reordering on the matrix converted to it (precond.h:1667-1713).
+template <typename T>
+class Pipeline {
+ public:
+  // input: CSR in T with explicit zeros removed
+  int n = 0, nnz = 0;
+  std::vector<int> in_rp, in_ci;
+  std::vector<T> in_val;
+  // options
+  bool do_db = true, scale = true, var_band = true;
+  double drop_frac = 0;
+  int max_bandwidth = std::numeric_limits<int>::max();
+  int P_req = 1;
+
+  // outputs
+  std::vector<int> db_row_perm;                  // input row i -> row db_row_perm[i]
+  std::vector<double> row_scale, col_scale;      // DB scalings (double)
+  std::vector<int> rcm_order, rcm_pos;           // RCM: position -> node, node -> position
+  std::vector<int> second_order, second_pos;     // second level, same convention
+  std::vector<int> final_pos, final_order;       // composed: input row -> band row; band col -> input col
+  std::vector<int> first_rows;
+  std::vector<T> offd;                           // coupling blocks, row-major K x K, 2 per interface
+  std::vector<int> part_k;                       // K_p of the variable band
+  int k_db = 0, k_reorder = 0, K = 0, P = 1;
+  T drop_actual = T(0);
+
+  // working matrices: the reordered matrix and its diagonal blocks (CSR in T)
+  std::vector<int> m_rp, m_ci, d_rp, d_ci;
+  std::vector<T> m_val, d_val;
+  std::vector<char> couples_right;
+
+  // weight[e] = log(rowmax[row(e)] / |a_e|) and rowmax, both from the device
+  void run(const std::vector<double>& weight, const std::vector<double>& rowmax);
+
+ private:
+  void db(const std::vector<double>& weight, const std::vector<double>& rowmax);
+  int rcm();
+  int drop_off(T frac, int max_bw);
+  void assemble_coupling(int K, int P);
+  void second_level(int K, int P);
+  void assemble_var_band(int P);
+};
+
+}  // namespace rp
+}  // namespace sapb

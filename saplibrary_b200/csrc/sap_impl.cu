@@ -20,6 +20,7 @@
 #include "krylov_kernels.cuh"
 #include "precond_kernels.cuh"
 #include "reorder.h"
+#include "reorder_pipeline.h"
 
 namespace sapb {
 
@@ -120,12 +121,11 @@ class PrecBase {
   std::vector<PartDev> parts_h;
   DBuf<PartDev> parts_d;
 
-  // reordering (sparse path): row/column permutations and scalings
+  // reordering (sparse path): permutations, interface map, statistics
   bool reordered = false;
-  Reorder ro;
-  DBuf<int> perm_in_d, perm_out_d;
-  DBuf<double> scale_in_d, scale_out_d;
-  DBuf<double> vtmp, ztmp;
+  bool var_band = false;
+  DBuf<int> gin_d, sout_d, iface_d, partcol_d;
+  std::vector<int> final_pos_h, final_order_h, db_row_perm_h, first_rows_h, part_k_h;
 
   // statistics
   double t_toBanded = 0, t_offDiags = 0, t_bandLU = 0, t_assembly = 0, t_fullLU = 0, t_transfer = 0;
@@ -138,8 +138,9 @@ class PrecBase {
   // used without reordering.
   virtual void setup_rowmajor(const double* A_dev, int n_, int K_) = 0;
   virtual void setup_csr_direct(const Csr& A, int K_) = 0;
+  virtual void setup_sparse(const Csr& A) = 0;
   virtual void apply_band(const double* v, double* z) = 0;
-  void apply(const double* v, double* z);
+  void apply(const double* v, double* z) { apply_band(v, z); }
 
   void clamp_partitions_banded() {
     // convertToBandedMatrix (sap/precond.h:2116-2117, 2258-2259)
@@ -178,6 +179,7 @@ class PrecondT : public PrecBase {
   DBuf<int> first1_d, first2_d, pchunk0_d, pnchunk_d;
   DBuf<T> T1, T2, tails1, tails2, carry1, carry2;
   DBuf<T> F, Gv, Y;
+  DBuf<T> sin_d, cout_d;  // DB row / column scales in band order (reordered path)
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
 
@@ -206,6 +208,177 @@ class PrecondT : public PrecBase {
     SAPB_CUDA(cudaStreamSynchronize(st));
     t_toBanded = ms_since(t1);
     setup_from_band();
+  }
+
+  // transformToBandedMatrix (sap/precond.h:1656-2101) and the rest of the
+  // setup for a CSR matrix with reordering: DB weights on the device, the
+  // graph pipeline on the host, then the band, factors, spikes and sweeps on
+  // the device.
+  void setup_sparse(const Csr& A) override {
+    if (o.dbFirstStageOnly) throw Error(SAP_ERR_UNSUPPORTED, "dbFirstStageOnly is not supported");
+    if (o.ilu_level >= 0) throw Error(SAP_ERR_UNSUPPORTED, "ILU preconditioning is out of scope");
+    auto t0 = Clock::now();
+    n = A.n;
+    rp::Pipeline<T> pl;
+    pl.n = n;
+    pl.P_req = P_req;
+    pl.do_db = o.performDB != 0;
+    pl.scale = o.applyScaling != 0;
+    pl.drop_frac = o.dropOffFraction;
+    pl.max_bandwidth = o.maxBandwidth;
+    pl.var_band = o.variableBandwidth != 0;
+    // the matrix in the preconditioner's value type, explicit zeros removed
+    pl.in_rp.assign(n + 1, 0);
+    pl.in_ci.reserve(A.nnz);
+    pl.in_val.reserve(A.nnz);
+    for (int i = 0; i < n; i++) {
+      for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) {
+        T a = (T)A.v_h[e];
+        if (a != T(0)) { pl.in_ci.push_back(A.ci_h[e]); pl.in_val.push_back(a); }
+      }
+      pl.in_rp[i + 1] = (int)pl.in_ci.size();
+    }
+    pl.nnz = (int)pl.in_ci.size();
+    std::vector<double> w, rmax;
+    if (pl.do_db) {
+      DBuf<int> drp;
+      DBuf<double> da, dw, dmax;
+      std::vector<double> av(pl.in_val.begin(), pl.in_val.end());
+      drp.upload(pl.in_rp, st);
+      da.upload(av, st);
+      dw.alloc(av.size());
+      dmax.alloc(n);
+      k_db_weights<<<grid_for((long long)n * 32, 256, 148 * 32), 256, 0, st>>>(drp.get(), da.get(), dw.get(), dmax.get(), n);
+      SAPB_LAUNCHED();
+      dw.download(w, st);
+      dmax.download(rmax, st);
+      SAPB_CUDA(cudaStreamSynchronize(st));
+    }
+    t_transfer = ms_since(t0);
+    auto t1 = Clock::now();
+    pl.run(w, rmax);
+    t_reorder = ms_since(t1);
+    k_db = pl.k_db;
+    k_reorder = pl.k_reorder;
+    drop_actual = (double)pl.drop_actual;
+    K = pl.K;
+    P = pl.P;
+    var_band = pl.var_band;
+    final_pos_h = pl.final_pos;
+    final_order_h = pl.final_order;
+    db_row_perm_h = pl.db_row_perm;
+    first_rows_h = pl.first_rows;
+    part_k_h = pl.part_k;
+    // leftTrans / rightTrans as gathers and scatters in band order
+    {
+      std::vector<int> gin(n), sout(n);
+      std::vector<T> sn(n), cn(n);
+      for (int q = 0; q < n; q++) {
+        gin[pl.final_pos[q]] = q;
+        sn[pl.final_pos[q]] = pl.scale ? (T)pl.row_scale[q] : T(1);
+      }
+      for (int k = 0; k < n; k++) {
+        sout[k] = pl.final_order[k];
+        cn[k] = pl.scale ? (T)pl.col_scale[pl.final_order[k]] : T(1);
+      }
+      gin_d.upload(gin, st);
+      sout_d.upload(sout, st);
+      sin_d.upload(sn, st);
+      cout_d.upload(cn, st);
+    }
+    reordered = true;
+    if (!var_band) {
+      // constant band over the whole reordered matrix (assembleBandedMatrix, graph.h:1019-1091)
+      B.alloc((size_t)(2 * K + 1) * n);
+      B.zero(st);
+      DBuf<int> drp, dci;
+      DBuf<double> dv;
+      std::vector<double> mv(pl.m_val.begin(), pl.m_val.end());
+      drp.upload(pl.m_rp, st);
+      dci.upload(pl.m_ci, st);
+      dv.upload(mv, st);
+      k_band_from_csr<T><<<grid_for(n, 256), 256, 0, st>>>(drp.get(), dci.get(), dv.get(), B.get(), n, K);
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      t_cpu_assemble = ms_since(t0);
+      setup_from_band();
+      return;
+    }
+    // variable band: partitions with their own K_p (>= 1 for storage)
+    ptype = o.precondType;
+    spike = (ptype == SAP_PRECOND_SPIKE && P > 1);
+    lu_ul = false;  // a variable band forces LU_only (driver_test.cu:832-833)
+    if (ptype == SAP_PRECOND_NONE) return;
+    parts_h.resize(P);
+    const int q = n / P, r = n % P;
+    long long off = 0;
+    std::vector<int> partcol(n);
+    for (int p = 0; p < P; p++) {
+      PartDev d{};
+      d.start = p * q + std::min(p, r);
+      d.size = q + (p < r ? 1 : 0);
+      d.K = std::max(1, pl.part_k[p]);
+      d.ul = 0;
+      d.boff = off;
+      off += (long long)d.size * (2 * d.K + 1);
+      parts_h[p] = d;
+      for (int i = d.start; i < d.start + d.size; i++) partcol[i] = p;
+    }
+    parts_d.upload(parts_h, st);
+    partcol_d.upload(partcol, st);
+    B.alloc((size_t)off);
+    B.zero(st);
+    {
+      std::vector<int> rows(pl.d_ci.size());
+      for (int i = 0; i < n; i++)
+        for (int e = pl.d_rp[i]; e < pl.d_rp[i + 1]; e++) rows[e] = i;
+      DBuf<int> drows, dcols;
+      DBuf<T> dvals;
+      drows.upload(rows, st);
+      dcols.upload(pl.d_ci, st);
+      dvals.upload(pl.d_val, st);
+      k_band_from_coo_var<T><<<grid_for((long long)rows.size(), 256, 148 * 32), 256, 0, st>>>(
+          drows.get(), dcols.get(), dvals.get(), (long long)rows.size(), parts_d.get(), partcol_d.get(), B.get());
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+    }
+    t_cpu_assemble = ms_since(t0) - t_reorder - t_transfer;
+    auto t2 = Clock::now();
+    factor();
+    t_bandLU = ms_since(t2);
+    if (spike) {
+      t2 = Clock::now();
+      const size_t KK = (size_t)K * K;
+      offd.upload(pl.offd, st);
+      std::vector<int> iface((size_t)(P - 1) * 2 * K);
+      for (int i = 0; i < P - 1; i++) {
+        const int e_i = parts_h[i].start + parts_h[i].size, s1 = parts_h[i + 1].start;
+        for (int k = 0; k < K; k++) {
+          iface[(size_t)i * 2 * K + k] = pl.second_pos[e_i - K + k];
+          iface[(size_t)i * 2 * K + K + k] = pl.second_pos[s1 + k];
+        }
+      }
+      iface_d.upload(iface, st);
+      V.alloc(KK * (P - 1));
+      W.alloc(KK * (P - 1));
+      S.alloc(KK * (P - 1));
+      int maxsz = 0;
+      for (auto& d : parts_h) maxsz = std::max(maxsz, d.size);
+      scratch.alloc((size_t)2 * (P - 1) * maxsz * K);
+      if (K > 1024) throw Error(SAP_ERR_UNSUPPORTED, "coupling width above 1024 is not supported by the spike kernel");
+      k_spikes_var<T><<<dim3(P - 1, 2), ((K + 31) / 32) * 32, 0, st>>>(parts_d.get(), B.get(), offd.get(), iface_d.get(),
+                                                                   V.get(), W.get(), scratch.get(), (long long)maxsz, K);
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      scratch.release();
+      t_assembly = ms_since(t2);
+      t2 = Clock::now();
+      k_reduced_factor<T><<<P - 1, 512, 0, st>>>(V.get(), W.get(), S.get(), K, o.safeFactorization ? 1 : 0);
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      t_fullLU = ms_since(t2);
+    }
+    build_sweeps();
   }
 
   void setup_from_band() {
@@ -264,18 +437,19 @@ class PrecondT : public PrecBase {
   void factor() {
     std::vector<FactorJob> jobs;
     bool boost;
-    if (!spike) {
+    // the variable-band kernels always boost (partBlockedBandedLU_var, precond.h:4546-4631)
+    if (var_band) {
+      boost = true;
+      for (const auto& d : parts_h) jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 0, 0, 0, d.boff});
+    } else if (!spike) {
       boost = o.safeFactorization || (P > 1 && K >= 70);
-      for (int p = 0; p < P; p++) {
-        const auto& d = parts_h[p];
-        jobs.push_back(FactorJob{d.start, d.start + d.size, K, 0, 0, 0, d.boff});
-      }
+      for (const auto& d : parts_h) jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 0, 0, 0, d.boff});
     } else {
       boost = o.safeFactorization || K >= 70;
       int nlu = lu_ul ? P - 1 : P;
       for (int p = 0; p < nlu; p++) {
         const auto& d = parts_h[p];
-        jobs.push_back(FactorJob{d.start, d.start + d.size, K, 0, 0, 0, d.boff});
+        jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 0, 0, 0, d.boff});
       }
       if (lu_ul) {
         if (P > 2) {
@@ -285,7 +459,7 @@ class PrecondT : public PrecBase {
         for (int p = 1; p < P; p++) {
           const auto& d = parts_h[p];
           int target = (p == P - 1) ? 0 : 1;
-          jobs.push_back(FactorJob{d.start, d.start + d.size, K, 1, target, 0, d.boff});
+          jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 1, target, 0, d.boff});
         }
       }
     }
@@ -293,11 +467,12 @@ class PrecondT : public PrecBase {
     jobs_d.upload(jobs, st);
     flag.alloc(1);
     flag.zero(st);
-    int G = std::max(1, std::min(K, 512 / std::max(K, 1)));
-    int NT = ((K * G + 31) / 32) * 32;
+    const int Kmax = parts_maxK();
+    int G = std::max(1, std::min(Kmax, 512 / std::max(Kmax, 1)));
+    int NT = ((Kmax * G + 31) / 32) * 32;
     NT = std::max(NT, 64);
     constexpr int D = 8;
-    size_t smem = ((size_t)(K + 1 + D) * (2 * K + 1) + (K + 1 + D)) * sizeof(T);
+    size_t smem = ((size_t)(Kmax + 1 + D) * (2 * Kmax + 1) + (Kmax + 1 + D)) * sizeof(T);
     if (smem <= 200 * 1024) {
       SAPB_CUDA(cudaFuncSetAttribute(k_factor_smem<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       SAPB_PROF("factor", st);
@@ -311,7 +486,7 @@ class PrecondT : public PrecBase {
     int hflag = 0;
     SAPB_CUDA(cudaMemcpyAsync(&hflag, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     SAPB_CUDA(cudaStreamSynchronize(st));
-    if (hflag && !o.safeFactorization) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
+    if (hflag && !o.safeFactorization && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
   }
 
   void build_sweeps() {
@@ -397,7 +572,8 @@ class PrecondT : public PrecBase {
     const size_t ssm = (size_t)(maxK + scanG * maxK) * sizeof(T);
     {
       SAPB_PROF("pass1", st);
-      k_pass1<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), koff_d.get(), B.get(), vin, F.get(), tails1.get());
+      k_pass1<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), koff_d.get(), B.get(), vin, F.get(), tails1.get(),
+                                          reordered ? gin_d.get() : nullptr, reordered ? sin_d.get() : nullptr);
       SAPB_LAUNCHED();
     }
     {
@@ -421,7 +597,8 @@ class PrecondT : public PrecBase {
     {
       SAPB_PROF("pass3", st);
       k_pass3<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), first2_d.get(), koff_d.get(), B.get(), Y.get(),
-                                          carry2.get(), zout, gout);
+                                          carry2.get(), zout, gout, reordered ? sout_d.get() : nullptr,
+                                          reordered ? cout_d.get() : nullptr);
       SAPB_LAUNCHED();
     }
   }
@@ -434,6 +611,7 @@ class PrecondT : public PrecBase {
       return;
     }
     if (K == 0) {
+      if (reordered) throw Error(SAP_ERR_UNSUPPORTED, "a diagonal matrix after reordering is not supported");
       k_diag_apply<T><<<grid_for(n, 256), 256, 0, st>>>(B.get(), v, z, n);
       SAPB_LAUNCHED();
       return;
@@ -443,7 +621,8 @@ class PrecondT : public PrecBase {
       {
       SAPB_PROF("reduced_apply", st);
       k_reduced_apply<T><<<P - 1, ((K + 31) / 32) * 32, 3 * K * sizeof(T), st>>>(parts_d.get(), V.get(), W.get(), S.get(),
-                                                                            offd.get(), Gv.get(), F.get(), K);
+                                                                            offd.get(), Gv.get(), F.get(), K,
+                                                                            var_band ? iface_d.get() : nullptr);
       SAPB_LAUNCHED();
       }
       sweep_pair(nullptr, z, nullptr);
@@ -709,21 +888,6 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
   }
   SAPB_CUDA(cudaStreamSynchronize(st));
 }
-
-// Precond::operator() with the reordering transforms (leftTrans / rightTrans,
-// sap/precond.h:1535-1559) around the band apply.
-void PrecBase::apply(const double* v, double* z) {
-  if (!reordered) { apply_band(v, z); return; }
-  reorder_apply_in(*this, v, vtmp.get());
-  apply_band(vtmp.get(), ztmp.get());
-  reorder_apply_out(*this, ztmp.get(), z);
-}
-
-void reorder_setup(PrecBase&, const Csr&) {
-  throw Error(SAP_ERR_UNSUPPORTED, "reordering is not available yet");
-}
-void reorder_apply_in(PrecBase&, const double*, double*) {}
-void reorder_apply_out(PrecBase&, const double*, double*) {}
 
 }  // namespace sapb
 
@@ -1010,7 +1174,7 @@ int sap_solver_setup_csr(sap_solver* h, const sap_csr* A) {
         for (int p = A->c.rp_h[i]; p < A->c.rp_h[i + 1]; p++) K = std::max(K, std::abs(i - A->c.ci_h[p]));
       pc.setup_csr_direct(A->c, K);
     } else {
-      reorder_setup(pc, A->c);
+      pc.setup_sparse(A->c);
     }
     SAPB_CUDA(cudaStreamSynchronize(pc.st));
     S.n = pc.n;
@@ -1098,6 +1262,24 @@ int sap_solver_info(const sap_solver* h, int* n, int* k, int* P) {
     if (n) *n = h->s->pcp->n;
     if (k) *k = h->s->pcp->K;
     if (P) *P = h->s->pcp->P;
+  });
+}
+
+int sap_solver_get_reorder(const sap_solver* h, int which, int* out, int64_t* count) {
+  SAP_TRY({
+    SAP_REQUIRE(h && count, "null argument");
+    const PrecBase& pc = *h->s->pcp;
+    const std::vector<int>* v = nullptr;
+    switch (which) {
+      case 0: v = &pc.db_row_perm_h; break;
+      case 1: v = &pc.final_pos_h; break;
+      case 2: v = &pc.final_order_h; break;
+      case 3: v = &pc.first_rows_h; break;
+      case 4: v = &pc.part_k_h; break;
+      default: throw Error(SAP_ERR_INVALID_ARGUMENT, "unknown reorder array");
+    }
+    *count = (int64_t)v->size();
+    if (out) std::copy(v->begin(), v->end(), out);
   });
 }
 
