@@ -42,7 +42,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC,-fopenmp", "-o", LIB, *objs, "-lgomp"]
+    cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC,-fopenmp", "-o", LIB, *objs, "-lgomp", "-lcublas",
+           "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -21,6 +21,7 @@
 #include "precond_kernels.cuh"
 #include "reorder.h"
 #include "reorder_pipeline.h"
+#include "wide_host.cuh"
 
 namespace sapb {
 
@@ -182,6 +183,71 @@ class PrecondT : public PrecBase {
   DBuf<T> sin_d, cout_d;  // DB row / column scales in band order (reordered path)
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
+  std::unique_ptr<WideBand<T>> wide;  // block (GEMM) path of wide bands
+
+  // Half-bandwidths from this value up are factored and applied as block
+  // tridiagonal partitions (wide_host.cuh); above 1024 that is the only
+  // path.  The environment variable SAPB_WIDE_MIN_K overrides the threshold.
+  static int wide_min_k() {
+    const char* e = std::getenv("SAPB_WIDE_MIN_K");
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? v : 256;
+  }
+  static bool use_wide(int kmax) { return kmax > 1024 || kmax >= wide_min_k(); }
+
+  // Boosting of the band factorization (partBandedLU and its variants,
+  // sap/precond.h:3882-3983): the variable-band kernels always boost; the
+  // constant-band kernels boost for K >= 70 (with more than one partition
+  // when decoupled) or when safeFactorization is set.
+  bool factor_boost() const {
+    if (var_band) return true;
+    if (!spike) return o.safeFactorization || (P > 1 && K >= 70);
+    return o.safeFactorization || K >= 70;
+  }
+
+  void wide_check_memory(int kmax) {
+    size_t fr = 0, tot = 0;
+    SAPB_CUDA(cudaMemGetInfo(&fr, &tot));
+    const double need = WideBand<T>::factor_bytes(n, P, kmax);
+    if (need > 0.92 * (double)fr)
+      throw Error(SAP_ERR_OUT_OF_MEMORY, "wide-band factors need " + std::to_string(need / 1e9) + " GB, " +
+                                             std::to_string((double)fr / 1e9) + " GB free");
+  }
+
+  // Interface unknowns of the variable band: the last K first-level rows of
+  // partition i and the first K of partition i+1, in band (second-level) order.
+  std::vector<int> var_iface(const rp::Pipeline<T>& pl) const {
+    std::vector<int> iface((size_t)(P - 1) * 2 * K);
+    for (int i = 0; i < P - 1; i++) {
+      const int e_i = parts_h[i].start + parts_h[i].size, s1 = parts_h[i + 1].start;
+      for (int k = 0; k < K; k++) {
+        iface[(size_t)i * 2 * K + k] = pl.second_pos[e_i - K + k];
+        iface[(size_t)i * 2 * K + K + k] = pl.second_pos[s1 + k];
+      }
+    }
+    return iface;
+  }
+
+  void wide_init(int kmax) {
+    wide_check_memory(kmax);
+    std::vector<int> ps(P), pz(P);
+    for (int p = 0; p < P; p++) {
+      ps[p] = parts_h[p].start;
+      pz[p] = parts_h[p].size;
+    }
+    wide = std::make_unique<WideBand<T>>();
+    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz);
+  }
+
+  // spikes and reduced system of the block path
+  void wide_couple(const std::vector<T>& oh, const std::vector<int>& iface) {
+    auto t0 = Clock::now();
+    wide->spikes(oh, iface, K);
+    t_assembly = ms_since(t0);
+    t0 = Clock::now();
+    wide->reduced(oh, iface, o.safeFactorization != 0);
+    t_fullLU = ms_since(t0);
+  }
 
   void setup_rowmajor(const double* A_dev, int n_, int K_) override {
     n = n_;
@@ -217,6 +283,7 @@ class PrecondT : public PrecBase {
   void setup_sparse(const Csr& A) override {
     if (o.dbFirstStageOnly) throw Error(SAP_ERR_UNSUPPORTED, "dbFirstStageOnly is not supported");
     if (o.ilu_level >= 0) throw Error(SAP_ERR_UNSUPPORTED, "ILU preconditioning is out of scope");
+    wide.reset();
     auto t0 = Clock::now();
     n = A.n;
     rp::Pipeline<T> pl;
@@ -326,6 +393,26 @@ class PrecondT : public PrecBase {
     }
     parts_d.upload(parts_h, st);
     partcol_d.upload(partcol, st);
+    if (use_wide(parts_maxK())) {
+      wide_init(parts_maxK());
+      std::vector<int> rows(pl.d_ci.size());
+      for (int i = 0; i < n; i++)
+        for (int e = pl.d_rp[i]; e < pl.d_rp[i + 1]; e++) rows[e] = i;
+      {
+        DBuf<int> drows, dcols;
+        DBuf<T> dvals;
+        drows.upload(rows, st);
+        dcols.upload(pl.d_ci, st);
+        dvals.upload(pl.d_val, st);
+        wide->load_coo(drows.get(), dcols.get(), dvals.get(), (long long)rows.size());
+      }
+      t_cpu_assemble = ms_since(t0) - t_reorder - t_transfer;
+      auto t2 = Clock::now();
+      wide->factor(true);
+      t_bandLU = ms_since(t2);
+      if (spike) wide_couple(pl.offd, var_iface(pl));
+      return;
+    }
     B.alloc((size_t)off);
     B.zero(st);
     {
@@ -350,15 +437,7 @@ class PrecondT : public PrecBase {
       t2 = Clock::now();
       const size_t KK = (size_t)K * K;
       offd.upload(pl.offd, st);
-      std::vector<int> iface((size_t)(P - 1) * 2 * K);
-      for (int i = 0; i < P - 1; i++) {
-        const int e_i = parts_h[i].start + parts_h[i].size, s1 = parts_h[i + 1].start;
-        for (int k = 0; k < K; k++) {
-          iface[(size_t)i * 2 * K + k] = pl.second_pos[e_i - K + k];
-          iface[(size_t)i * 2 * K + K + k] = pl.second_pos[s1 + k];
-        }
-      }
-      iface_d.upload(iface, st);
+      iface_d.upload(var_iface(pl), st);
       V.alloc(KK * (P - 1));
       W.alloc(KK * (P - 1));
       S.alloc(KK * (P - 1));
@@ -382,6 +461,7 @@ class PrecondT : public PrecBase {
   }
 
   void setup_from_band() {
+    wide.reset();
     ptype = o.precondType;
     spike = (ptype == SAP_PRECOND_SPIKE && P > 1);
     lu_ul = spike && o.factMethod == SAP_LU_UL;
@@ -397,6 +477,33 @@ class PrecondT : public PrecBase {
     }
     SAPB_CUDA(cudaStreamSynchronize(st));
     t_offDiags = ms_since(t0);
+    if (use_wide(K)) {
+      wide_init(K);
+      std::vector<long long> boff(P);
+      std::vector<int> kp(P, K);
+      for (int p = 0; p < P; p++) boff[p] = parts_h[p].boff;
+      wide->load_band(B.get(), boff, kp);
+      B.release();
+      t0 = Clock::now();
+      wide->factor(factor_boost());
+      t_bandLU = ms_since(t0);
+      if (spike) {
+        std::vector<T> oh;
+        offd.download(oh, st);
+        SAPB_CUDA(cudaStreamSynchronize(st));
+        offd.release();
+        std::vector<int> iface((size_t)(P - 1) * 2 * K);
+        for (int i = 0; i < P - 1; i++) {
+          const int s1 = parts_h[i + 1].start;
+          for (int k = 0; k < K; k++) {
+            iface[(size_t)i * 2 * K + k] = s1 - K + k;
+            iface[(size_t)i * 2 * K + K + k] = s1 + k;
+          }
+        }
+        wide_couple(oh, iface);
+      }
+      return;
+    }
     t0 = Clock::now();
     factor();
     SAPB_CUDA(cudaStreamSynchronize(st));
@@ -436,16 +543,11 @@ class PrecondT : public PrecBase {
   // partBandedLU / partBlockedBandedUL (sap/precond.h:3882-3983, 4336-4418, 4780-4846).
   void factor() {
     std::vector<FactorJob> jobs;
-    bool boost;
+    const bool boost = factor_boost();
     // the variable-band kernels always boost (partBlockedBandedLU_var, precond.h:4546-4631)
-    if (var_band) {
-      boost = true;
-      for (const auto& d : parts_h) jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 0, 0, 0, d.boff});
-    } else if (!spike) {
-      boost = o.safeFactorization || (P > 1 && K >= 70);
+    if (var_band || !spike) {
       for (const auto& d : parts_h) jobs.push_back(FactorJob{d.start, d.start + d.size, d.K, 0, 0, 0, d.boff});
     } else {
-      boost = o.safeFactorization || K >= 70;
       int nlu = lu_ul ? P - 1 : P;
       for (int p = 0; p < nlu; p++) {
         const auto& d = parts_h[p];
@@ -614,6 +716,11 @@ class PrecondT : public PrecBase {
       if (reordered) throw Error(SAP_ERR_UNSUPPORTED, "a diagonal matrix after reordering is not supported");
       k_diag_apply<T><<<grid_for(n, 256), 256, 0, st>>>(B.get(), v, z, n);
       SAPB_LAUNCHED();
+      return;
+    }
+    if (wide) {
+      wide->apply(v, z, reordered ? gin_d.get() : nullptr, reordered ? sin_d.get() : nullptr,
+                  reordered ? sout_d.get() : nullptr, reordered ? cout_d.get() : nullptr);
       return;
     }
     if (spike) {

@@ -1,0 +1,248 @@
+// Wide-band partitions (half-bandwidth of hundreds to thousands): every
+// partition is treated as block tridiagonal with bs x bs blocks (bs >= K_p),
+//     A_p = tridiag(F_{i-1}, D_i, E_i),
+// and factored without pivoting blockwise:
+//     D_i <- D_i - L_{i,i-1} U_{i-1,i};  D_i = L_ii U_ii;
+//     U_{i,i+1} = L_ii^-1 E_i;  L_{i+1,i} = F_i U_ii^-1.
+// These are exactly the L and U factors of the band LU (the LU without
+// pivoting is unique), computed as dense block operations: the diagonal block
+// LU is recursive and also returns L_ii^-1 and U_ii^-1, so every step except
+// a 32x32 leaf is a matrix product.  The apply then reduces to batched
+// matrix-vector products per block row:
+//     y_i = L_ii^-1 (f_i - L_{i,i-1} y_{i-1}),  x_i = U_ii^-1 (y_i - U_{i,i+1} x_{i+1}).
+// Blocks are column-major (element (r, c) at c*bs + r); vectors are padded to
+// nb*bs rows per partition, padding rows carry an identity diagonal.
+#pragma once
+
+#include "common.cuh"
+
+namespace sapb {
+
+constexpr int kLeaf = 32;
+
+// COO entries of the diagonal blocks (row j, col l in band order) into the
+// blocks of their partition: D (slot Dm), E = A_{i,i+1} (slot Em), F = A_{i+1,i} (slot Fm).
+template <typename T>
+__global__ void k_wb_scatter(const int* __restrict__ rows, const int* __restrict__ cols, const T* __restrict__ vals,
+                             long long nz, const int* __restrict__ part_of_row, const int* __restrict__ pstart,
+                             const int* __restrict__ psize, int bs, int nb, T* __restrict__ Dm, T* __restrict__ Em, T* __restrict__ Fm) {
+  const long long BB = (long long)bs * bs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nz;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int j = rows[e], l = cols[e];
+    const int p = part_of_row[j];
+    const int a = j - pstart[p], c = l - pstart[p];
+    if (c < 0 || c >= psize[p]) continue;  // outside the partition's diagonal block
+    const int bi = a / bs, bj = c / bs;
+    const long long off = (long long)(c - bj * bs) * bs + (a - bi * bs);
+    if (bi == bj) Dm[((long long)p * nb + bi) * BB + off] = vals[e];
+    else if (bj == bi + 1) Em[((long long)p * (nb - 1) + bi) * BB + off] = vals[e];
+    else if (bj + 1 == bi) Fm[((long long)p * (nb - 1) + bj) * BB + off] = vals[e];
+  }
+}
+
+// Identity diagonal on the padding rows [psize_p, nb*bs) of every partition.
+template <typename T>
+__global__ void k_wb_pad(T* __restrict__ Dm, const int* __restrict__ psize, int bs, int nb) {
+  const int p = blockIdx.y;
+  const long long BB = (long long)bs * bs;
+  for (int r = psize[p] + blockIdx.x * blockDim.x + threadIdx.x; r < nb * bs; r += gridDim.x * blockDim.x) {
+    const int bi = r / bs, q = r - bi * bs;
+    Dm[((long long)p * nb + bi) * BB + (long long)q * bs + q] = T(1);
+  }
+}
+
+// Band storage (column-major, 2K_p+1 rows per column, element (i, j) of a
+// partition at boff + (j-start)*(2K_p+1) + K_p + (i-j)) into the blocks.
+template <typename T>
+__global__ void k_wb_from_band(const T* __restrict__ B, const long long* __restrict__ boff,
+                               const int* __restrict__ kp, const int* __restrict__ psize, int bs, int nb,
+                               T* __restrict__ Dm, T* __restrict__ Em, T* __restrict__ Fm) {
+  const int p = blockIdx.y;
+  const int Kp = kp[p], sz = psize[p];
+  const long long SW = 2LL * Kp + 1, BB = (long long)bs * bs;
+  const T* Bp = B + boff[p];
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)sz * SW;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e / SW);
+    const int a = c + (int)(e - (long long)c * SW) - Kp;
+    if (a < 0 || a >= sz) continue;
+    const T v = Bp[e];
+    if (v == T(0)) continue;
+    const int bi = a / bs, bj = c / bs;
+    const long long off = (long long)(c - bj * bs) * bs + (a - bi * bs);
+    if (bi == bj) Dm[((long long)p * nb + bi) * BB + off] = v;
+    else if (bj == bi + 1) Em[((long long)p * (nb - 1) + bi) * BB + off] = v;
+    else if (bj + 1 == bi) Fm[((long long)p * (nb - 1) + bj) * BB + off] = v;
+  }
+}
+
+// Batched copy of an m x n sub-matrix (column-major, leading dimensions lds/ldd).
+template <typename T>
+__global__ void k_sub_copy(const T* __restrict__ src, int lds, long long ss, T* __restrict__ dst, int ldd,
+                           long long sd, int m, int n, T scale) {
+  const int b = blockIdx.z;
+  for (int c = blockIdx.y; c < n; c += gridDim.y)
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+      dst[b * sd + (long long)c * ldd + r] = scale * src[b * ss + (long long)c * lds + r];
+}
+
+// Leaf of the recursive LU: an n x n (n <= 32) diagonal block factored in
+// place without pivoting (the reference's boosting rule when `boost`), and
+// its L^-1 (unit lower) and U^-1 (upper) written to Li / Ui.  One CTA of 32
+// threads per batch element; thread r owns row r.
+template <typename T>
+__global__ void __launch_bounds__(32) k_leaf_lu(T* __restrict__ M, T* __restrict__ Li, T* __restrict__ Ui, int ld,
+                                                long long stride, int n, int boost, int* __restrict__ zero_flag) {
+  __shared__ T a[kLeaf][kLeaf + 1];
+  __shared__ T li[kLeaf][kLeaf + 1];
+  __shared__ T ui[kLeaf][kLeaf + 1];
+  const int r = threadIdx.x;
+  T* Mb = M + blockIdx.x * stride;
+  T* Lb = Li + blockIdx.x * stride;
+  T* Ub = Ui + blockIdx.x * stride;
+  for (int c = 0; c < n; c++) a[r][c] = (r < n) ? Mb[(long long)c * ld + r] : T(0);
+  __syncwarp();
+  for (int j = 0; j < n; j++) {
+    T p = a[j][j];
+    if (boost) p = boost_pivot(p);
+    else if (r == 0 && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
+    __syncwarp();
+    if (r == j) a[j][j] = p;
+    if (r > j && r < n) {
+      const T l = a[r][j] / p;
+      a[r][j] = l;
+      for (int c = j + 1; c < n; c++) a[r][c] -= l * a[j][c];
+    }
+    __syncwarp();
+  }
+  // inverses: column r of L^-1 by forward substitution, row r of U^-1 by
+  // backward substitution (each thread independent)
+  if (r < n) {
+    for (int i = 0; i < n; i++) li[i][r] = (i == r) ? T(1) : T(0);
+    for (int i = r + 1; i < n; i++) {
+      T s = T(0);
+      for (int k = r; k < i; k++) s += a[i][k] * li[k][r];
+      li[i][r] = -s;
+    }
+    for (int c = 0; c < n; c++) ui[r][c] = T(0);
+  }
+  __syncwarp();
+  // U^-1 column by column: column c solved by thread c
+  if (r < n) {
+    const int c = r;
+    ui[c][c] = T(1) / a[c][c];
+    for (int i = c - 1; i >= 0; i--) {
+      T s = T(0);
+      for (int k = i + 1; k <= c; k++) s += a[i][k] * ui[k][c];
+      ui[i][c] = -s / a[i][i];
+    }
+  }
+  __syncwarp();
+  if (r < n)
+    for (int c = 0; c < n; c++) {
+      Mb[(long long)c * ld + r] = a[r][c];
+      Lb[(long long)c * ld + r] = li[r][c];
+      Ub[(long long)c * ld + r] = ui[r][c];
+    }
+}
+
+// Batched dense matrix-vector product with an n x n column-major block:
+//   y = A x            (mode 0)
+//   y = c - A x        (mode 1)
+// one thread per row, x staged in shared memory in tiles.  Batch b uses
+// A + b*sA, x + b*sx, c + b*sc, y + b*sy (c may alias y).
+template <typename T>
+__global__ void __launch_bounds__(256) k_bgemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c,
+                                               long long sc, T* y, long long sy, int n, int mode) {
+  __shared__ T xs[256];
+  const int b = blockIdx.y;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const T* Ab = A + b * sA;
+  const T* xb = x + b * sx;
+  T acc = T(0);
+  for (int k0 = 0; k0 < n; k0 += 256) {
+    const int kk = k0 + threadIdx.x;
+    xs[threadIdx.x] = kk < n ? xb[kk] : T(0);
+    __syncthreads();
+    if (r < n) {
+      const int kend = min(256, n - k0);
+      const T* col = Ab + (long long)k0 * ld + r;
+#pragma unroll 8
+      for (int k = 0; k < kend; k++) acc += col[(long long)k * ld] * xs[k];
+    }
+    __syncthreads();
+  }
+  if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - acc : acc;
+}
+
+// Band-order vector <-> padded block vectors of the partitions.
+template <typename T>
+__global__ void k_wb_to_blocks(const T* __restrict__ v, T* __restrict__ out, const int* __restrict__ pstart,
+                               const int* __restrict__ psize, long long plen) {
+  const int p = blockIdx.y;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < plen; r += (long long)gridDim.x * blockDim.x)
+    out[p * plen + r] = r < psize[p] ? v[pstart[p] + r] : T(0);
+}
+template <typename T>
+__global__ void k_wb_from_blocks(const T* __restrict__ in, T* __restrict__ v, const int* __restrict__ pstart,
+                                 const int* __restrict__ psize, long long plen) {
+  const int p = blockIdx.y;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < psize[p];
+       r += (long long)gridDim.x * blockDim.x)
+    v[pstart[p] + r] = in[p * plen + r];
+}
+
+
+// dst[idx[e]] = vals[e]  /  dst[e] = src[idx[e]]   (64-bit indices; idx < 0 gives 0)
+template <typename T>
+__global__ void k_scatter_idx(const long long* __restrict__ idx, const T* __restrict__ vals, long long m,
+                              T* __restrict__ dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    dst[idx[e]] = vals[e];
+}
+template <typename T>
+__global__ void k_gather_idx(const T* __restrict__ src, const long long* __restrict__ idx, long long m,
+                             T* __restrict__ dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    dst[e] = idx[e] >= 0 ? src[idx[e]] : T(0);
+}
+
+// leftTrans into the band-order right-hand side: F[row] = T(v[gin[row]]) * sin[row]
+template <typename T>
+__global__ void k_wb_in(const double* __restrict__ v, const int* __restrict__ gin, const T* __restrict__ sin,
+                        T* __restrict__ F, int n) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    F[r] = gin ? (T)v[gin[r]] * sin[r] : (T)v[r];
+}
+// rightTrans out of the padded block vectors: z[sout[row]] = x(row) * cout[row]
+template <typename T>
+__global__ void k_wb_out(const T* __restrict__ xb, const int* __restrict__ rowpart, const int* __restrict__ pstart,
+                         long long plen, const int* __restrict__ sout, const T* __restrict__ cout,
+                         double* __restrict__ z, int n) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int p = rowpart[r];
+    const T x = xb[p * plen + (r - pstart[p])];
+    if (sout) z[sout[r]] = (double)(x * cout[r]);
+    else z[r] = (double)x;
+  }
+}
+
+// dst[didx[e]] = src[sidx[e]]
+template <typename T>
+__global__ void k_move_idx(const T* __restrict__ src, const long long* __restrict__ sidx,
+                           const long long* __restrict__ didx, long long m, T* __restrict__ dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    dst[didx[e]] = src[sidx[e]];
+}
+
+// S = I (K x K column-major per batch element)
+template <typename T>
+__global__ void k_identity(T* __restrict__ S, int K, long long stride) {
+  const int b = blockIdx.y;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)K * K;
+       e += (long long)gridDim.x * blockDim.x)
+    S[b * stride + e] = (e % K == e / K) ? T(1) : T(0);
+}
+
+}  // namespace sapb

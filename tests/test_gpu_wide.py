@@ -1,0 +1,76 @@
+"""The wide-band block path (half-bandwidth from 256 up by default, and every
+band above 1024) against the oracle through the C ABI.
+
+The block path factors each partition as block tridiagonal with dense block
+LUs; the factors equal the band LU's up to rounding, so applies are held to
+the same relative 2-norm tolerances as the narrow path (1e-10 FP64, 2e-4
+FP32 preconditioner) and FP64 solves to the reference's criterion
+||b - A x|| <= relTol ||b||.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+import oracle
+import saplibrary_b200 as sap
+from tests.helpers import band_to_scipy
+from tests.test_gpu_parity import APPLY_TOL, apply_gpu, setup_pair
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+WIDE_CASES = [  # n, K, P, d, dist, fact, precond type
+    (20000, 300, 4, 1.0, 1, sap.LU_UL, sap.Spike),
+    (24011, 257, 5, 0.8, 2, sap.LU_only, sap.Spike),  # ragged partitions, padded last block
+    (7000, 300, 1, 1.0, 1, sap.LU_UL, sap.Spike),     # one partition: no reduced system
+    (12000, 280, 4, 1.0, 0, sap.LU_UL, sap.Block),    # decoupled partitions
+    (6600, 1100, 2, 1.0, 1, sap.LU_UL, sap.Spike),    # above the narrow kernels' limit
+]
+
+
+@pytest.mark.parametrize("dtype", ["double", "float"])
+@pytest.mark.parametrize("n,K,P,d,dist,fact,ptype", WIDE_CASES)
+def test_wide_apply_matches_oracle(n, K, P, d, dist, fact, ptype, dtype):
+    band = sap.generate_band_host(n, K, d, dist, seed=n + K)
+    A, s, o = setup_pair(band, n, K, P, dtype, fact, ptype)
+    assert s.info() == o.info()
+    rng = np.random.default_rng(K)
+    for _ in range(2):
+        v = rng.standard_normal(n)
+        z = apply_gpu(s, v)
+        zo = o.apply(v)
+        assert np.all(np.isfinite(z))
+        rel = np.linalg.norm(z - zo) / np.linalg.norm(zo)
+        assert rel <= APPLY_TOL[dtype], rel
+
+
+def test_threshold_override_runs_block_path_on_narrow_band(monkeypatch):
+    n, K, P = 30011, 50, 10
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=n + K)
+    v = np.random.default_rng(1).standard_normal(n)
+    _, s_narrow, o = setup_pair(band, n, K, P, "double")
+    monkeypatch.setenv("SAPB_WIDE_MIN_K", "32")
+    _, s_wide, _ = setup_pair(band, n, K, P, "double")
+    zo = o.apply(v)
+    for s in (s_narrow, s_wide):
+        z = apply_gpu(s, v)
+        assert np.linalg.norm(z - zo) / np.linalg.norm(zo) <= 1e-10
+
+
+def test_wide_fp64_solve_matches_oracle_and_direct():
+    n, K, P = 40000, 300, 8
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=11)
+    xt = np.ones(n)
+    b = oracle.spmv_banded(band, n, K, xt)
+    A, s, o = setup_pair(band, n, K, P, "double")
+    x = np.zeros(n)
+    ok = s.solve(sap.MVBanded(A), b, x)
+    xo, res = o.solve(b, band=band, K=K, L=2, maxit=100, reltol=1e-10)
+    assert ok and res.code == 1
+    assert s.getMonitorCode() == 1
+    st = s.getStats()
+    assert st.relResidualNorm <= 1e-10
+    assert abs(st.numIterations - res.iterations) <= 0.5
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-9
+    xd = sl.solve_banded((K, K), band_to_scipy(band, n, K), b)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
