@@ -260,7 +260,7 @@ class BandedMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.sap_banded_destroy(h)
             self._h = None
 
@@ -283,7 +283,7 @@ class CsrMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.sap_csr_destroy(h)
             self._h = None
 
@@ -299,7 +299,7 @@ class _Spmv:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.sap_spmv_destroy(h)
             self._h = None
 
@@ -418,7 +418,7 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and _lib is not None:
             _lib.sap_solver_destroy(h)
             self._h = None
 

@@ -240,13 +240,15 @@ class PrecondT : public PrecBase {
   }
 
   // spikes and reduced system of the block path
-  void wide_couple(const std::vector<T>& oh, const std::vector<int>& iface) {
+  // (offd: the row-major coupling blocks on the device, released afterwards)
+  void wide_couple(const std::vector<int>& iface) {
     auto t0 = Clock::now();
-    wide->spikes(oh, iface, K);
+    wide->spikes(offd.get(), iface, K);
     t_assembly = ms_since(t0);
     t0 = Clock::now();
-    wide->reduced(oh, iface, o.safeFactorization != 0);
+    wide->reduced(offd.get(), iface, o.safeFactorization != 0);
     t_fullLU = ms_since(t0);
+    offd.release();
   }
 
   void setup_rowmajor(const double* A_dev, int n_, int K_) override {
@@ -410,7 +412,10 @@ class PrecondT : public PrecBase {
       auto t2 = Clock::now();
       wide->factor(true);
       t_bandLU = ms_since(t2);
-      if (spike) wide_couple(pl.offd, var_iface(pl));
+      if (spike) {
+        offd.upload(pl.offd, st);
+        wide_couple(var_iface(pl));
+      }
       return;
     }
     B.alloc((size_t)off);
@@ -488,10 +493,6 @@ class PrecondT : public PrecBase {
       wide->factor(factor_boost());
       t_bandLU = ms_since(t0);
       if (spike) {
-        std::vector<T> oh;
-        offd.download(oh, st);
-        SAPB_CUDA(cudaStreamSynchronize(st));
-        offd.release();
         std::vector<int> iface((size_t)(P - 1) * 2 * K);
         for (int i = 0; i < P - 1; i++) {
           const int s1 = parts_h[i + 1].start;
@@ -500,7 +501,7 @@ class PrecondT : public PrecBase {
             iface[(size_t)i * 2 * K + K + k] = s1 + k;
           }
         }
-        wide_couple(oh, iface);
+        wide_couple(iface);
       }
       return;
     }

@@ -176,6 +176,119 @@ __global__ void __launch_bounds__(256) k_bgemv(const T* A, int ld, long long sA,
   if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - acc : acc;
 }
 
+// Batched matrix-vector product over n x n column-major blocks, for the
+// block sweeps and the reduced system:
+//   y = A x (mode 0),  y = c - A x (mode 1; c may alias y),
+// with tri = 1 (lower: row r reads columns <= r), 2 (upper: columns >= r)
+// or 0 (all).  Skipped entries are exact zeros of the factors, so the
+// triangular forms read half the bytes.  A CTA of 8 warps owns 64-row tiles
+// (lane rows r0+lane and r0+32+lane: every load instruction is a coalesced
+// 256-byte column segment), its warps split the columns and reduce in
+// shared memory in a fixed order.  Tiles are paired j with (T-1-j) so
+// triangular work is the same for every CTA.  Batch b uses A + b*sA,
+// x + b*sx, c + b*sc, y + b*sy.
+constexpr int kGemvRows = 64, kGemvWarps = 8;
+template <typename T>
+__global__ void __launch_bounds__(256) k_tgemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c,
+                                               long long sc, T* y, long long sy, int n, int mode, int tri) {
+  __shared__ T part[kGemvWarps][kGemvRows];
+  const int b = blockIdx.y;
+  const int ntile = (n + kGemvRows - 1) / kGemvRows;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const T* Ab = A + b * sA;
+  const T* xb = x + b * sx;
+  for (int half = 0; half < 2; half++) {
+    const int tile = half == 0 ? (int)blockIdx.x : ntile - 1 - (int)blockIdx.x;
+    if (half == 1 && tile <= (int)blockIdx.x) break;
+    const int r0 = tile * kGemvRows;
+    int c0 = 0, c1 = n;
+    if (tri == 1) c1 = min(n, r0 + kGemvRows);
+    else if (tri == 2) c0 = r0;
+    const int ra = r0 + lane, rb = r0 + 32 + lane;
+    const bool va = ra < n, vb = rb < n;
+    T acc0 = T(0), acc1 = T(0);
+#pragma unroll 4
+    for (int col = c0 + w; col < c1; col += kGemvWarps) {
+      const T xv = xb[col];
+      const T* cp = Ab + (long long)col * ld;
+      if (va) acc0 += cp[ra] * xv;
+      if (vb) acc1 += cp[rb] * xv;
+    }
+    part[w][lane] = acc0;
+    part[w][32 + lane] = acc1;
+    __syncthreads();
+    if (threadIdx.x < kGemvRows) {
+      const int r = r0 + threadIdx.x;
+      T s = T(0);
+#pragma unroll
+      for (int q = 0; q < kGemvWarps; q++) s += part[q][threadIdx.x];
+      if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+    }
+    __syncthreads();
+  }
+}
+
+// Nonzero columns of the coupling blocks: flag[blk][c] = any row of column c
+// of row-major K x K block blk (blk = 2t + which) is nonzero.
+template <typename T>
+__global__ void k_nz_cols(const T* __restrict__ offd, int K, int* __restrict__ flag) {
+  const int blk = blockIdx.y;
+  const long long KK = (long long)K * K;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < K; c += gridDim.x * blockDim.x) {
+    const T* M = offd + blk * KK + c;
+    int nz = 0;
+    for (int r = 0; r < K && !nz; r++) nz = M[(long long)r * K] != T(0);
+    flag[(long long)blk * K + c] = nz;
+  }
+}
+
+// Right-hand sides of the spike solves: column jj of interface t's slab is
+// coupling-block column cols[t][j0+jj], placed at the interface rows
+// pos[t][k] of the partition's block vector (X pre-zeroed).
+template <typename T>
+__global__ void k_spike_rhs(const T* __restrict__ offd, int which, int K, const int* __restrict__ cols, int ncol,
+                            int j0, const int* __restrict__ pos, T* __restrict__ X, long long sX, long long plen) {
+  const int jj = blockIdx.x, t = blockIdx.y;
+  const int col = (j0 + jj < ncol) ? cols[(long long)t * ncol + j0 + jj] : -1;
+  if (col < 0) return;
+  const long long KK = (long long)K * K;
+  const T* M = offd + (2LL * t + which) * KK + col;
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    X[t * sX + jj * plen + pos[(long long)t * K + k]] = M[(long long)k * K];
+}
+
+// Spike tips out of the solved slab: out[t][col][k] (column-major K x K).
+template <typename T>
+__global__ void k_spike_tips(const T* __restrict__ X, long long sX, long long plen, const int* __restrict__ cols,
+                             int ncol, int j0, const int* __restrict__ pos, int K, T* __restrict__ out) {
+  const int jj = blockIdx.x, t = blockIdx.y;
+  const int col = (j0 + jj < ncol) ? cols[(long long)t * ncol + j0 + jj] : -1;
+  if (col < 0) return;
+  const long long KK = (long long)K * K;
+  for (int k = threadIdx.x; k < K; k += blockDim.x)
+    out[t * KK + (long long)col * K + k] = X[t * sX + jj * plen + pos[(long long)t * K + k]];
+}
+
+// Row-major coupling block (2t + which) -> column-major out[t], via 32x32 tiles.
+template <typename T>
+__global__ void k_couple_colmajor(const T* __restrict__ offd, int which, int K, T* __restrict__ out) {
+  __shared__ T tile[32][33];
+  const int t = blockIdx.z;
+  const long long KK = (long long)K * K;
+  const T* M = offd + (2LL * t + which) * KK;
+  T* O = out + t * KK;
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < K && c < K) ? M[(long long)r * K + c] : T(0);
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (r < K && c < K) O[(long long)c * K + r] = tile[threadIdx.x][i];
+  }
+}
+
 // Band-order vector <-> padded block vectors of the partitions.
 template <typename T>
 __global__ void k_wb_to_blocks(const T* __restrict__ v, T* __restrict__ out, const int* __restrict__ pstart,

@@ -246,13 +246,17 @@ class WideBand {
     if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
   }
 
+  // tri: 0 full, 1 lower, 2 upper (see k_tgemv)
   void gemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y, long long sy,
-            int m, int nbatch, int mode) {
-    k_bgemv<T><<<dim3((m + 255) / 256, nbatch), 256, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode);
+            int m, int nbatch, int mode, int tri) {
+    const int ntile = (m + kGemvRows - 1) / kGemvRows;
+    k_tgemv<T><<<dim3((ntile + 1) / 2, nbatch), 256, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri);
     SAPB_LAUNCHED();
   }
 
-  // x <- A_p^-1 x for the padded block vectors of all partitions
+  // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
+  // and U_{i,i+1} = L_ii^-1 E_i are lower triangular, U_ii^-1 and
+  // L_{i+1,i} = F_i U_ii^-1 upper triangular (the band fits in one block).
   void solve_blocks(T* x) {
     T* y = yv.get();
     T* t = tv.get();
@@ -261,22 +265,36 @@ class WideBand {
       const T* rhs = x + (long long)i * bs;
       if (i > 0) {
         gemv(Loff.get() + (long long)(i - 1) * BB, bs, (long long)(nb - 1) * BB, y + (long long)(i - 1) * bs, sv,
-             x + (long long)i * bs, sv, t, sv, bs, P, 1);
+             x + (long long)i * bs, sv, t, sv, bs, P, 1, 2);
         rhs = t;
       }
       gemv(Linv.get() + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, y + (long long)i * bs, sv, bs,
-           P, 0);
+           P, 0, 1);
     }
     for (int i = nb - 1; i >= 0; i--) {  // x_i = U_ii^-1 (y_i - U_{i,i+1} x_{i+1})
       const T* rhs = y + (long long)i * bs;
       if (i < nb - 1) {
         gemv(Uoff.get() + (long long)i * BB, bs, (long long)(nb - 1) * BB, x + (long long)(i + 1) * bs, sv,
-             y + (long long)i * bs, sv, t, sv, bs, P, 1);
+             y + (long long)i * bs, sv, t, sv, bs, P, 1, 1);
         rhs = t;
       }
       gemv(Uinv.get() + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, x + (long long)i * bs, sv, bs,
-           P, 0);
+           P, 0, 2);
     }
+  }
+
+  // Interface positions inside the partitions' block vectors: pos[t][k] for
+  // the bottom (which 0, partition t) or top (which 1, partition t+1) unknowns.
+  std::vector<int> iface_pos(const std::vector<int>& iface, int which) const {
+    const int nI = P - 1;
+    std::vector<int> pos((size_t)nI * K);
+    for (int t = 0; t < nI; t++)
+      for (int k = 0; k < K; k++) {
+        const int q = iface[(size_t)t * 2 * K + (size_t)which * K + k] - pstart_h[t + which];
+        if (q < 0 || q >= psize_h[t + which]) throw Error(SAP_ERR_INVALID_ARGUMENT, "interface row outside its partition");
+        pos[(size_t)t * K + k] = q;
+      }
+    return pos;
   }
 
   // Spike tips of every interface t (column-major K x K):
@@ -284,9 +302,10 @@ class WideBand {
   //   W_t = rows at the top interface unknowns of A_{t+1}^-1 [.. C_t ..],
   // by block solves whose right-hand sides are the coupling blocks' nonzero
   // columns, batched over the interfaces (slabs of columns bound the memory).
-  // offd: row-major coupling blocks, B_t at 2t, C_t at 2t+1; iface: [P-1][2K]
-  // band rows, bottom unknowns of partition t then top unknowns of t+1.
-  void spikes(const std::vector<T>& offd, const std::vector<int>& iface, int K_) {
+  // offd (device): row-major coupling blocks, B_t at 2t, C_t at 2t+1;
+  // iface: [P-1][2K] band rows, bottom unknowns of partition t, then top
+  // unknowns of partition t+1.
+  void spikes(const T* offd, const std::vector<int>& iface, int K_) {
     K = K_;
     spike = true;
     const int nI = P - 1;
@@ -295,26 +314,37 @@ class WideBand {
     Wc.alloc((size_t)nI * KK);
     Vc.zero(st);
     Wc.zero(st);
-    auto pos_of = [&](int t, int which, int k) {
-      return iface[(size_t)t * 2 * K + (size_t)which * K + k] - pstart_h[t + which];
-    };
+    std::vector<int> nzh;
+    {
+      DBuf<int> nzd;
+      nzd.alloc((size_t)2 * nI * K);
+      k_nz_cols<T><<<dim3(grid1d(K, 256, 64), 2 * nI), 256, 0, st>>>(offd, K, nzd.get());
+      SAPB_LAUNCHED();
+      nzd.download(nzh, st);
+      SAPB_CUDA(cudaStreamSynchronize(st));
+    }
     // the X slab holds nI * plen * cs values
     const double budget = 8.0e9;
     const int cs_max = (int)std::max<double>(32.0, std::min<double>(K, budget / ((double)nI * plen * sizeof(T))));
     for (int which = 0; which < 2; which++) {
-      std::vector<std::vector<int>> cols(nI);
+      const std::vector<int> pos = iface_pos(iface, which);
       int ncol = 0, minpos = (int)plen;
+      std::vector<int> cnt(nI, 0);
       for (int t = 0; t < nI; t++) {
-        const T* Mt = offd.data() + (size_t)(2 * t + which) * KK;
-        for (int c = 0; c < K; c++) {
-          bool nz = false;
-          for (int r = 0; r < K && !nz; r++) nz = Mt[(size_t)r * K + c] != T(0);
-          if (nz) cols[t].push_back(c);
-        }
-        ncol = std::max(ncol, (int)cols[t].size());
-        for (int k = 0; k < K; k++) minpos = std::min(minpos, pos_of(t, which, k));
+        for (int c = 0; c < K; c++) cnt[t] += nzh[(size_t)(2 * t + which) * K + c];
+        ncol = std::max(ncol, cnt[t]);
+        for (int k = 0; k < K; k++) minpos = std::min(minpos, pos[(size_t)t * K + k]);
       }
       if (ncol == 0) continue;
+      std::vector<int> cols((size_t)nI * ncol, -1);
+      for (int t = 0; t < nI; t++) {
+        int j = 0;
+        for (int c = 0; c < K; c++)
+          if (nzh[(size_t)(2 * t + which) * K + c]) cols[(size_t)t * ncol + j++] = c;
+      }
+      DBuf<int> cols_d, pos_d;
+      cols_d.upload(cols, st);
+      pos_d.upload(pos, st);
       const int cs = std::min(ncol, cs_max);
       const long long sX = plen * cs;
       DBuf<T> X, Wt;
@@ -331,37 +361,13 @@ class WideBand {
       auto Fk = [&](DBuf<T>& a, int per, int i) {
         return Mat<T>{a.get() + (long long)which * per * BB + (long long)i * BB, bs, (long long)per * BB};
       };
+      const int kt = std::min(1024, ((K + 31) / 32) * 32);
       for (int j0 = 0; j0 < ncol; j0 += cs) {
         const int w = std::min(cs, ncol - j0);
-        std::vector<long long> idx, sidx, didx;
-        std::vector<T> vals;
-        for (int t = 0; t < nI; t++) {
-          const T* Mt = offd.data() + (size_t)(2 * t + which) * KK;
-          for (int jj = 0; jj < w && j0 + jj < (int)cols[t].size(); jj++) {
-            const int c = cols[t][j0 + jj];
-            for (int k = 0; k < K; k++) {
-              const long long xpos = t * sX + (long long)jj * plen + pos_of(t, which, k);
-              const T v = Mt[(size_t)k * K + c];
-              if (v != T(0)) {
-                idx.push_back(xpos);
-                vals.push_back(v);
-              }
-              sidx.push_back(xpos);
-              didx.push_back(t * KK + (long long)c * K + k);
-            }
-          }
-        }
         X.zero(st);
-        if (!idx.empty()) {
-          DBuf<long long> di;
-          DBuf<T> dv;
-          di.upload(idx, st);
-          dv.upload(vals, st);
-          k_scatter_idx<T><<<grid1d((long long)idx.size()), 256, 0, st>>>(di.get(), dv.get(), (long long)idx.size(),
-                                                                           X.get());
-          SAPB_LAUNCHED();
-          SAPB_CUDA(cudaStreamSynchronize(st));
-        }
+        k_spike_rhs<T><<<dim3(w, nI), kt, 0, st>>>(offd, which, K, cols_d.get(), ncol, j0, pos_d.get(), X.get(), sX,
+                                                    plen);
+        SAPB_LAUNCHED();
         for (int i = ib0; i < nb; i++) {
           if (i > ib0) ops.gemm(bs, w, bs, T(-1), Fk(Loff, nb - 1, i - 1), Xb(i - 1), T(1), Xb(i));
           ops.gemm(bs, w, bs, T(1), Fk(Linv, nb, i), Xb(i), T(0), Wm);
@@ -372,34 +378,26 @@ class WideBand {
           ops.gemm(bs, w, bs, T(1), Fk(Uinv, nb, i), Xb(i), T(0), Wm);
           ops.copy(Wm, Xb(i), bs, w);
         }
-        if (!sidx.empty()) {
-          DBuf<long long> ds, dd;
-          ds.upload(sidx, st);
-          dd.upload(didx, st);
-          k_move_idx<T><<<grid1d((long long)sidx.size()), 256, 0, st>>>(X.get(), ds.get(), dd.get(),
-                                                                         (long long)sidx.size(),
-                                                                         which ? Wc.get() : Vc.get());
-          SAPB_LAUNCHED();
-          SAPB_CUDA(cudaStreamSynchronize(st));
-        }
+        k_spike_tips<T><<<dim3(w, nI), kt, 0, st>>>(X.get(), sX, plen, cols_d.get(), ncol, j0, pos_d.get(), K,
+                                                     which ? Wc.get() : Vc.get());
+        SAPB_LAUNCHED();
       }
+      SAPB_CUDA(cudaStreamSynchronize(st));
     }
   }
 
   // S_t = I - W_t V_t, factored with its triangular inverses (boosted only
   // when `boost`); coupling blocks kept column-major for the apply.
-  void reduced(const std::vector<T>& offd, const std::vector<int>& iface, bool boost) {
+  void reduced(const T* offd, const std::vector<int>& iface, bool boost) {
     const int nI = P - 1;
     const long long KK = (long long)K * K;
-    std::vector<T> Bh((size_t)nI * KK), Ch((size_t)nI * KK);
-    for (int t = 0; t < nI; t++)
-      for (int r = 0; r < K; r++)
-        for (int c = 0; c < K; c++) {
-          Bh[(size_t)t * KK + (size_t)c * K + r] = offd[(size_t)(2 * t) * KK + (size_t)r * K + c];
-          Ch[(size_t)t * KK + (size_t)c * K + r] = offd[(size_t)(2 * t + 1) * KK + (size_t)r * K + c];
-        }
-    Bc.upload(Bh, st);
-    Cc.upload(Ch, st);
+    Bc.alloc((size_t)nI * KK);
+    Cc.alloc((size_t)nI * KK);
+    const dim3 tg((K + 31) / 32, (K + 31) / 32, nI);
+    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 0, K, Bc.get());
+    SAPB_LAUNCHED();
+    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 1, K, Cc.get());
+    SAPB_LAUNCHED();
     DBuf<T> S, Ws;
     DBuf<int> sflag;
     S.alloc((size_t)nI * KK);
@@ -423,13 +421,15 @@ class WideBand {
     lu.gemm(K, K, K, T(-1), Mat<T>{Wc.get(), K, KK}, Mat<T>{Vc.get(), K, KK}, T(1), Sm);
     lu.rec(Sm, Mat<T>{SLi.get(), K, KK}, Mat<T>{SUi.get(), K, KK}, K);
     std::vector<long long> pos((size_t)nI * 2 * K), rows((size_t)nI * 2 * K);
-    for (int t = 0; t < nI; t++)
-      for (int k = 0; k < 2 * K; k++) {
-        const int p = t + (k >= K ? 1 : 0);
-        const int row = iface[(size_t)t * 2 * K + k];
-        pos[(size_t)t * 2 * K + k] = p * plen + (row - pstart_h[p]);
-        rows[(size_t)t * 2 * K + k] = row;
-      }
+    for (int which = 0; which < 2; which++) {
+      const std::vector<int> q = iface_pos(iface, which);
+      for (int t = 0; t < nI; t++)
+        for (int k = 0; k < K; k++) {
+          const size_t e = (size_t)t * 2 * K + (size_t)which * K + k;
+          pos[e] = (t + which) * plen + q[(size_t)t * K + k];
+          rows[e] = iface[e];
+        }
+    }
     ipos.upload(pos, st);
     irow.upload(rows, st);
     xbt.alloc((size_t)nI * 2 * K);
@@ -452,12 +452,12 @@ class WideBand {
     T* xt = xbt.get() + K;
     T* fb = fbt.get();
     T* ft = fbt.get() + K;
-    gemv(Wc.get(), K, KK, xb, s2, xt, s2, t1.get(), K, K, nI, 1);            // t1 = xt - W xb
-    gemv(SLi.get(), K, KK, t1.get(), K, nullptr, 0, t2.get(), K, K, nI, 0);  // t2 = L_S^-1 t1
-    gemv(SUi.get(), K, KK, t2.get(), K, nullptr, 0, t1.get(), K, K, nI, 0);  // z2 = U_S^-1 t2
-    gemv(Vc.get(), K, KK, t1.get(), K, xb, s2, t2.get(), K, K, nI, 1);       // z1 = xb - V z2
-    gemv(Bc.get(), K, KK, t1.get(), K, fb, s2, fb, s2, K, nI, 1);            // f_b -= B z2
-    gemv(Cc.get(), K, KK, t2.get(), K, ft, s2, ft, s2, K, nI, 1);            // f_t -= C z1
+    gemv(Wc.get(), K, KK, xb, s2, xt, s2, t1.get(), K, K, nI, 1, 0);            // t1 = xt - W xb
+    gemv(SLi.get(), K, KK, t1.get(), K, nullptr, 0, t2.get(), K, K, nI, 0, 1);  // t2 = L_S^-1 t1
+    gemv(SUi.get(), K, KK, t2.get(), K, nullptr, 0, t1.get(), K, K, nI, 0, 2);  // z2 = U_S^-1 t2
+    gemv(Vc.get(), K, KK, t1.get(), K, xb, s2, t2.get(), K, K, nI, 1, 0);       // z1 = xb - V z2
+    gemv(Bc.get(), K, KK, t1.get(), K, fb, s2, fb, s2, K, nI, 1, 0);            // f_b -= B z2
+    gemv(Cc.get(), K, KK, t2.get(), K, ft, s2, ft, s2, K, nI, 1, 0);            // f_t -= C z1
     k_scatter_idx<T><<<grid1d(m), 256, 0, st>>>(irow.get(), fbt.get(), m, F);
     SAPB_LAUNCHED();
   }
