@@ -59,7 +59,7 @@ enum { SAP_LU_UL = 0, SAP_LU_ONLY = 1 };
 enum { SAP_PRECOND_SPIKE = 0, SAP_PRECOND_BLOCK = 1, SAP_PRECOND_NONE = 2 };
 /* Preconditioner value type: the Solver's PrecValueType template argument
  * (sap/solver.h:153). */
-enum { SAP_PREC_FLOAT = 0, SAP_PREC_DOUBLE = 1 };
+enum { SAP_PREC_FLOAT = 0, SAP_PREC_DOUBLE = 1, SAP_PREC_TF32 = 2 };
 
 /* sap::Options (sap/solver.h:52-81); same fields, same defaults
  * (sap/solver.h:233-256).  Booleans are ints (0/1). */
@@ -85,6 +85,11 @@ typedef struct sap_options {
   int trackReordering;
   int useBCR;
   int ilu_level;
+  /* Extension (not in the reference): when > 0, solve() runs up to this many
+   * FP64 iterative-refinement sweeps r = b - A x, A d = r by BiCGStab(L)
+   * (stopping at the global tolerance, on stagnation or at the iteration
+   * budget), x += d.  0 (the default) runs the reference's single solve. */
+  int refinementSweeps;
 } sap_options;
 
 /* sap::Stats (sap/solver.h:89-140); times in milliseconds as in the
@@ -185,7 +190,10 @@ int sap_blas_dots_noalloc(int n, int nq, const double* const* x, const double* c
                           void* stream);
 
 /* ---- solver --------------------------------------------------------------- */
-/* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297). */
+/* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297).  prec_dtype
+ * is the preconditioner's PrecValueType: SAP_PREC_FLOAT or SAP_PREC_DOUBLE,
+ * or SAP_PREC_TF32 (FP32 storage whose wide-band block products run on the
+ * tensor cores in TF32 with FP32 accumulation; narrow bands as FP32). */
 int sap_solver_create(int num_partitions, const sap_options* opts, int prec_dtype,
                       sap_solver** out);
 int sap_solver_destroy(sap_solver* s);

@@ -63,7 +63,7 @@ class _COptions(ctypes.Structure):
                 ("gpuCount", ctypes.c_int), ("dropOffFraction", ctypes.c_double), ("factMethod", ctypes.c_int),
                 ("precondType", ctypes.c_int), ("safeFactorization", ctypes.c_int),
                 ("variableBandwidth", ctypes.c_int), ("trackReordering", ctypes.c_int), ("useBCR", ctypes.c_int),
-                ("ilu_level", ctypes.c_int)]
+                ("ilu_level", ctypes.c_int), ("refinementSweeps", ctypes.c_int)]
 
 
 _STAT_FIELDS = (["timeSetup", "timeUpdate", "timeSolve", "time_DB", "time_DB_pre", "time_DB_first",
@@ -183,6 +183,9 @@ def generate_band_host(n: int, k: int, d: float, dist: int = 1, seed: int = 0) -
 
 
 # ---- Options / Stats ------------------------------------------------------------
+_PREC = {"float": 0, "double": 1, "tf32": 2}
+
+
 @dataclass
 class Options:
     """sap::Options (sap/solver.h:52-81), defaults of sap/solver.h:233-256."""
@@ -207,6 +210,8 @@ class Options:
     trackReordering: bool = False
     useBCR: bool = False
     ilu_level: int = -1
+    # extension: FP64 refinement sweeps around BiCGStab(L) (0: the reference's solve)
+    refinementSweeps: int = 0
 
     def _c(self) -> _COptions:
         c = _COptions()
@@ -341,8 +346,9 @@ class Solver:
         self._opts = opts
         h = ctypes.c_void_p()
         copts = opts._c()
-        _check(_lib.sap_solver_create(int(numPartitions), ctypes.byref(copts), 0 if prec == "float" else 1,
-                                      ctypes.byref(h)))
+        if prec not in _PREC:
+            raise ValueError(f"prec must be one of {sorted(_PREC)}")
+        _check(_lib.sap_solver_create(int(numPartitions), ctypes.byref(copts), _PREC[prec], ctypes.byref(h)))
         self._h = h
 
     def setup(self, A) -> bool:

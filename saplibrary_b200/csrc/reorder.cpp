@@ -12,6 +12,7 @@
 #include "reorder_pipeline.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <limits>
@@ -402,7 +403,9 @@ template <typename T>
 void Pipeline<T>::assemble_coupling(int K, int P) {
   const int q = n / P, rem = n % P;
   const size_t KK = (size_t)K * K;
-  offd.assign(2 * KK * (P - 1), T(0));
+  offd_size = 2 * KK * (P - 1);
+  offd_idx.clear();
+  offd_val.clear();
   couples_right.assign(n, 0);
   d_rp.assign(n + 1, 0);
   d_ci.clear();
@@ -420,11 +423,13 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
         couples_right[j] = 1;
         const int row_end = q * pr + (pr < rem ? pr + q + 1 : rem + q);
         const int col_start = q * pc + (pc < rem ? pc : rem);
-        offd[pr * 2 * KK + (size_t)(j + K - row_end) * K + (l - col_start)] = m_val[e];
+        offd_idx.push_back((long long)(pr * 2 * KK + (size_t)(j + K - row_end) * K + (l - col_start)));
+        offd_val.push_back(m_val[e]);
       } else {
         const int row_start = q * pr + (pr < rem ? pr : rem);
         const int col_end = q * pc + (pc < rem ? pc + q + 1 : rem + q);
-        offd[(pc * 2 + 1) * KK + (size_t)(j - row_start) * K + (l - col_end + K)] = m_val[e];
+        offd_idx.push_back((long long)((pc * 2 + 1) * KK + (size_t)(j - row_start) * K + (l - col_end + K)));
+        offd_val.push_back(m_val[e]);
       }
     }
   }
@@ -446,10 +451,15 @@ void Pipeline<T>::second_level(int K, int P) {
   second_order.assign(n, 0);
   second_pos.assign(n, 0);
   std::vector<int> order(n, 0);
-  int nb = 0, e0 = 0;
-  for (int p = 0; p < P; p++) {
-    const int ne = nb + q + (p < rem ? 1 : 0);
-    const int e1 = d_rp[ne];
+  std::vector<int> pnb(P + 1, 0);
+  for (int p = 0; p < P; p++) pnb[p + 1] = pnb[p] + q + (p < rem ? 1 : 0);
+  // One partition.  Returns false, in the parallel pass, when a trial root
+  // leaves the partition (the reference's root search walks on to the next
+  // index): that trial's writes reach another partition, so every partition
+  // is then redone serially in order, as the reference does.
+  auto part = [&](int p, bool serial) -> bool {
+    const int nb = pnb[p], ne = pnb[p + 1];
+    const int e0 = d_rp[nb], e1 = d_rp[ne];
     for (int i = nb; i < ne; i++) second_order[i] = i;
     int best_bw = 0;
     for (int e = e0; e < e1; e++) best_bw = std::max(best_bw, std::abs(row[e] - d_ci[e]));
@@ -458,7 +468,7 @@ void Pipeline<T>::second_level(int K, int P) {
     std::vector<int> rowlen(ne - nb);
     for (int i = nb; i < ne; i++) rowlen[i - nb] = d_rp[i + 1] - d_rp[i];
     std::vector<char> tried(n, 0);
-    std::vector<int> pushed(ne, -1), level(n, 0);
+    std::vector<int> pushed(n, -1), level(n, 0);
     int last_level = 0, prev_last = 0;
     for (int trial = 0; trial < 5; trial++) {
       int root;
@@ -477,6 +487,7 @@ void Pipeline<T>::second_level(int K, int P) {
         }
         while (tried[root]) root = (root + 1) % n;
       }
+      if (!serial && (root < nb || root >= ne)) return false;
       tried[root] = 1;
       if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level)) break;
       for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
@@ -494,8 +505,14 @@ void Pipeline<T>::second_level(int K, int P) {
       if (best_bw <= 128) break;
     }
     for (int k = nb; k < ne; k++) second_pos[second_order[k]] = k;
-    nb = ne;
-    e0 = e1;
+    return true;
+  };
+  int ok = 1;
+#pragma omp parallel for schedule(dynamic, 1) reduction(&& : ok)
+  for (int p = 0; p < P; p++) ok = part(p, false) && ok;
+  if (!ok) {
+    second_pos.assign(n, 0);
+    for (int p = 0; p < P; p++) part(p, true);
   }
   std::vector<int> key(dz), col(dz);
   for (int e = 0; e < dz; e++) {
@@ -532,6 +549,13 @@ void Pipeline<T>::assemble_var_band(int P) {
 // up to the band layout.
 template <typename T>
 void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<double>& rowmax) {
+  stage_ms.clear();
+  auto t0 = std::chrono::steady_clock::now();
+  auto lap = [&](const char* name) {
+    auto t1 = std::chrono::steady_clock::now();
+    stage_ms.emplace_back(name, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  };
   if (do_db) {
     db(weight, rowmax);
   } else {
@@ -544,6 +568,7 @@ void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<doubl
   k_db = 0;
   for (int i = 0; i < n; i++)
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) k_db = std::max(k_db, std::abs(i - m_ci[e]));
+  lap("db");
   if (max_bandwidth > 64) {
     k_reorder = rcm();
   } else {
@@ -552,18 +577,23 @@ void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<doubl
     rcm_pos.resize(n);
     for (int i = 0; i < n; i++) rcm_order[i] = rcm_pos[i] = i;
   }
+  lap("rcm");
   if (k_reorder > max_bandwidth || drop_frac > 0) {
     K = drop_off((T)drop_frac, max_bandwidth);
   } else {
     K = k_reorder;
     drop_actual = T(0);
   }
+  lap("drop_off");
   P = std::min(P_req, std::max(n / (K + 1), 1));
   if (P == 1 || K == 0) var_band = false;
   if (var_band) {
     assemble_coupling(K, P);
+    lap("coupling");
     second_level(K, P);
+    lap("second_level");
     assemble_var_band(P);
+    lap("assemble");
   } else {
     second_order.resize(n);
     second_pos.resize(n);
@@ -575,6 +605,7 @@ void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<doubl
   final_order.resize(n);
   for (int k = 0; k < n; k++) final_order[k] = rcm_order[second_order[k]];
   for (int i = 0; i < n; i++) final_pos[i] = second_pos[rcm_pos[db_row_perm[i]]];
+  lap("compose");
 }
 
 template class Pipeline<float>;

@@ -4,6 +4,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/sap_b200.h"
@@ -42,7 +43,11 @@ class Pipeline {
   std::vector<int> second_order, second_pos;     // second level, same convention
   std::vector<int> final_pos, final_order;       // composed: input row -> band row; band col -> input col
   std::vector<int> first_rows;
-  std::vector<T> offd;                           // coupling blocks, row-major K x K, 2 per interface
+  // coupling blocks (row-major K x K, B_t at 2t, C_t at 2t+1) as entries of
+  // the dense [P-1][2][K][K] layout: index and value
+  std::vector<long long> offd_idx;
+  std::vector<T> offd_val;
+  size_t offd_size = 0;
   std::vector<int> part_k;                       // K_p of the variable band
   int k_db = 0, k_reorder = 0, K = 0, P = 1;
   T drop_actual = T(0);
@@ -51,6 +56,15 @@ class Pipeline {
   std::vector<int> m_rp, m_ci, d_rp, d_ci;
   std::vector<T> m_val, d_val;
   std::vector<char> couples_right;
+
+  // wall time of the stages of run(), in order (ms)
+  std::vector<std::pair<const char*, double>> stage_ms;
+  double stage(const char* name) const {
+    double t = 0;
+    for (const auto& s : stage_ms)
+      if (std::string(s.first) == name) t += s.second;
+    return t;
+  }
 
   // weight[e] = log(rowmax[row(e)] / |a_e|) and rowmax, both from the device
   void run(const std::vector<double>& weight, const std::vector<double>& rowmax);

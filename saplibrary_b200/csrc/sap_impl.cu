@@ -118,6 +118,7 @@ class PrecBase {
 
   int n = 0, K = 0, P = 1;
   bool spike = false, lu_ul = false;
+  bool tf32 = false;  // wide-band block products in TF32 (FP32 storage)
   int ptype = SAP_PRECOND_SPIKE;
   std::vector<PartDev> parts_h;
   DBuf<PartDev> parts_d;
@@ -130,7 +131,8 @@ class PrecBase {
 
   // statistics
   double t_toBanded = 0, t_offDiags = 0, t_bandLU = 0, t_assembly = 0, t_fullLU = 0, t_transfer = 0;
-  double t_reorder = 0, t_dropOff = 0, t_cpu_assemble = 0;
+  double t_reorder = 0, t_dropOff = 0, t_cpu_assemble = 0, t_DB = 0;
+  double t_pipeline = 0;  // the whole host pipeline
   int k_reorder = 0, k_db = 0;
   double drop_actual = 0;
 
@@ -228,6 +230,22 @@ class PrecondT : public PrecBase {
     return iface;
   }
 
+  // dense coupling blocks on the device from the pipeline's entries
+  void upload_coupling(const rp::Pipeline<T>& pl) {
+    offd.alloc(pl.offd_size);
+    offd.zero(st);
+    if (!pl.offd_idx.empty()) {
+      DBuf<long long> di;
+      DBuf<T> dv;
+      di.upload(pl.offd_idx, st);
+      dv.upload(pl.offd_val, st);
+      const long long m = (long long)pl.offd_idx.size();
+      k_scatter_idx<T><<<grid1d(m), 256, 0, st>>>(di.get(), dv.get(), m, offd.get());
+      SAPB_LAUNCHED();
+      SAPB_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+
   void wide_init(int kmax) {
     wide_check_memory(kmax);
     std::vector<int> ps(P), pz(P);
@@ -236,7 +254,7 @@ class PrecondT : public PrecBase {
       pz[p] = parts_h[p].size;
     }
     wide = std::make_unique<WideBand<T>>();
-    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz);
+    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz, tf32);
   }
 
   // spikes and reduced system of the block path
@@ -326,7 +344,12 @@ class PrecondT : public PrecBase {
     t_transfer = ms_since(t0);
     auto t1 = Clock::now();
     pl.run(w, rmax);
-    t_reorder = ms_since(t1);
+    t_pipeline = ms_since(t1);
+    // stage times as the reference's timers split them: DB, reordering
+    // (RCM and the second level), drop-off; the rest is assembly
+    t_DB = pl.stage("db");
+    t_reorder = pl.stage("rcm") + pl.stage("second_level");
+    t_dropOff = pl.stage("drop_off");
     k_db = pl.k_db;
     k_reorder = pl.k_reorder;
     drop_actual = (double)pl.drop_actual;
@@ -369,7 +392,7 @@ class PrecondT : public PrecBase {
       k_band_from_csr<T><<<grid_for(n, 256), 256, 0, st>>>(drp.get(), dci.get(), dv.get(), B.get(), n, K);
       SAPB_LAUNCHED();
       SAPB_CUDA(cudaStreamSynchronize(st));
-      t_cpu_assemble = ms_since(t0);
+      t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
       setup_from_band();
       return;
     }
@@ -408,12 +431,12 @@ class PrecondT : public PrecBase {
         dvals.upload(pl.d_val, st);
         wide->load_coo(drows.get(), dcols.get(), dvals.get(), (long long)rows.size());
       }
-      t_cpu_assemble = ms_since(t0) - t_reorder - t_transfer;
+      t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
       auto t2 = Clock::now();
       wide->factor(true);
       t_bandLU = ms_since(t2);
       if (spike) {
-        offd.upload(pl.offd, st);
+        upload_coupling(pl);
         wide_couple(var_iface(pl));
       }
       return;
@@ -434,14 +457,14 @@ class PrecondT : public PrecBase {
       SAPB_LAUNCHED();
       SAPB_CUDA(cudaStreamSynchronize(st));
     }
-    t_cpu_assemble = ms_since(t0) - t_reorder - t_transfer;
+    t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
     auto t2 = Clock::now();
     factor();
     t_bandLU = ms_since(t2);
     if (spike) {
       t2 = Clock::now();
       const size_t KK = (size_t)K * K;
-      offd.upload(pl.offd, st);
+      upload_coupling(pl);
       iface_d.upload(var_iface(pl), st);
       V.alloc(KK * (P - 1));
       W.alloc(KK * (P - 1));
@@ -796,11 +819,19 @@ class Solver {
   DBuf<unsigned int> dots_ctr;
   double* pinned = nullptr;
   DBuf<double> bvec, xvec;
+  // persistent Krylov vectors (allocated at the first solve of size n)
+  std::vector<DBuf<double>> ws;
+  double* wsv(int i) {
+    if ((int)ws.size() <= i) ws.resize(i + 1);
+    ws[i].alloc(n);
+    return ws[i].get();
+  }
 
   Solver(int P, const sap_options& o, int dtype) : opts(o), P_req(P), prec_dtype(dtype) {
     SAPB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (dtype == SAP_PREC_DOUBLE) pcp = std::make_unique<PrecondT<double>>();
     else pcp = std::make_unique<PrecondT<float>>();
+    pcp->tf32 = dtype == SAP_PREC_TF32;
     pcp->o = o;
     pcp->P_req = P;
     pcp->st = st;
@@ -861,19 +892,80 @@ class Solver {
 
   // bicgstabl<..., L> (sap/bicgstab2.h:32-360)
   void bicgstabl(const Spmv& A, double* x, const double* b, int L);
+
+  // FP64 iterative refinement around bicgstabl (options.refinementSweeps):
+  // every sweep solves A d = r for the true residual r = b - A x to the
+  // global tolerance (or until the inner monitor stops), then x += d.  The
+  // monitor reports the final true residual and the total iteration count.
+  void refine(const Spmv& A, double* x, const double* b, int L, int sweeps) {
+    // slots 30, 31: beyond bicgstabl's (2L+2+10 <= 16 for L <= 2)
+    struct Vec {
+      double* p;
+      double* get() const { return p; }
+    } r{wsv(30)}, d{wsv(31)};
+    const double bn = mon.rhsNorm;
+    const double tol = opts.absTol + opts.relTol * bn;
+    auto residual = [&]() {
+      A.apply(x, r.get(), st);
+      axpby(b, r.get(), r.get(), 1.0, -1.0);
+      return nrm2(r.get());
+    };
+    double rn = residual();
+    float total = 0;
+    int code = 0;
+    std::string msg;
+    for (int sw = 0; sw < sweeps; sw++) {
+      if (rn <= tol) break;
+      const float left = (float)opts.maxNumIterations - total;
+      if (left <= 0) { code = -1; msg = "Maximum number of iterations was reached"; break; }
+      SAPB_CUDA(cudaMemsetAsync(d.p, 0, (size_t)n * sizeof(double), st));
+      mon.init(rn);
+      mon.relTol = tol / rn;
+      mon.absTol = 0;
+      mon.maxIt = (int)std::ceil(left);
+      bicgstabl(A, d.get(), r.get(), L);
+      total += mon.it;
+      code = mon.code;
+      msg = mon.msg;
+      axpy(d.get(), x, 1.0);
+      const double rnew = residual();
+      const bool progress = rnew < rn;
+      rn = rnew;
+      if (!progress) break;
+    }
+    mon.relTol = opts.relTol;
+    mon.absTol = opts.absTol;
+    mon.maxIt = opts.maxNumIterations;
+    mon.rhsNorm = bn;
+    mon.rNorm = rn;
+    mon.it = total;
+    if (std::isnan(rn)) { code = -2; msg = "Residual norm is NaN"; }
+    else if (rn <= tol) { code = 1; msg = "Converged"; }
+    else if (code > 0) { code = -3; msg = "Stagnation encountered"; }
+    mon.code = code;
+    mon.msg = msg;
+    SAPB_CUDA(cudaStreamSynchronize(st));
+  }
 };
 
 void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
   const double eps = 1e-20;
   double rho0 = 1, alpha = 0, omega = 1, rho1;
-  std::vector<DBuf<double>> rr(L + 1), uu(L + 1);
-  DBuf<double> r0, xx, Pv, x_min, Pxx, APxx;
+  // workspace slots 0..2L+1: rr, uu; then the named vectors
+  struct Vec {
+    double* p;
+    double* get() const { return p; }
+  };
+  std::vector<Vec> rr(L + 1), uu(L + 1);
   for (int k = 0; k <= L; k++) {
-    rr[k].alloc(n); rr[k].zero(st);
-    uu[k].alloc(n); uu[k].zero(st);
+    rr[k].p = wsv(k);
+    uu[k].p = wsv(L + 1 + k);
+    SAPB_CUDA(cudaMemsetAsync(rr[k].p, 0, (size_t)n * sizeof(double), st));
+    SAPB_CUDA(cudaMemsetAsync(uu[k].p, 0, (size_t)n * sizeof(double), st));
   }
-  r0.alloc(n); xx.alloc(n); Pv.alloc(n); x_min.alloc(n); Pxx.alloc(n); APxx.alloc(n);
-  x_min.zero(st);
+  const int w0 = 2 * L + 2;
+  Vec r0{wsv(w0)}, xx{wsv(w0 + 1)}, Pv{wsv(w0 + 2)}, x_min{wsv(w0 + 3)}, Pxx{wsv(w0 + 4)}, APxx{wsv(w0 + 5)};
+  SAPB_CUDA(cudaMemsetAsync(x_min.p, 0, (size_t)n * sizeof(double), st));
   std::vector<std::vector<double>> tao(L + 1, std::vector<double>(L + 1, 0.0));
   std::vector<double> gamma(L + 2), gp(L + 2), gpp(L + 2), sigma(L + 2);
   auto Pm = [&](const double* in, double* out) { pcp->apply(in, out); };
@@ -982,8 +1074,7 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
   if (mon.code > 0) {
     Pm(xx.get(), x);
   } else {
-    DBuf<double> Pxmin, APxmin, rc, rcm;
-    Pxmin.alloc(n); APxmin.alloc(n); rc.alloc(n); rcm.alloc(n);
+    Vec Pxmin{wsv(w0 + 6)}, APxmin{wsv(w0 + 7)}, rc{wsv(w0 + 8)}, rcm{wsv(w0 + 9)};
     Pm(xx.get(), Pxx.get());
     Am(Pxx.get(), APxx.get());
     axpby(b, APxx.get(), rc.get(), 1.0, -1.0);
@@ -1223,7 +1314,9 @@ int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y,
 int sap_solver_create(int P, const sap_options* opts, int prec_dtype, sap_solver** out) {
   SAP_TRY({
     SAP_REQUIRE(out && opts && P >= 1, "invalid solver arguments");
-    SAP_REQUIRE(prec_dtype == SAP_PREC_FLOAT || prec_dtype == SAP_PREC_DOUBLE, "invalid preconditioner type");
+    SAP_REQUIRE(prec_dtype == SAP_PREC_FLOAT || prec_dtype == SAP_PREC_DOUBLE || prec_dtype == SAP_PREC_TF32,
+                "invalid preconditioner type");
+    SAP_REQUIRE(opts->refinementSweeps >= 0, "refinementSweeps must be >= 0");
     auto h = std::make_unique<sap_solver>();
     h->s = std::make_unique<Solver>(P, *opts, prec_dtype);
     *out = h.release();
@@ -1246,6 +1339,7 @@ static void finish_setup_stats(Solver& S, double t_setup) {
   st.time_bandLU = pc.t_bandLU;
   st.time_assembly = pc.t_assembly;
   st.time_fullLU = pc.t_fullLU;
+  st.time_DB = pc.t_DB;
   st.time_reorder = pc.t_reorder;
   st.time_dropOff = pc.t_dropOff;
   st.time_cpu_assemble = pc.t_cpu_assemble;
@@ -1326,7 +1420,8 @@ int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, 
     SAPB_CUDA(cudaMemcpyAsync(S.bvec.get(), b, bytes, kin, S.st));
     SAPB_CUDA(cudaMemcpyAsync(S.xvec.get(), x, bytes, kin, S.st));
     S.mon.init(S.nrm2(S.bvec.get()));
-    S.bicgstabl(spmv->op, S.xvec.get(), S.bvec.get(), L);
+    if (S.opts.refinementSweeps > 0) S.refine(spmv->op, S.xvec.get(), S.bvec.get(), L, S.opts.refinementSweeps);
+    else S.bicgstabl(spmv->op, S.xvec.get(), S.bvec.get(), L);
     cudaMemcpyKind kout = memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     SAPB_CUDA(cudaMemcpyAsync(x, S.xvec.get(), bytes, kout, S.st));
     SAPB_CUDA(cudaStreamSynchronize(S.st));

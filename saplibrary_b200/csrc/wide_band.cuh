@@ -14,6 +14,8 @@
 // nb*bs rows per partition, padding rows carry an identity diagonal.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace sapb {
@@ -181,52 +183,132 @@ __global__ void __launch_bounds__(256) k_bgemv(const T* A, int ld, long long sA,
 //   y = A x (mode 0),  y = c - A x (mode 1; c may alias y),
 // with tri = 1 (lower: row r reads columns <= r), 2 (upper: columns >= r)
 // or 0 (all).  Skipped entries are exact zeros of the factors, so the
-// triangular forms read half the bytes.  A CTA of 8 warps owns 64-row tiles
-// (lane rows r0+lane and r0+32+lane: every load instruction is a coalesced
-// 256-byte column segment), its warps split the columns and reduce in
-// shared memory in a fixed order.  Tiles are paired j with (T-1-j) so
-// triangular work is the same for every CTA.  Batch b uses A + b*sA,
-// x + b*sx, c + b*sc, y + b*sy.
-constexpr int kGemvRows = 64, kGemvWarps = 8;
+// triangular forms read half the bytes.  A CTA of 16 warps owns tiles of
+// R = 32*VEC rows; lane l holds rows r0+VEC*l .. r0+VEC*l+VEC-1, so one load
+// instruction of a warp is a coalesced column segment of 32*VEC elements
+// (16-byte vectors when VEC*sizeof(T) = 16; VEC > 1 needs the leading
+// dimension and batch stride to be multiples of VEC and A aligned to
+// VEC*sizeof(T)).  The warps split the columns (8 columns in flight per
+// warp) and reduce in shared memory in a fixed order.  Tiles are paired j
+// with (T-1-j) so triangular work is the same for every CTA.  Batch b uses
+// A + b*sA, x + b*sx, c + b*sc, y + b*sy.
+constexpr int kGemvWarps = 16;
+template <typename T, int VEC>
+struct VecOf;
+template <>
+struct VecOf<double, 2> { using type = double2; };
+template <>
+struct VecOf<float, 4> { using type = float4; };
 template <typename T>
-__global__ void __launch_bounds__(256) k_tgemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c,
-                                               long long sc, T* y, long long sy, int n, int mode, int tri) {
-  __shared__ T part[kGemvWarps][kGemvRows];
+__device__ __forceinline__ void vec_fma(const double2& a, T xv, T* acc) {
+  acc[0] += a.x * xv;
+  acc[1] += a.y * xv;
+}
+template <typename T>
+__device__ __forceinline__ void vec_fma(const float4& a, T xv, T* acc) {
+  acc[0] += a.x * xv;
+  acc[1] += a.y * xv;
+  acc[2] += a.z * xv;
+  acc[3] += a.w * xv;
+}
+
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, long long sA, const T* x, long long sx,
+                                                           const T* c, long long sc, T* y, long long sy, int n,
+                                                           int mode, int tri) {
+  constexpr int R = 32 * (VEC > 1 ? VEC : 2);
+  __shared__ T part[kGemvWarps][R];
   const int b = blockIdx.y;
-  const int ntile = (n + kGemvRows - 1) / kGemvRows;
+  const int ntile = (n + R - 1) / R;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const T* Ab = A + b * sA;
   const T* xb = x + b * sx;
   for (int half = 0; half < 2; half++) {
     const int tile = half == 0 ? (int)blockIdx.x : ntile - 1 - (int)blockIdx.x;
     if (half == 1 && tile <= (int)blockIdx.x) break;
-    const int r0 = tile * kGemvRows;
+    const int r0 = tile * R;
     int c0 = 0, c1 = n;
-    if (tri == 1) c1 = min(n, r0 + kGemvRows);
+    if (tri == 1) c1 = min(n, r0 + R);
     else if (tri == 2) c0 = r0;
-    const int ra = r0 + lane, rb = r0 + 32 + lane;
-    const bool va = ra < n, vb = rb < n;
-    T acc0 = T(0), acc1 = T(0);
-#pragma unroll 4
-    for (int col = c0 + w; col < c1; col += kGemvWarps) {
-      const T xv = xb[col];
-      const T* cp = Ab + (long long)col * ld;
-      if (va) acc0 += cp[ra] * xv;
-      if (vb) acc1 += cp[rb] * xv;
+    // 8 independent column loads in flight per warp, then the FMAs
+    constexpr int U = 8;
+    constexpr int S = kGemvWarps;
+    if constexpr (VEC > 1) {
+      using V = typename VecOf<T, VEC>::type;
+      T acc[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; v++) acc[v] = T(0);
+      const int r = r0 + VEC * lane;
+      const int valid = min(VEC, max(0, n - r));
+      const T* base = Ab + r;
+      int col = c0 + w;
+      if (valid == VEC) {
+        for (; col + (U - 1) * S < c1; col += U * S) {
+          V a[U];
+          T xv[U];
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            a[u] = *reinterpret_cast<const V*>(base + (long long)(col + u * S) * ld);
+            xv[u] = xb[col + u * S];
+          }
+#pragma unroll
+          for (int u = 0; u < U; u++) vec_fma<T>(a[u], xv[u], acc);
+        }
+        for (; col < c1; col += S) vec_fma<T>(*reinterpret_cast<const V*>(base + (long long)col * ld), xb[col], acc);
+      } else {
+        for (; col < c1; col += S) {
+          const T xv = xb[col];
+          for (int v = 0; v < valid; v++) acc[v] += base[(long long)col * ld + v] * xv;
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < VEC; v++) part[w][VEC * lane + v] = acc[v];
+    } else {
+      T acc0 = T(0), acc1 = T(0);
+      const int ra = r0 + lane, rb = r0 + 32 + lane;
+      const bool va = ra < n, vb = rb < n;
+      const T* pa = Ab + (va ? ra : 0);
+      const T* pb = Ab + (vb ? rb : 0);
+      int col = c0 + w;
+      for (; col + (U - 1) * S < c1; col += U * S) {
+        T a0[U], a1[U], xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const long long o = (long long)(col + u * S) * ld;
+          a0[u] = va ? pa[o] : T(0);
+          a1[u] = vb ? pb[o] : T(0);
+          xv[u] = xb[col + u * S];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          acc0 += a0[u] * xv[u];
+          acc1 += a1[u] * xv[u];
+        }
+      }
+      for (; col < c1; col += S) {
+        const T xv = xb[col];
+        const long long o = (long long)col * ld;
+        if (va) acc0 += pa[o] * xv;
+        if (vb) acc1 += pb[o] * xv;
+      }
+      part[w][lane] = acc0;
+      part[w][32 + lane] = acc1;
     }
-    part[w][lane] = acc0;
-    part[w][32 + lane] = acc1;
     __syncthreads();
-    if (threadIdx.x < kGemvRows) {
-      const int r = r0 + threadIdx.x;
+    for (int q = threadIdx.x; q < R; q += blockDim.x) {
+      const int r = r0 + q;
       T s = T(0);
 #pragma unroll
-      for (int q = 0; q < kGemvWarps; q++) s += part[q][threadIdx.x];
+      for (int k = 0; k < kGemvWarps; k++) s += part[k][q];
       if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
     }
     __syncthreads();
   }
 }
+
+// rows per tile of k_tgemv<T, VEC>
+template <typename T, int VEC>
+constexpr int tgemv_rows() { return 32 * (VEC > 1 ? VEC : 2); }
 
 // Nonzero columns of the coupling blocks: flag[blk][c] = any row of column c
 // of row-major K x K block blk (blk = 2t + which) is nonzero.
@@ -257,26 +339,29 @@ __global__ void k_spike_rhs(const T* __restrict__ offd, int which, int K, const 
     X[t * sX + jj * plen + pos[(long long)t * K + k]] = M[(long long)k * K];
 }
 
-// Spike tips out of the solved slab: out[t][col][k] (column-major K x K).
+// Spike tips out of the solved slab: element (k, col) of out[t], column-major
+// with leading dimension ldo and batch stride so.
 template <typename T>
 __global__ void k_spike_tips(const T* __restrict__ X, long long sX, long long plen, const int* __restrict__ cols,
-                             int ncol, int j0, const int* __restrict__ pos, int K, T* __restrict__ out) {
+                             int ncol, int j0, const int* __restrict__ pos, int K, int ldo, long long so,
+                             T* __restrict__ out) {
   const int jj = blockIdx.x, t = blockIdx.y;
   const int col = (j0 + jj < ncol) ? cols[(long long)t * ncol + j0 + jj] : -1;
   if (col < 0) return;
-  const long long KK = (long long)K * K;
   for (int k = threadIdx.x; k < K; k += blockDim.x)
-    out[t * KK + (long long)col * K + k] = X[t * sX + jj * plen + pos[(long long)t * K + k]];
+    out[t * so + (long long)col * ldo + k] = X[t * sX + jj * plen + pos[(long long)t * K + k]];
 }
 
-// Row-major coupling block (2t + which) -> column-major out[t], via 32x32 tiles.
+// Row-major coupling block (2t + which) -> column-major out[t] (leading
+// dimension ldo, batch stride so), via 32x32 tiles.
 template <typename T>
-__global__ void k_couple_colmajor(const T* __restrict__ offd, int which, int K, T* __restrict__ out) {
+__global__ void k_couple_colmajor(const T* __restrict__ offd, int which, int K, int ldo, long long so,
+                                  T* __restrict__ out) {
   __shared__ T tile[32][33];
   const int t = blockIdx.z;
   const long long KK = (long long)K * K;
   const T* M = offd + (2LL * t + which) * KK;
-  T* O = out + t * KK;
+  T* O = out + t * so;
   const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int r = r0 + i, c = c0 + threadIdx.x;
@@ -285,7 +370,7 @@ __global__ void k_couple_colmajor(const T* __restrict__ offd, int which, int K, 
   __syncthreads();
   for (int i = threadIdx.y; i < 32; i += blockDim.y) {
     const int c = c0 + i, r = r0 + threadIdx.x;
-    if (r < K && c < K) O[(long long)c * K + r] = tile[threadIdx.x][i];
+    if (r < K && c < K) O[(long long)c * ldo + r] = tile[threadIdx.x][i];
   }
 }
 
@@ -349,13 +434,14 @@ __global__ void k_move_idx(const T* __restrict__ src, const long long* __restric
     dst[didx[e]] = src[sidx[e]];
 }
 
-// S = I (K x K column-major per batch element)
+// S = I (K x K column-major with leading dimension ld, per batch element;
+// padding rows zero)
 template <typename T>
-__global__ void k_identity(T* __restrict__ S, int K, long long stride) {
+__global__ void k_identity(T* __restrict__ S, int K, int ld, long long stride) {
   const int b = blockIdx.y;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)K * K;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)ld * K;
        e += (long long)gridDim.x * blockDim.x)
-    S[b * stride + e] = (e % K == e / K) ? T(1) : T(0);
+    S[b * stride + e] = (e % ld == e / ld) ? T(1) : T(0);
 }
 
 }  // namespace sapb

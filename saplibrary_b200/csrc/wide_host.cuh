@@ -115,6 +115,8 @@ class WideBand {
   cublasHandle_t h = nullptr;
   cudaStream_t st = nullptr;
   int n = 0, P = 0, bs = 0, nb = 0, K = 0;  // K: width of the coupling blocks
+  int ldK = 0;                               // leading dimension of the K x K blocks (16-byte multiple)
+  long long sK = 0;                          // their batch stride, ldK * K
   bool spike = false;
   long long plen = 0, BB = 0;
   std::vector<int> pstart_h, psize_h;
@@ -142,8 +144,18 @@ class WideBand {
     return 4.0 * P * nbp * b * b * sizeof(T);
   }
 
-  void init(cudaStream_t s, int n_, int bs_, const std::vector<int>& pstart, const std::vector<int>& psize) {
+  // tf32: FP32 block products on the tensor cores (TF32 inputs, FP32
+  // accumulation) for the partition factors and spikes; the reduced system
+  // keeps full FP32 products.
+  bool tf32 = false;
+  void math_mode(bool fast) {
+    cublas_check(cublasSetMathMode(h, fast ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_PEDANTIC_MATH), "cublasSetMathMode");
+  }
+
+  void init(cudaStream_t s, int n_, int bs_, const std::vector<int>& pstart, const std::vector<int>& psize,
+            bool tf32_ = false) {
     st = s;
+    tf32 = tf32_ && sizeof(T) == 4;
     n = n_;
     P = (int)pstart.size();
     bs = bs_;
@@ -151,6 +163,7 @@ class WideBand {
     psize_h = psize;
     cublas_check(cublasCreate(&h), "cublasCreate");
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
+    math_mode(tf32);
     int maxsz = 0;
     for (int v : psize) maxsz = std::max(maxsz, v);
     nb = std::max(1, (maxsz + bs - 1) / bs);
@@ -249,8 +262,17 @@ class WideBand {
   // tri: 0 full, 1 lower, 2 upper (see k_tgemv)
   void gemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y, long long sy,
             int m, int nbatch, int mode, int tri) {
-    const int ntile = (m + kGemvRows - 1) / kGemvRows;
-    k_tgemv<T><<<dim3((ntile + 1) / 2, nbatch), 256, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri);
+    constexpr int V = 16 / sizeof(T);  // 16-byte loads
+    const bool vec = ld % V == 0 && sA % V == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
+    if (vec) {
+      const int ntile = (m + tgemv_rows<T, V>() - 1) / tgemv_rows<T, V>();
+      k_tgemv<T, V><<<dim3((ntile + 1) / 2, nbatch), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m,
+                                                                             mode, tri);
+    } else {
+      const int ntile = (m + tgemv_rows<T, 1>() - 1) / tgemv_rows<T, 1>();
+      k_tgemv<T, 1><<<dim3((ntile + 1) / 2, nbatch), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m,
+                                                                             mode, tri);
+    }
     SAPB_LAUNCHED();
   }
 
@@ -307,11 +329,13 @@ class WideBand {
   // unknowns of partition t+1.
   void spikes(const T* offd, const std::vector<int>& iface, int K_) {
     K = K_;
+    constexpr int V = 16 / sizeof(T);
+    ldK = (K + V - 1) / V * V;
+    sK = (long long)ldK * K;
     spike = true;
     const int nI = P - 1;
-    const long long KK = (long long)K * K;
-    Vc.alloc((size_t)nI * KK);
-    Wc.alloc((size_t)nI * KK);
+    Vc.alloc((size_t)nI * sK);
+    Wc.alloc((size_t)nI * sK);
     Vc.zero(st);
     Wc.zero(st);
     std::vector<int> nzh;
@@ -378,8 +402,8 @@ class WideBand {
           ops.gemm(bs, w, bs, T(1), Fk(Uinv, nb, i), Xb(i), T(0), Wm);
           ops.copy(Wm, Xb(i), bs, w);
         }
-        k_spike_tips<T><<<dim3(w, nI), kt, 0, st>>>(X.get(), sX, plen, cols_d.get(), ncol, j0, pos_d.get(), K,
-                                                     which ? Wc.get() : Vc.get());
+        k_spike_tips<T><<<dim3(w, nI), kt, 0, st>>>(X.get(), sX, plen, cols_d.get(), ncol, j0, pos_d.get(), K, ldK,
+                                                     sK, which ? Wc.get() : Vc.get());
         SAPB_LAUNCHED();
       }
       SAPB_CUDA(cudaStreamSynchronize(st));
@@ -389,26 +413,28 @@ class WideBand {
   // S_t = I - W_t V_t, factored with its triangular inverses (boosted only
   // when `boost`); coupling blocks kept column-major for the apply.
   void reduced(const T* offd, const std::vector<int>& iface, bool boost) {
+    math_mode(false);
     const int nI = P - 1;
-    const long long KK = (long long)K * K;
-    Bc.alloc((size_t)nI * KK);
-    Cc.alloc((size_t)nI * KK);
+    Bc.alloc((size_t)nI * sK);
+    Cc.alloc((size_t)nI * sK);
+    Bc.zero(st);
+    Cc.zero(st);
     const dim3 tg((K + 31) / 32, (K + 31) / 32, nI);
-    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 0, K, Bc.get());
+    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 0, K, ldK, sK, Bc.get());
     SAPB_LAUNCHED();
-    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 1, K, Cc.get());
+    k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 1, K, ldK, sK, Cc.get());
     SAPB_LAUNCHED();
     DBuf<T> S, Ws;
     DBuf<int> sflag;
-    S.alloc((size_t)nI * KK);
-    Ws.alloc((size_t)nI * KK);
+    S.alloc((size_t)nI * sK);
+    Ws.alloc((size_t)nI * sK);
     sflag.alloc(1);
     sflag.zero(st);
-    SLi.alloc((size_t)nI * KK);
-    SUi.alloc((size_t)nI * KK);
+    SLi.alloc((size_t)nI * sK);
+    SUi.alloc((size_t)nI * sK);
     SLi.zero(st);
     SUi.zero(st);
-    k_identity<T><<<dim3(grid1d(KK, 256, 4096), nI), 256, 0, st>>>(S.get(), K, KK);
+    k_identity<T><<<dim3(grid1d(sK, 256, 4096), nI), 256, 0, st>>>(S.get(), K, ldK, sK);
     SAPB_LAUNCHED();
     BlockLU<T> lu;
     lu.h = h;
@@ -416,10 +442,10 @@ class WideBand {
     lu.batch = nI;
     lu.boost = boost;
     lu.flag = sflag.get();
-    lu.W = Mat<T>{Ws.get(), K, KK};
-    const Mat<T> Sm{S.get(), K, KK};
-    lu.gemm(K, K, K, T(-1), Mat<T>{Wc.get(), K, KK}, Mat<T>{Vc.get(), K, KK}, T(1), Sm);
-    lu.rec(Sm, Mat<T>{SLi.get(), K, KK}, Mat<T>{SUi.get(), K, KK}, K);
+    lu.W = Mat<T>{Ws.get(), ldK, sK};
+    const Mat<T> Sm{S.get(), ldK, sK};
+    lu.gemm(K, K, K, T(-1), Mat<T>{Wc.get(), ldK, sK}, Mat<T>{Vc.get(), ldK, sK}, T(1), Sm);
+    lu.rec(Sm, Mat<T>{SLi.get(), ldK, sK}, Mat<T>{SUi.get(), ldK, sK}, K);
     std::vector<long long> pos((size_t)nI * 2 * K), rows((size_t)nI * 2 * K);
     for (int which = 0; which < 2; which++) {
       const std::vector<int> q = iface_pos(iface, which);
@@ -443,7 +469,7 @@ class WideBand {
   // band-order right-hand side; F's interface rows get f -= offdiag * z.
   void reduced_apply(const T* x, T* F) {
     const int nI = P - 1;
-    const long long KK = (long long)K * K, m = (long long)nI * 2 * K, s2 = 2LL * K;
+    const long long m = (long long)nI * 2 * K, s2 = 2LL * K;
     k_gather_idx<T><<<grid1d(m), 256, 0, st>>>(x, ipos.get(), m, xbt.get());
     SAPB_LAUNCHED();
     k_gather_idx<T><<<grid1d(m), 256, 0, st>>>(F, irow.get(), m, fbt.get());
@@ -452,12 +478,12 @@ class WideBand {
     T* xt = xbt.get() + K;
     T* fb = fbt.get();
     T* ft = fbt.get() + K;
-    gemv(Wc.get(), K, KK, xb, s2, xt, s2, t1.get(), K, K, nI, 1, 0);            // t1 = xt - W xb
-    gemv(SLi.get(), K, KK, t1.get(), K, nullptr, 0, t2.get(), K, K, nI, 0, 1);  // t2 = L_S^-1 t1
-    gemv(SUi.get(), K, KK, t2.get(), K, nullptr, 0, t1.get(), K, K, nI, 0, 2);  // z2 = U_S^-1 t2
-    gemv(Vc.get(), K, KK, t1.get(), K, xb, s2, t2.get(), K, K, nI, 1, 0);       // z1 = xb - V z2
-    gemv(Bc.get(), K, KK, t1.get(), K, fb, s2, fb, s2, K, nI, 1, 0);            // f_b -= B z2
-    gemv(Cc.get(), K, KK, t2.get(), K, ft, s2, ft, s2, K, nI, 1, 0);            // f_t -= C z1
+    gemv(Wc.get(), ldK, sK, xb, s2, xt, s2, t1.get(), K, K, nI, 1, 0);            // t1 = xt - W xb
+    gemv(SLi.get(), ldK, sK, t1.get(), K, nullptr, 0, t2.get(), K, K, nI, 0, 1);  // t2 = L_S^-1 t1
+    gemv(SUi.get(), ldK, sK, t2.get(), K, nullptr, 0, t1.get(), K, K, nI, 0, 2);  // z2 = U_S^-1 t2
+    gemv(Vc.get(), ldK, sK, t1.get(), K, xb, s2, t2.get(), K, K, nI, 1, 0);       // z1 = xb - V z2
+    gemv(Bc.get(), ldK, sK, t1.get(), K, fb, s2, fb, s2, K, nI, 1, 0);            // f_b -= B z2
+    gemv(Cc.get(), ldK, sK, t2.get(), K, ft, s2, ft, s2, K, nI, 1, 0);            // f_t -= C z1
     k_scatter_idx<T><<<grid1d(m), 256, 0, st>>>(irow.get(), fbt.get(), m, F);
     SAPB_LAUNCHED();
   }

@@ -74,3 +74,42 @@ def test_wide_fp64_solve_matches_oracle_and_direct():
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-9
     xd = sl.solve_banded((K, K), band_to_scipy(band, n, K), b)
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
+
+
+@pytest.mark.parametrize("prec", ["float", "tf32"])
+def test_refinement_reaches_fp64_tolerance_with_low_precision_preconditioner(prec):
+    # the FP32 / TF32 preconditioner stagnates BiCGStab(2) near FP32
+    # accuracy; FP64 refinement sweeps around it reach 1e-10
+    from saplibrary_b200.problems import convection_diffusion_csr, csr_matvec
+    m, P = 100, 16
+    rp, ci, v, _ = convection_diffusion_csr(m=m, fill_reach=5 * m, seed=m)
+    n = m * m
+    A = sap.CsrMatrix(rp, ci, v)
+    b = np.random.default_rng(3).standard_normal(n)
+    s = sap.Solver(P, sap.Options(dropOffFraction=1e-4, relTol=1e-10, maxNumIterations=100,
+                                  refinementSweeps=6), prec=prec)
+    s.setup(A)
+    assert s.getStats().bandwidth >= 256  # the block path
+    x = np.zeros(n)
+    assert s.solve(sap.SpmvCusp(A), b, x)
+    assert s.getMonitorCode() == 1
+    st = s.getStats()
+    assert st.relResidualNorm <= 1e-10
+    true_rel = np.linalg.norm(b - csr_matvec(rp, ci, v, x)) / np.linalg.norm(b)
+    assert true_rel <= 1.01e-10
+    assert abs(true_rel - st.relResidualNorm) <= 1e-12
+
+
+def test_tf32_banded_refinement():
+    n, K, P = 40000, 300, 8
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=12)
+    b = oracle.spmv_banded(band, n, K, np.ones(n))
+    A = sap.BandedMatrix.from_array(band, n, K)
+    opts = sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False, factMethod=sap.LU_UL,
+                       relTol=1e-10, maxNumIterations=100, refinementSweeps=4)
+    s = sap.Solver(P, opts, prec="tf32")
+    s.setup(A)
+    x = np.zeros(n)
+    assert s.solve(sap.MVBanded(A), b, x)
+    assert s.getStats().relResidualNorm <= 1e-10
+    assert np.linalg.norm(x - 1.0) / np.sqrt(n) <= 1e-8
