@@ -1,10 +1,19 @@
-"""Benchmark of the SPIKE-preconditioned BiCGStab(2) solve on B200.
+"""Benchmark of the SPIKE-preconditioned Krylov solve on B200.
 
-One step = one time-to-solution of the named workload: preconditioner
-setup (band conversion, partitioned LU/UL factorisation, spike tips,
-reduced system, sweep transfer matrices) plus the BiCGStab(2) solve to
-FP64 relative residual 1e-10, as Solver::setup + Solver::solve of the
-reference (sap/solver.h:339-562).
+Workload (one step = one time-to-solution): the 1,000,000-row nonsymmetric
+CSR matrix of a 1000 x 1000 2D 5-point convection-diffusion stencil
+(diffusion 1, upwinded convection 0.3) plus 2 extra entries per row at
+seeded random columns within +-5,000 of the diagonal (values U[-0.1, 0.1]),
+rows permuted by a seeded random permutation; b ~ N(0, 1) seeded; P = 16,
+drop-off 1e-4; solve to FP64 relative residual 1e-10.  A step is
+Solver::setup(A) (DB matching, RCM, drop-off, second-level reordering,
+variable band, partition block LU, spike tips, reduced system) followed by
+Solver::solve(spmv, b, x) from x = 0 (sap/solver.h:339-562).
+
+Two forms are timed: the headline precision form (FP32 preconditioner whose
+wide-band block products run on the tensor cores in TF32, with FP64
+refinement sweeps around BiCGStab(2)) and the plain FP64 form (FP64
+preconditioner, the reference's single BiCGStab(2)).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -15,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -25,11 +35,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Workload: the banded config (N=200,000, K=50, off-diagonals iid U[-1,1],
-# diagonal = 1.0 x row sum of |off-diagonals|, x_true = 1, b = A x_true,
-# P=10, LU_UL, BiCGStab(2) to relative residual 1e-10).
-WORKLOAD = dict(name="banded_n200000_k50_d1.0_p10_lu_ul", n=200000, k=50, d=1.0, dist=1, P=10, relTol=1e-10,
-                maxit=100)
+WORKLOAD = dict(name="cd2d_m1000_conv0.3_fill2x5000_rowperm_p16_drop1e-4", m=1000, conv=0.3, fill_per_row=2,
+                fill_reach=5000, fill_mag=0.1, P=16, drop=1e-4, relTol=1e-10, maxit=100)
+FORMS = {
+    "tf32_refine": dict(prec="tf32", refinementSweeps=6),
+    "fp64": dict(prec="double", refinementSweeps=0),
+}
+HEADLINE = "tf32_refine"
+# rows of the CPU band-LU timing sample (about 5 s at K ~ 3000)
+LU_SAMPLE_ROWS = 400
 
 
 def measured_peaks():
@@ -50,20 +64,20 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.out = ""
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *a):
-        self.out = ""
         if self.proc is not None:
-            time.sleep(0.15)
+            time.sleep(0.25)
             self.proc.terminate()
             try:
                 self.out, _ = self.proc.communicate(timeout=5)
@@ -96,45 +110,87 @@ def dist_init():
     return ws, rank, local
 
 
-def oracle_time_to_solution(band, n, k, P, b, relTol, maxit):
-    """One setup + solve of the CPU oracle (FP64 preconditioner), seconds."""
+def make_problem(seed: int):
+    from saplibrary_b200.problems import convection_diffusion_csr
+    w = WORKLOAD
+    rp, ci, v, _ = convection_diffusion_csr(m=w["m"], conv=w["conv"], fill_per_row=w["fill_per_row"],
+                                            fill_reach=w["fill_reach"], fill_mag=w["fill_mag"], seed=seed)
+    b = np.random.default_rng(seed + 7).standard_normal(w["m"] * w["m"])
+    return rp, ci, v, b
+
+
+def cpu_reference_sample(rp, ci, v, applies: float):
+    """Time-to-solution of the CPU oracle (the reference's algorithm restated)
+    for this workload, from a bounded sample: the full reordering (DB, RCM,
+    drop-off, coupling blocks, second level) is run and timed; the partition
+    band LU is timed on its first LU_SAMPLE_ROWS pivots at the workload's K
+    and scaled to the rows every core factors (partitions in parallel over
+    the host threads); the spike tips are costed as 3 band sweeps of K
+    right-hand sides per interface (3 x the LU's n_p K^2) and every
+    preconditioner apply as 4 triangular band sweeps (4 n K)."""
     import oracle
+    w = WORKLOAD
     t0 = time.perf_counter()
-    pc = oracle.Precond(P, fact=0, dtype="double")
-    st = pc.setup_banded(band, n, k)
-    x, res = pc.solve(b, band=band, K=k, L=2, maxit=maxit, reltol=relTol)
-    dt = time.perf_counter() - t0
-    return dt, res, st
+    o = oracle.SparsePrecond(w["P"], dtype="double", dropFrac=w["drop"])
+    rc = o.setup(rp, ci, v, factor=False, band=False)
+    t_reorder = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError(f"oracle reordering failed: {o.message}")
+    info = o.info()
+    K, P, n = info.K, info.P, info.n
+    t_lu = oracle.band_lu_sample(K, LU_SAMPLE_ROWS)
+    per_row = t_lu / LU_SAMPLE_ROWS
+    cores = oracle.num_threads()
+    rows_per_core = math.ceil(n / P) * math.ceil(P / cores)
+    t_factor = per_row * rows_per_core
+    t_spikes = 3.0 * t_factor
+    t_solve = per_row * rows_per_core * 4.0 * applies / K
+    total = t_reorder + t_factor + t_spikes + t_solve
+    sample = (f"full oracle reordering ({t_reorder:.2f} s) + FP64 band LU of {LU_SAMPLE_ROWS} pivots at K={K} "
+              f"({per_row * 1e3:.2f} ms/row) scaled to {rows_per_core} rows per core (P={P}, {cores} threads); "
+              f"spike tips costed as 3x the LU, {applies:.0f} applies as 4nK each")
+    parts = {"reorder_s": t_reorder, "factor_s": t_factor, "spikes_s": t_spikes, "solve_s": t_solve}
+    return total, cores, sample, parts, K
 
 
 def run_reference(args, ws, rank):
+    """--impl reference: the oracle port of the reference's CPU path, timed on
+    a bounded sample of the workload per step (see cpu_reference_sample)."""
     if rank != 0:
         return
-    import oracle
-    import saplibrary_b200 as sap
-    w = WORKLOAD
-    band = sap.generate_band_host(w["n"], w["k"], w["d"], w["dist"], seed=1234)
-    b = oracle.spmv_banded(band, w["n"], w["k"], np.ones(w["n"]))
+    rp, ci, v, _ = make_problem(seed=1)
+    applies = 4 * 7.75  # BiCGStab(2) iterations of the plain FP64 form on this workload, 4 applies each
     for _ in range(args.warmup):
-        oracle_time_to_solution(band, w["n"], w["k"], w["P"], b, w["relTol"], w["maxit"])
-    times = []
-    res = None
+        cpu_reference_sample(rp, ci, v, applies)
+    vals = []
+    cores, sample, parts, K = 0, "", {}, 0
     for _ in range(args.steps):
-        dt, res, _ = oracle_time_to_solution(band, w["n"], w["k"], w["P"], b, w["relTol"], w["maxit"])
-        times.append(dt)
-    t = float(np.mean(times))
-    cores = oracle.num_threads()
+        t, cores, sample, parts, K = cpu_reference_sample(rp, ci, v, applies)
+        vals.append(t)
+    t = float(np.mean(vals))
     line = {
         "impl": "reference", "metric": "time_to_solution", "value": t, "unit": "s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["name"], "preconditioner": "fp64", "krylov": "BiCGStab2"},
-        "cpu_baseline": {"value": t, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": "full workload: setup + BiCGStab(2) solve to rel-res 1e-10 (OpenMP over partitions)"},
+        "config": {"workload": WORKLOAD["name"], "preconditioner": "fp64", "krylov": "BiCGStab2",
+                   "rel_tol": WORKLOAD["relTol"]},
+        "cpu_baseline": {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "monitor_code": int(res.code), "iterations": float(res.iterations), "rel_residual": float(res.rel_res_norm),
+        "parts": parts, "K": K,
     }
     print(json.dumps(line), flush=True)
+
+
+def sweep_bytes(bs: int, nb: int, P: int, vbytes: int) -> int:
+    """Algorithmic bytes of one block sweep (x <- A_p^-1 x for all partitions):
+    the 4*nb-2 triangles of bs(bs+1)/2 factor values it must read (L_ii^-1,
+    U_ii^-1, and the off-diagonal factor blocks, whose other triangle is
+    structurally zero), the right-hand side and carry vectors read and the
+    result written, for P partitions."""
+    tri = bs * (bs + 1) // 2
+    mats = (4 * nb - 2) * tri
+    vecs = (4 * nb - 2) * 2 * bs + (2 * nb - 2) * bs
+    return P * (mats + vecs) * vbytes
 
 
 def main():
@@ -144,6 +200,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--forms", default=",".join(FORMS), help="comma-separated forms to time")
     args = ap.parse_args()
     ws, rank, local = dist_init()
 
@@ -155,148 +213,160 @@ def main():
     import torch.distributed as dist
     torch.cuda.set_device(local)
     if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     import saplibrary_b200 as sap
 
     w = WORKLOAD
-    n, k, P = w["n"], w["k"], w["P"]
-    seed = 1234 + rank
-    band_host = sap.generate_band_host(n, k, w["d"], w["dist"], seed=seed)
-    pinned_band = torch.from_numpy(band_host).pin_memory()
-    band_np = pinned_band.numpy()
-    A = sap.BandedMatrix.from_array(band_np, n, k)
-    spmv = sap.MVBanded(A)
-    xt = torch.ones(n, device="cuda", dtype=torch.float64)
-    b = torch.empty_like(xt)
-    spmv(xt, b)
+    warm = max(3, args.warmup)
+    rp, ci, v, b_np = make_problem(seed=1 + rank)
+    n = len(rp) - 1
+    A = sap.CsrMatrix(rp, ci, v)
+    spmv = sap.SpmvCusp(A)
+    b = torch.tensor(b_np, device="cuda")
     x = torch.zeros_like(b)
-    opts = sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False, factMethod=sap.LU_UL,
-                       relTol=w["relTol"], maxNumIterations=w["maxit"])
-    solver = sap.Solver(P, opts, prec="double")
-    stream = torch.cuda.ExternalStream(solver.stream())
 
-    def step():
-        solver.setup(A)
-        x.zero_()
-        return solver.solve(spmv, b, x)
+    def solver_for(form):
+        f = FORMS[form]
+        opts = sap.Options(dropOffFraction=w["drop"], relTol=w["relTol"], maxNumIterations=w["maxit"],
+                           refinementSweeps=f["refinementSweeps"])
+        return sap.Solver(w["P"], opts, prec=f["prec"])
 
-    for _ in range(max(3, args.warmup)):
-        ok = step()
-    assert ok, "warm-up solve did not converge"
-
-    # per-kernel breakdown of one step (CUDA events on the launching stream)
-    families = ["factor", "transfer", "pass1", "pass2", "pass3", "scan", "reduced_apply", "spmv_banded", "dots"]
-    breakdown = {}
-    for fam in families:
-        sap.profile_select(fam)
-        step()
-        ms, cnt = sap.profile_read()
-        breakdown[fam] = {"ms": ms, "launches": cnt}
-    sap.profile_select(None)
-    dominant = max(breakdown, key=lambda f: breakdown[f]["ms"])
-
-    # ---- timed region: device events on the solver stream ----------------------
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sap.profile_select(dominant)
-    launches0 = sap.kernel_launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            ok = step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    gpu_launches = sap.kernel_launch_count() - launches0
-    dom_ms, dom_cnt = sap.profile_read()
-    sap.profile_select(None)
-    ms_total = ev0.elapsed_time(ev1)
-    ms_step = ms_total / args.steps
-    if ws > 1:
-        t = torch.tensor([ms_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
-    st = solver.getStats()
-    code = solver.getMonitorCode()
-    err = float(torch.linalg.norm(x - xt) / torch.linalg.norm(xt))
-
-    # ---- end to end through the C ABI with host buffers ---------------------------
-    b_host = torch.empty(n, dtype=torch.float64).pin_memory()
-    b_host.copy_(b.cpu())
-    x_host = torch.zeros(n, dtype=torch.float64).pin_memory()
-    b_np, x_np = b_host.numpy(), x_host.numpy()
-    solver_h = sap.Solver(P, opts, prec="double")
-
-    def step_e2e():
-        Ah = sap.BandedMatrix.from_array(band_np, n, k)   # host -> device copy of the matrix
-        solver_h.setup(Ah)
-        x_np[:] = 0.0
-        ok_ = solver_h.solve(sap.MVBanded(Ah), b_np, x_np)  # b, x0 in; x out
-        return ok_
-
-    for _ in range(2):
-        step_e2e()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ok_e2e = step_e2e()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if ws > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    h2d = band_np.nbytes + 2 * n * 8
-    d2h = n * 8
-
-    # ---- roofline of the dominant kernel --------------------------------------------
+    results = {}
+    forms = [f for f in args.forms.split(",") if f]
+    if HEADLINE not in forms:
+        forms.insert(0, HEADLINE)
     peaks, peak_kind = measured_peaks()
-    SW = 2 * k + 1
-    nfact = 2 * (n - n // P)  # LU rows of partitions 0..P-2 + UL rows of partitions 1..P-1
-    bytes_per_launch = {
-        "factor": 2 * 8 * SW * nfact,                 # read + write of every factored band column (FP64)
-        "pass1": 8 * (k + 1) * n + 8 * n + 8 * n,     # half band + rhs in + F out
-        "pass2": 8 * SW * n + 3 * 8 * n,              # full band + F in + Y out
-        "pass3": 8 * (k + 1) * n + 2 * 8 * n,         # half band + Y in + out
-        "spmv_banded": 8 * SW * n + 16 * n,           # row-major FP64 band + x + y
-        "dots": 2 * 8 * n,
-        "transfer": 2 * 8 * (k + 1) * n,
-        "scan": 0, "reduced_apply": 0,
-    }
-    avg_ms = dom_ms / max(1, dom_cnt)
-    alg = bytes_per_launch.get(dominant, 0)
-    achieved = alg / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
-    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peak_kind,
-                "avg_launch_ms": avg_ms, "launches": dom_cnt}
+    clocks, head_launches = None, 0
+    for form in forms:
+        solver = solver_for(form)
+        stream = torch.cuda.ExternalStream(solver.stream())
+
+        def step():
+            solver.setup(A)
+            x.zero_()
+            return solver.solve(spmv, b, x)
+
+        ok = False
+        for _ in range(warm):
+            ok = step()
+        assert ok, f"{form}: warm-up solve did not converge"
+        steps = args.steps if form == HEADLINE else min(args.steps, 3)
+        # ---- timed region: device events on the solver stream ----------------
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sap.profile_select("block_sweep")
+        launches0, lib0 = sap.kernel_launch_count(), sap.library_call_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            for _ in range(steps):
+                ok = step()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        sweep_ms, sweep_cnt = sap.profile_read()
+        sap.profile_select(None)
+        launches = sap.kernel_launch_count() - launches0
+        lib_calls = sap.library_call_count() - lib0
+        ms_step = ev0.elapsed_time(ev1) / steps
+        if ws > 1:
+            t = torch.tensor([ms_step], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_step = float(t.item())
+        st = solver.getStats()
+        bs, nb, vb = solver.blockLayout()
+        _, K, P = solver.info()
+        # true FP64 residual of the last step's solution
+        r = torch.empty_like(b)
+        spmv(x, r)
+        true_rel = float(torch.linalg.norm(b - r) / torch.linalg.norm(b))
+        res = {
+            "tts_s": ms_step / 1e3, "steps": steps, "ok": bool(ok), "monitor_code": solver.getMonitorCode(),
+            "iterations": st.numIterations, "rel_residual": st.relResidualNorm, "true_rel_residual": true_rel,
+            "K": K, "P": P, "block_size": bs, "blocks_per_partition": nb, "value_bytes": vb,
+            "gpu_launches_per_step": launches / steps, "cublas_calls_per_step": lib_calls / steps,
+            "stage_ms": {k: round(getattr(st, k), 2) for k in
+                         ("time_DB", "time_reorder", "time_dropOff", "time_cpu_assemble", "time_transfer",
+                          "time_bandLU", "time_assembly", "time_fullLU", "timeSetup", "timeSolve")},
+        }
+        if bs > 0 and sweep_cnt > 0:
+            avg = sweep_ms / sweep_cnt
+            alg = sweep_bytes(bs, nb, P, vb)
+            res["block_sweep"] = {"avg_ms": avg, "launches": sweep_cnt, "bytes": alg,
+                                  "gbs": alg / (avg * 1e-3) / 1e9}
+        results[form] = res
+        if form == HEADLINE:
+            clocks = clk.summary()
+            head_launches = launches
+        del solver, stream
+        torch.cuda.empty_cache()
+
+    head = results[HEADLINE]
+
+    # ---- end to end through the public API with host buffers ----------------------
+    e2e = None
+    if not args.no_e2e:
+        solver_h = solver_for(HEADLINE)
+        b_host = torch.from_numpy(b_np.copy()).pin_memory()
+        x_host = torch.zeros(n, dtype=torch.float64).pin_memory()
+        bh, xh = b_host.numpy(), x_host.numpy()
+
+        def step_e2e():
+            Ah = sap.CsrMatrix(rp, ci, v)  # host -> device copy of the matrix
+            solver_h.setup(Ah)
+            xh[:] = 0.0
+            return solver_h.solve(sap.SpmvCusp(Ah), bh, xh)  # b, x0 in; x out
+
+        for _ in range(2):
+            step_e2e()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step_e2e()
+        e2e_s = (time.perf_counter() - t0) / args.steps
+        if ws > 1:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = rp.nbytes + ci.nbytes + v.nbytes + 2 * n * 8
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": n * 8}
+        del solver_h
+
+    # ---- roofline of the dominant kernel: the block-sweep gemv (k_tgemv) ----------
+    roofline = None
+    if "block_sweep" in head:
+        bsw = head["block_sweep"]
+        roofline = {"kernel": "k_tgemv (one block_sweep = 4*nb-2 launches)", "bound": "hbm", "achieved": bsw["gbs"],
+                    "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": bsw["gbs"] / peaks["hbm_gbs"],
+                    "traffic": None, "peak_source": peak_kind, "avg_sweep_ms": bsw["avg_ms"],
+                    "bytes_per_sweep": bsw["bytes"]}
 
     line = {
-        "metric": "time_to_solution", "value": ms_step / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": w["name"], "preconditioner": "fp64 (plain SaP form)", "krylov": "BiCGStab2",
+        "metric": "time_to_solution", "value": head["tts_s"], "unit": "s", "n_gpus": ws, "steps": args.steps,
+        "warmup": warm, "ms_per_step": head["tts_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 Krylov / tf32-f32 preconditioner", "data": "synthetic",
+        "config": {"workload": w["name"], "form": HEADLINE, "krylov": "BiCGStab2 + FP64 refinement",
                    "rel_tol": w["relTol"], "parallelism": f"replicas{ws}",
-                   "l2": "inputs larger than L2 (FP64 band 161.6 MB)"},
-        "solves_per_s": ws * 1e3 / ms_step,
-        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": int(gpu_launches),
+                   "l2": "inputs larger than L2 (CSR 84 MB, factors tens of GB)"},
+        "solves_per_s": ws / head["tts_s"],
+        "plain_fp64_tts_s": results["fp64"]["tts_s"] if "fp64" in results else None,
+        "speedup_vs_plain_fp64": (results["fp64"]["tts_s"] / head["tts_s"]) if "fp64" in results else None,
+        "e2e": e2e,
+        "gpu_launches": int(head_launches),
         "roofline": roofline,
-        "breakdown_ms": {f: round(v["ms"], 4) for f, v in breakdown.items()},
-        "clocks": clk.summary(),
-        "monitor_code": code, "iterations": st.numIterations, "rel_residual": st.relResidualNorm,
-        "err_vs_xtrue": err, "setup_ms": st.timeSetup, "solve_ms": st.timeSolve,
+        "clocks": clocks,
+        "forms": results,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        dt, res, _ = oracle_time_to_solution(band_host, n, k, P, b.cpu().numpy(), w["relTol"], w["maxit"])
-        import oracle
-        line["cpu_baseline"] = {"value": dt, "unit": "s", "cores": oracle.num_threads(), "kind": "port",
-                                "sample": "one full setup + solve of the same workload (FP64 preconditioner)"}
+        applies = 4 * results["fp64"]["iterations"] if "fp64" in results else 31.0
+        t, cores, sample, parts, _ = cpu_reference_sample(rp, ci, v, applies)
+        line["cpu_baseline"] = {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample,
+                                "parts": parts}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del solver, solver_h
     if ws > 1:
         dist.destroy_process_group()
 

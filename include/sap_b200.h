@@ -237,8 +237,14 @@ int sap_solver_info(const sap_solver* s, int* n, int* k, int* num_partitions);
 int sap_solver_get_reorder(const sap_solver* s, int which, int* out, int64_t* count);
 /* The cudaStream_t all device work of this solver is enqueued on. */
 void* sap_solver_stream(const sap_solver* s);
-/* Number of kernels this library has enqueued since load (all handles). */
+/* Layout of the wide-band block path after setup: the block size and the
+ * number of blocks per partition (both 0 when the narrow band kernels are
+ * used), and the bytes of one preconditioner value (4 or 8). */
+int sap_solver_block_layout(const sap_solver* s, int* block_size, int* blocks_per_partition, int* value_bytes);
+/* Number of this library's own kernels enqueued since load (all handles). */
 int64_t sap_kernel_launch_count(void);
+/* Number of cuBLAS calls (batched GEMMs of the wide-band path) since load. */
+int64_t sap_library_call_count(void);
 /* Live kernel timing with CUDA events on the launching stream: while a
  * kernel name is selected, every launch of that kernel is bracketed by an
  * event pair; sap_profile_read returns the summed duration (ms) and the

@@ -58,6 +58,8 @@ def lib():
         L.orc_solve.argtypes = [vp, i, i, dp, ip, ip, dp, dp, dp, i, i, ctypes.c_double, ctypes.c_double,
                                 ctypes.POINTER(OrcResult)]
         L.orc_num_threads.restype = i
+        L.orc_band_lu_sample.restype = ctypes.c_double
+        L.orc_band_lu_sample.argtypes = [i, i]
         _lib = L
     return _lib
 
@@ -136,6 +138,12 @@ def spmv_csr(rp, ci, v, x):
     return y
 
 
+def band_lu_sample(K: int, steps: int) -> float:
+    """Seconds of the first `steps` pivots of the FP64 partition band LU at
+    half-bandwidth K (a CPU-baseline timing sample)."""
+    return lib().orc_band_lu_sample(int(K), int(steps))
+
+
 def num_threads() -> int:
     return lib().orc_num_threads()
 
@@ -188,12 +196,15 @@ class SparsePrecond:
             _sparse_lib().orc_sparse_destroy(self.h)
             self.h = None
 
-    def setup(self, rp, ci, v, factor=True):
+    def setup(self, rp, ci, v, factor=True, band=True):
+        """factor: also factor the band; band=False (with factor=False) stops
+        after the permutations, without assembling the band storage."""
         self._csr = [np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
                      np.ascontiguousarray(v, np.float64)]
         msg = ctypes.create_string_buffer(256)
+        mode = 1 if factor else (0 if band else 2)
         rc = _sparse_lib().orc_sparse_setup(self.h, self._csr[0].size - 1, *[_p(a) for a in self._csr],
-                                            int(factor), msg, 256)
+                                            mode, msg, 256)
         self.message = msg.value.decode()
         return rc
 

@@ -776,7 +776,8 @@ static double wall() { timespec t; clock_gettime(CLOCK_MONOTONIC, &t); return t.
 #define ORC_STAGE(name) do { if (getenv("ORC_TIMING")) fprintf(stderr, "[oracle] %-24s %8.3f s\n", name, wall() - t_stage); t_stage = wall(); } while (0)
 
 template <typename T>
-static void sparse_reorder(SparsePrecond<T>& sp, int n, const int* rp, const int* ci, const double* v) {
+static void sparse_reorder(SparsePrecond<T>& sp, int n, const int* rp, const int* ci, const double* v,
+                           bool assemble = true) {
   double t_stage = wall();
   // CSR in PrecValueType with explicit zeros dropped (precond.h:1667-1713)
   std::vector<int> Arp(n + 1, 0), Aci;
@@ -837,9 +838,11 @@ static void sparse_reorder(SparsePrecond<T>& sp, int n, const int* rp, const int
     secondLevelReordering(g, K, P, sp.secondReorder, sp.secondPerm, sp.first_rows);
     ORC_STAGE("secondLevelReordering");
     assembleBandedVar(g, P, sp.ks, sp.boff, sp.ks_col, sp.ks_row);
+    if (!assemble) sp.boff.assign(P + 1, 0);  // permutations only: no band storage
     sp.B.assign(sp.boff[P], T(0));
-    for (int j = 0; j < n; j++)
-      for (int it = g.drp[j]; it < g.drp[j + 1]; it++) sp.at(part_of(g.dci[it], q, rem), j, g.dci[it]) = g.dval[it];
+    if (assemble)
+      for (int j = 0; j < n; j++)
+        for (int it = g.drp[j]; it < g.drp[j + 1]; it++) sp.at(part_of(g.dci[it], q, rem), j, g.dci[it]) = g.dval[it];
   } else {
     // constant band over the whole reordered matrix (assembleBandedMatrix, graph.h:1019-1091)
     sp.ks.assign(P, K);
@@ -1065,12 +1068,14 @@ void* orc_sparse_create(int P, int dtype, int doDB, int scale, double dropFrac, 
 
 void orc_sparse_destroy(void* h) { delete (orc_sparse_handle*)h; }
 
-// Runs the reorder pipeline only (stage 0) or reorder + factorisation (1).
+// Runs the reorder pipeline only (factor 0), reorder + factorisation (1), or
+// the permutations only, without assembling the band (2).
 int orc_sparse_setup(void* h, int n, const int* rp, const int* ci, const double* v, int factor, char* msg, int msglen) {
   auto* H = (orc_sparse_handle*)h;
   return H->visit([&](auto& sp) -> int {
     try {
-      orc::sparse_reorder(sp, n, rp, ci, v);
+      orc::sparse_reorder(sp, n, rp, ci, v, factor != 2);
+      if (factor == 2) factor = 0;
       if (!sp.varBand && sp.P > 1) { sp.status = -103; sp.msg = "constant band with reordering not restated"; }
       else if (factor) orc::sparse_factor(sp);
     } catch (const orc::DBError& e) {

@@ -19,6 +19,7 @@
 //  * row-major input band (sap/banded_matrix.h:66-92): element (i,j) at
 //    i*(2K+1) + K + (j-i).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -748,6 +749,41 @@ void* orc_precond_create(int P, int fact, int ptype, int safe, int dtype) {
 }
 
 void orc_precond_destroy(void* h) { delete (orc::Handle*)h; }
+
+// CPU-baseline timing sample: the first `steps` pivots of the partition LU
+// above (lu_partition, restating bandLU_g32) on a diagonally dominant band
+// of half-bandwidth K (off-diagonals from a fixed LCG in [-1, 1], diagonal
+// the row sum of their magnitudes), in FP64.  Returns the seconds of the
+// pivots alone (band construction excluded).
+double orc_band_lu_sample(int K, int steps) {
+  orc::Precond<double> pc;
+  pc.K = K;
+  const int n = steps + K + 1;
+  pc.n = n;
+  pc.B.assign((size_t)(2 * K + 1) * n, 0.0);
+  unsigned long long s = 0x9E3779B97F4A7C15ull;
+  std::vector<double> rowsum(n, 0.0);
+  for (int j = 0; j < n; j++)
+    for (int i = std::max(0, j - K); i <= std::min(n - 1, j + K); i++) {
+      if (i == j) continue;
+      s = s * 6364136223846793005ull + 1442695040888963407ull;
+      const double v = (double)(s >> 11) / 9007199254740992.0 * 2.0 - 1.0;
+      pc.at(i, j) = v;
+      rowsum[i] += std::fabs(v);
+    }
+  for (int i = 0; i < n; i++) pc.at(i, i) = rowsum[i];
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int j = 0; j < steps; j++) {
+    const int w = std::min(K, n - 1 - j);
+    const double piv = pc.at(j, j);
+    for (int r = 1; r <= w; r++) pc.at(j + r, j) /= piv;
+    for (int c = 1; c <= w; c++) {
+      const double u = pc.at(j, j + c);
+      for (int r = 1; r <= w; r++) pc.at(j + r, j + c) -= pc.at(j + r, j) * u;
+    }
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
 // convertToBandedMatrix(BandedMatrix) (sap/precond.h:2103-2233).
 int orc_setup_banded(void* h, int n, int K, const double* band_rm) {

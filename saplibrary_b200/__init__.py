@@ -86,6 +86,8 @@ _pp = ctypes.POINTER(ctypes.c_void_p)
 _sig = {
     "sap_last_error": (ctypes.c_char_p, []),
     "sap_kernel_launch_count": (ctypes.c_int64, []),
+    "sap_library_call_count": (ctypes.c_int64, []),
+    "sap_solver_block_layout": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_options_default": (_i, [ctypes.POINTER(_COptions)]),
     "sap_banded_create": (_i, [_i, _i, _vp, _i, _pp]),
     "sap_banded_generate": (_i, [_i, _i, _d, _i, ctypes.c_uint64, _pp]),
@@ -151,6 +153,11 @@ def _ptr(a):
 def kernel_launch_count() -> int:
     """Number of kernels this library has enqueued since it was loaded."""
     return int(_lib.sap_kernel_launch_count())
+
+
+def library_call_count() -> int:
+    """Number of cuBLAS calls (wide-band batched GEMMs) since the library was loaded."""
+    return int(_lib.sap_library_call_count())
 
 
 def profile_select(kernel_name: str | None) -> None:
@@ -406,6 +413,13 @@ class Solver:
         n, k, p = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(_lib.sap_solver_info(self._h, ctypes.byref(n), ctypes.byref(k), ctypes.byref(p)))
         return n.value, k.value, p.value
+
+    def blockLayout(self):
+        """(block size, blocks per partition, bytes per preconditioner value) of
+        the wide-band block path; (0, 0, bytes) for the narrow band kernels."""
+        bs, nb, vb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.sap_solver_block_layout(self._h, ctypes.byref(bs), ctypes.byref(nb), ctypes.byref(vb)))
+        return bs.value, nb.value, vb.value
 
     REORDER_ARRAYS = ("dbRowPerm", "finalPerm", "finalReordering", "first_rows", "ks")
 

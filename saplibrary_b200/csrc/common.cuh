@@ -38,7 +38,9 @@ void set_last_error(const std::string& msg);
 
 // Number of kernels enqueued by this library (reported by the bench).
 extern std::atomic<int64_t> g_launches;
+extern std::atomic<int64_t> g_lib_calls;
 inline void count_launch(int k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+inline void count_lib_call() { g_lib_calls.fetch_add(1, std::memory_order_relaxed); }
 #define SAPB_LAUNCHED() do { ::sapb::count_launch(); SAPB_CUDA(cudaGetLastError()); } while (0)
 
 // Event bracketing of the launches of one selected kernel (sap_profile_*).

@@ -26,6 +26,7 @@
 namespace sapb {
 
 std::atomic<int64_t> g_launches{0};
+std::atomic<int64_t> g_lib_calls{0};
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -143,6 +144,7 @@ class PrecBase {
   virtual void setup_csr_direct(const Csr& A, int K_) = 0;
   virtual void setup_sparse(const Csr& A) = 0;
   virtual void apply_band(const double* v, double* z) = 0;
+  virtual void block_layout(int& bs, int& nb) const = 0;
   void apply(const double* v, double* z) { apply_band(v, z); }
 
   void clamp_partitions_banded() {
@@ -186,6 +188,10 @@ class PrecondT : public PrecBase {
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
   std::unique_ptr<WideBand<T>> wide;  // block (GEMM) path of wide bands
+  void block_layout(int& bs, int& nb) const override {
+    bs = wide ? wide->bs : 0;
+    nb = wide ? wide->nb : 0;
+  }
 
   // Half-bandwidths from this value up are factored and applied as block
   // tridiagonal partitions (wide_host.cuh); above 1024 that is the only
@@ -1121,6 +1127,7 @@ extern "C" {
 
 const char* sap_last_error(void) { return g_last_error.c_str(); }
 int64_t sap_kernel_launch_count(void) { return g_launches.load(); }
+int64_t sap_library_call_count(void) { return g_lib_calls.load(); }
 
 int sap_profile_select(const char* name) {
   SAP_TRY({
@@ -1465,6 +1472,18 @@ int sap_solver_info(const sap_solver* h, int* n, int* k, int* P) {
     if (n) *n = h->s->pcp->n;
     if (k) *k = h->s->pcp->K;
     if (P) *P = h->s->pcp->P;
+  });
+}
+
+int sap_solver_block_layout(const sap_solver* h, int* block_size, int* blocks_per_partition, int* value_bytes) {
+  SAP_TRY({
+    SAP_REQUIRE(h, "null argument");
+    const PrecBase& pc = *h->s->pcp;
+    int bs = 0, nb = 0;
+    pc.block_layout(bs, nb);
+    if (block_size) *block_size = bs;
+    if (blocks_per_partition) *blocks_per_partition = nb;
+    if (value_bytes) *value_bytes = h->s->prec_dtype == SAP_PREC_DOUBLE ? 8 : 4;
   });
 }
 

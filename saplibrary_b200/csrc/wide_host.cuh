@@ -30,7 +30,7 @@ struct Gemm<double> {
     cublas_check(cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &alpha, A, lda, sA, B, ldb, sB, &beta,
                                            C, ldc, sC, batch),
                  "cublasDgemmStridedBatched");
-    count_launch();
+    count_lib_call();
   }
 };
 template <>
@@ -41,7 +41,7 @@ struct Gemm<float> {
     cublas_check(cublasSgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &alpha, A, lda, sA, B, ldb, sB, &beta,
                                            C, ldc, sC, batch),
                  "cublasSgemmStridedBatched");
-    count_launch();
+    count_lib_call();
   }
 };
 

@@ -64,3 +64,23 @@ def test_sparse_fp64_solve_matches_oracle(m, P):
     assert s.getStats().numIterations == res.iterations
     assert s.getStats().relResidualNorm <= 1e-10
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-8
+
+
+@pytest.mark.parametrize("dtype", ["double", "float"])
+def test_config1_size_permutations_bit_exact(dtype):
+    # the 1M-row reordered sparse workload: DB, RCM, drop-off and the
+    # second-level reordering against the oracle at full size (permutations
+    # only: the oracle does not assemble the band)
+    m, P = 1000, 16
+    rp, ci, v, _ = convection_diffusion_csr(m=m, fill_reach=5 * m, seed=1)
+    o = oracle.SparsePrecond(P, dtype=dtype, dropFrac=1e-4)
+    assert o.setup(rp, ci, v, factor=False, band=False) == 0
+    A = sap.CsrMatrix(rp, ci, v)
+    s = sap.Solver(P, sap.Options(dropOffFraction=1e-4, relTol=1e-10), prec="tf32" if dtype == "float" else dtype)
+    s.setup(A)
+    inf, st = o.info(), s.getStats()
+    assert (st.bandwidthDB, st.bandwidthReorder, st.bandwidth, st.numPartitions) == \
+        (inf.k_db, inf.k_reorder, inf.K, inf.P)
+    assert st.actualDropOff == inf.drop_actual
+    for name in ("dbRowPerm", "finalPerm", "finalReordering", "first_rows", "ks"):
+        assert np.array_equal(s.getReorder(name), o.ints(name)), name
