@@ -10,10 +10,12 @@ Solver::setup(A) (DB matching, RCM, drop-off, second-level reordering,
 variable band, partition block LU, spike tips, reduced system) followed by
 Solver::solve(spmv, b, x) from x = 0 (sap/solver.h:339-562).
 
-Two forms are timed: the headline precision form (FP32 preconditioner whose
-wide-band block products run on the tensor cores in TF32, with FP64
-refinement sweeps around BiCGStab(2)) and the plain FP64 form (FP64
-preconditioner, the reference's single BiCGStab(2)).
+Two forms are timed by default: the headline precision form (FP32
+preconditioner whose wide-band block products run on the tensor cores in
+TF32, inside flexible GMRES(50) with FP64 Arnoldi) and the plain FP64 form
+(FP64 preconditioner, the reference's BiCGStab(2)).  A third form
+(tf32_refine: the TF32 preconditioner with FP64 refinement sweeps around
+BiCGStab(2)) can be selected with --forms.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -38,10 +40,12 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(name="cd2d_m1000_conv0.3_fill2x5000_rowperm_p16_drop1e-4", m=1000, conv=0.3, fill_per_row=2,
                 fill_reach=5000, fill_mag=0.1, P=16, drop=1e-4, relTol=1e-10, maxit=100)
 FORMS = {
-    "tf32_refine": dict(prec="tf32", refinementSweeps=6),
-    "fp64": dict(prec="double", refinementSweeps=0),
+    "tf32_refine": dict(prec="tf32", solver="BiCGStab2", refinementSweeps=6),
+    "tf32_fgmres": dict(prec="tf32", solver="FGMRES", refinementSweeps=0),
+    "fp64": dict(prec="double", solver="BiCGStab2", refinementSweeps=0),
 }
-HEADLINE = "tf32_refine"
+HEADLINE = "tf32_fgmres"
+DEFAULT_FORMS = "tf32_fgmres,fp64"
 # rows of the CPU band-LU timing sample (about 5 s at K ~ 3000)
 LU_SAMPLE_ROWS = 400
 
@@ -108,6 +112,14 @@ def dist_init():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return ws, rank, local
+
+
+def set_grid(m: int) -> None:
+    """Grid side of the workload (1000 is the benchmarked size; smaller sides
+    serve profiler captures of the same kernels)."""
+    if m != WORKLOAD["m"]:
+        WORKLOAD["m"] = m
+        WORKLOAD["name"] = WORKLOAD["name"].replace("m1000", f"m{m}")
 
 
 def make_problem(seed: int):
@@ -201,8 +213,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
-    ap.add_argument("--forms", default=",".join(FORMS), help="comma-separated forms to time")
+    ap.add_argument("--forms", default=DEFAULT_FORMS, help="comma-separated forms to time (" + ", ".join(FORMS) + ")")
+    ap.add_argument("--m", type=int, default=WORKLOAD["m"], help="grid side (profiler captures only)")
     args = ap.parse_args()
+    set_grid(args.m)
     ws, rank, local = dist_init()
 
     if args.impl == "reference":
@@ -227,7 +241,8 @@ def main():
 
     def solver_for(form):
         f = FORMS[form]
-        opts = sap.Options(dropOffFraction=w["drop"], relTol=w["relTol"], maxNumIterations=w["maxit"],
+        opts = sap.Options(solverType=getattr(sap, f["solver"]), dropOffFraction=w["drop"], relTol=w["relTol"],
+                           maxNumIterations=w["maxit"] if f["solver"] != "FGMRES" else 4 * w["maxit"],
                            refinementSweeps=f["refinementSweeps"])
         return sap.Solver(w["P"], opts, prec=f["prec"])
 
@@ -348,7 +363,7 @@ def main():
         "metric": "time_to_solution", "value": head["tts_s"], "unit": "s", "n_gpus": ws, "steps": args.steps,
         "warmup": warm, "ms_per_step": head["tts_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 Krylov / tf32-f32 preconditioner", "data": "synthetic",
-        "config": {"workload": w["name"], "form": HEADLINE, "krylov": "BiCGStab2 + FP64 refinement",
+        "config": {"workload": w["name"], "form": HEADLINE, "krylov": "flexible GMRES(50), FP64 Arnoldi",
                    "rel_tol": w["relTol"], "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (CSR 84 MB, factors tens of GB)"},
         "solves_per_s": ws / head["tts_s"],

@@ -51,7 +51,12 @@ enum { SAP_HOST = 0, SAP_DEVICE = 1 };
 /* KrylovSolverType (sap/common.h:71-82); CUSP solvers are not provided. */
 enum {
   SAP_BICGSTAB_C = 0, SAP_GMRES_C = 1, SAP_CG_C = 2, SAP_CR_C = 3,
-  SAP_BICGSTAB1 = 4, SAP_BICGSTAB2 = 5, SAP_BICGSTAB = 6, SAP_MINRES = 7
+  SAP_BICGSTAB1 = 4, SAP_BICGSTAB2 = 5, SAP_BICGSTAB = 6, SAP_MINRES = 7,
+  /* Extension (not in the reference): flexible right-preconditioned
+   * GMRES(50) with FP64 Arnoldi, which tolerates a preconditioner that
+   * changes between applies (FP32 / TF32 factors) and so reaches FP64
+   * tolerances without refinement restarts. */
+  SAP_FGMRES = 8
 };
 /* FactorizationMethod (sap/common.h:86-89) */
 enum { SAP_LU_UL = 0, SAP_LU_ONLY = 1 };

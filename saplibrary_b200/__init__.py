@@ -29,6 +29,8 @@ _lib = ctypes.CDLL(_LIB_PATH)
 
 # ---- enums (sap/common.h) ----------------------------------------------------
 BiCGStab_C, GMRES_C, CG_C, CR_C, BiCGStab1, BiCGStab2, BiCGStab, MINRES = range(8)
+# extension: flexible GMRES(50) with FP64 Arnoldi (tolerates FP32 / TF32 preconditioners)
+FGMRES = 8
 LU_UL, LU_only = 0, 1
 Spike, Block, NoPrecond = 0, 1, 2
 HOST, DEVICE = 0, 1
@@ -444,5 +446,5 @@ class Solver:
 
 
 __all__ = ["Options", "Stats", "Solver", "BandedMatrix", "CsrMatrix", "MVBanded", "SpmvCusp", "SystemError",
-           "LibraryError", "generate_band_host", "kernel_launch_count", "BiCGStab1", "BiCGStab2", "LU_UL",
+           "LibraryError", "generate_band_host", "kernel_launch_count", "BiCGStab1", "BiCGStab2", "FGMRES", "LU_UL",
            "LU_only", "Spike", "Block", "NoPrecond", "EXPORTED_SYMBOLS"]

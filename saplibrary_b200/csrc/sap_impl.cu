@@ -899,6 +899,91 @@ class Solver {
   // bicgstabl<..., L> (sap/bicgstab2.h:32-360)
   void bicgstabl(const Spmv& A, double* x, const double* b, int L);
 
+  // Flexible GMRES(m) (Saad, SIAM J. Sci. Comput. 14 (1993) 461-469):
+  // right preconditioning with the preconditioned directions z_j kept, so
+  // the preconditioner may vary between applies; FP64 Arnoldi with modified
+  // Gram-Schmidt, Givens rotations for the least-squares residual, the true
+  // residual b - A x checked after every cycle.  Monitor: 1 converged,
+  // -1 iteration budget, -2 NaN, -3 a cycle that did not lower the residual.
+  void fgmres(const Spmv& A, double* x, const double* b, int m) {
+    const double tol = mon.tol();
+    double* r = wsv(39);
+    std::vector<double*> Vb(m + 1), Zb(m);
+    for (int i = 0; i <= m; i++) Vb[i] = wsv(40 + i);
+    for (int i = 0; i < m; i++) Zb[i] = wsv(41 + m + i);
+    std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m, 0.0), sn(m, 0.0), g(m + 1, 0.0);
+    auto h = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
+    auto residual = [&]() {
+      A.apply(x, r, st);
+      axpby(b, r, r, 1.0, -1.0);
+      return nrm2(r);
+    };
+    double beta = residual();
+    int total = 0;
+    while (true) {
+      mon.rNorm = beta;
+      if (std::isnan(beta)) { mon.stop(-2, "Residual norm is NaN"); break; }
+      if (beta <= tol) { mon.stop(1, "Converged"); break; }
+      if (total >= mon.maxIt) { mon.stop(-1, "Maximum number of iterations was reached"); break; }
+      axpby(r, r, Vb[0], 1.0 / beta, 0.0);
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = beta;
+      int j = 0;
+      bool nan = false;
+      while (j < m && total < mon.maxIt) {
+        pcp->apply(Vb[j], Zb[j]);
+        A.apply(Zb[j], Vb[j + 1], st);
+        for (int i = 0; i <= j; i++) {
+          const double hij = dot(Vb[j + 1], Vb[i]);
+          h(i, j) = hij;
+          axpy(Vb[i], Vb[j + 1], -hij);
+        }
+        const double hn = nrm2(Vb[j + 1]);
+        h(j + 1, j) = hn;
+        if (hn > 0) axpby(Vb[j + 1], Vb[j + 1], Vb[j + 1], 1.0 / hn, 0.0);
+        for (int i = 0; i < j; i++) {  // previous rotations on column j
+          const double a = h(i, j), c = h(i + 1, j);
+          h(i, j) = cs[i] * a + sn[i] * c;
+          h(i + 1, j) = -sn[i] * a + cs[i] * c;
+        }
+        const double a = h(j, j), c = h(j + 1, j);
+        const double rho = std::hypot(a, c);
+        cs[j] = rho > 0 ? a / rho : 1.0;
+        sn[j] = rho > 0 ? c / rho : 0.0;
+        h(j, j) = rho;
+        h(j + 1, j) = 0.0;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        j++;
+        total++;
+        mon.it = (float)total;
+        const double est = std::fabs(g[j]);
+        if (std::isnan(est)) { nan = true; break; }
+        if (est <= tol || hn == 0) break;
+      }
+      // y = R^-1 g, x += Z y
+      std::vector<double> y(j, 0.0);
+      for (int i = j - 1; i >= 0; i--) {
+        double s = g[i];
+        for (int k = i + 1; k < j; k++) s -= h(i, k) * y[k];
+        y[i] = h(i, i) != 0 ? s / h(i, i) : 0.0;
+      }
+      for (int i = 0; i < j; i++) axpy(Zb[i], x, y[i]);
+      const double bnew = residual();
+      if (nan || std::isnan(bnew)) { mon.rNorm = bnew; mon.stop(-2, "Residual norm is NaN"); break; }
+      const bool progress = bnew < beta;
+      beta = bnew;
+      if (!progress && beta > tol) { mon.rNorm = beta; mon.stop(-3, "Stagnation encountered"); break; }
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // The Krylov method of the options: BiCGStab(L) or flexible GMRES(50).
+  void krylov(const Spmv& A, double* x, const double* b, int L) {
+    if (L > 0) bicgstabl(A, x, b, L);
+    else fgmres(A, x, b, 50);
+  }
+
   // FP64 iterative refinement around bicgstabl (options.refinementSweeps):
   // every sweep solves A d = r for the true residual r = b - A x to the
   // global tolerance (or until the inner monitor stops), then x += d.  The
@@ -929,7 +1014,7 @@ class Solver {
       mon.relTol = tol / rn;
       mon.absTol = 0;
       mon.maxIt = (int)std::ceil(left);
-      bicgstabl(A, d.get(), r.get(), L);
+      krylov(A, d.get(), r.get(), L);
       total += mon.it;
       code = mon.code;
       msg = mon.msg;
@@ -1418,7 +1503,8 @@ int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, 
     int L = 0;
     if (S.opts.solverType == SAP_BICGSTAB2) L = 2;
     else if (S.opts.solverType == SAP_BICGSTAB1) L = 1;
-    else throw Error(SAP_ERR_UNSUPPORTED, "only BiCGStab1 / BiCGStab2 are provided");
+    else if (S.opts.solverType != SAP_FGMRES)
+      throw Error(SAP_ERR_UNSUPPORTED, "only BiCGStab1 / BiCGStab2 and the FGMRES extension are provided");
     auto t0 = Clock::now();
     const size_t bytes = (size_t)S.n * sizeof(double);
     S.bvec.alloc(S.n);
@@ -1428,7 +1514,7 @@ int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, 
     SAPB_CUDA(cudaMemcpyAsync(S.xvec.get(), x, bytes, kin, S.st));
     S.mon.init(S.nrm2(S.bvec.get()));
     if (S.opts.refinementSweeps > 0) S.refine(spmv->op, S.xvec.get(), S.bvec.get(), L, S.opts.refinementSweeps);
-    else S.bicgstabl(spmv->op, S.xvec.get(), S.bvec.get(), L);
+    else S.krylov(spmv->op, S.xvec.get(), S.bvec.get(), L);
     cudaMemcpyKind kout = memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     SAPB_CUDA(cudaMemcpyAsync(x, S.xvec.get(), bytes, kout, S.st));
     SAPB_CUDA(cudaStreamSynchronize(S.st));

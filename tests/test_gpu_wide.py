@@ -113,3 +113,53 @@ def test_tf32_banded_refinement():
     assert s.solve(sap.MVBanded(A), b, x)
     assert s.getStats().relResidualNorm <= 1e-10
     assert np.linalg.norm(x - 1.0) / np.sqrt(n) <= 1e-8
+
+
+@pytest.mark.parametrize("prec", ["double", "tf32"])
+def test_fgmres_reaches_fp64_tolerance(prec):
+    # flexible GMRES keeps the preconditioned directions, so a low-precision
+    # preconditioner needs no refinement restarts
+    from saplibrary_b200.problems import convection_diffusion_csr, csr_matvec
+    m, P = 100, 16
+    rp, ci, v, _ = convection_diffusion_csr(m=m, fill_reach=5 * m, seed=m)
+    n = m * m
+    A = sap.CsrMatrix(rp, ci, v)
+    b = np.random.default_rng(4).standard_normal(n)
+    s = sap.Solver(P, sap.Options(solverType=sap.FGMRES, dropOffFraction=1e-4, relTol=1e-10,
+                                  maxNumIterations=200), prec=prec)
+    s.setup(A)
+    x = np.zeros(n)
+    assert s.solve(sap.SpmvCusp(A), b, x)
+    assert s.getMonitorCode() == 1
+    st = s.getStats()
+    assert st.relResidualNorm <= 1e-10
+    true_rel = np.linalg.norm(b - csr_matvec(rp, ci, v, x)) / np.linalg.norm(b)
+    assert true_rel <= 1.01e-10
+    assert abs(true_rel - st.relResidualNorm) <= 1e-12
+
+
+def test_fgmres_narrow_band_matches_direct():
+    n, K, P = 60000, 16, 8
+    band = sap.generate_band_host(n, K, 0.9, 2, seed=7)
+    b = oracle.spmv_banded(band, n, K, np.ones(n))
+    A = sap.BandedMatrix.from_array(band, n, K)
+    opts = sap.Options(solverType=sap.FGMRES, performReorder=False, variableBandwidth=False, applyScaling=False,
+                       factMethod=sap.LU_UL, relTol=1e-10, maxNumIterations=200)
+    s = sap.Solver(P, opts, prec="float")
+    s.setup(A)
+    x = np.zeros(n)
+    assert s.solve(sap.MVBanded(A), b, x)
+    assert s.getStats().relResidualNorm <= 1e-10
+    xd = sl.solve_banded((K, K), band_to_scipy(band, n, K), b)
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
+
+
+def test_illegal_solver_type_is_unsupported():
+    n, K = 2000, 4
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=2)
+    A = sap.BandedMatrix.from_array(band, n, K)
+    opts = sap.Options(solverType=sap.MINRES, performReorder=False, variableBandwidth=False, applyScaling=False)
+    s = sap.Solver(2, opts, prec="double")
+    s.setup(A)
+    with pytest.raises(sap.LibraryError):
+        s.solve(sap.MVBanded(A), np.ones(n), np.zeros(n))
