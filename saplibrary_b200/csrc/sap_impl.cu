@@ -187,10 +187,11 @@ class PrecondT : public PrecBase {
   DBuf<T> sin_d, cout_d;  // DB row / column scales in band order (reordered path)
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
-  std::unique_ptr<WideBand<T>> wide;  // block (GEMM) path of wide bands
+  std::unique_ptr<WideBand<T>> wide;  // block (GEMM) path of wide bands (buffers kept across setups)
+  bool wide_active = false;           // the last setup used the block path
   void block_layout(int& bs, int& nb) const override {
-    bs = wide ? wide->bs : 0;
-    nb = wide ? wide->nb : 0;
+    bs = wide_active ? wide->bs : 0;
+    nb = wide_active ? wide->nb : 0;
   }
 
   // Half-bandwidths from this value up are factored and applied as block
@@ -216,6 +217,7 @@ class PrecondT : public PrecBase {
   void wide_check_memory(int kmax) {
     size_t fr = 0, tot = 0;
     SAPB_CUDA(cudaMemGetInfo(&fr, &tot));
+    if (wide) fr += wide->bytes_held();  // reused (or released) by the new setup
     const double need = WideBand<T>::factor_bytes(n, P, kmax);
     if (need > 0.92 * (double)fr)
       throw Error(SAP_ERR_OUT_OF_MEMORY, "wide-band factors need " + std::to_string(need / 1e9) + " GB, " +
@@ -259,8 +261,9 @@ class PrecondT : public PrecBase {
       ps[p] = parts_h[p].start;
       pz[p] = parts_h[p].size;
     }
-    wide = std::make_unique<WideBand<T>>();
+    if (!wide) wide = std::make_unique<WideBand<T>>();
     wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz, tf32);
+    wide_active = true;
   }
 
   // spikes and reduced system of the block path
@@ -309,7 +312,7 @@ class PrecondT : public PrecBase {
   void setup_sparse(const Csr& A) override {
     if (o.dbFirstStageOnly) throw Error(SAP_ERR_UNSUPPORTED, "dbFirstStageOnly is not supported");
     if (o.ilu_level >= 0) throw Error(SAP_ERR_UNSUPPORTED, "ILU preconditioning is out of scope");
-    wide.reset();
+    wide_active = false;
     auto t0 = Clock::now();
     n = A.n;
     rp::Pipeline<T> pl;
@@ -447,6 +450,7 @@ class PrecondT : public PrecBase {
       }
       return;
     }
+    wide.reset();
     B.alloc((size_t)off);
     B.zero(st);
     {
@@ -495,7 +499,7 @@ class PrecondT : public PrecBase {
   }
 
   void setup_from_band() {
-    wide.reset();
+    wide_active = false;
     ptype = o.precondType;
     spike = (ptype == SAP_PRECOND_SPIKE && P > 1);
     lu_ul = spike && o.factMethod == SAP_LU_UL;
@@ -534,6 +538,7 @@ class PrecondT : public PrecBase {
       }
       return;
     }
+    wide.reset();
     t0 = Clock::now();
     factor();
     SAPB_CUDA(cudaStreamSynchronize(st));
@@ -748,7 +753,7 @@ class PrecondT : public PrecBase {
       SAPB_LAUNCHED();
       return;
     }
-    if (wide) {
+    if (wide_active) {
       wide->apply(v, z, reordered ? gin_d.get() : nullptr, reordered ? sin_d.get() : nullptr,
                   reordered ? sout_d.get() : nullptr, reordered ? cout_d.get() : nullptr);
       return;

@@ -212,13 +212,22 @@ __device__ __forceinline__ void vec_fma(const float4& a, T xv, T* acc) {
   acc[3] += a.w * xv;
 }
 
+//
+// Column split (gridDim.z = S > 1, for grids with few tiles): CTA s takes
+// the s-th contiguous slice of each of its tiles' column ranges and writes
+// its R partial sums to ws[((b*ntile + tile)*S + s)*R ..]; the CTA that
+// arrives last at the tile's counter (ctr, zero between launches) adds the S
+// slices in order s = 0..S-1, writes y and resets the counter.  No CTA waits
+// for another.
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, long long sA, const T* x, long long sx,
                                                            const T* c, long long sc, T* y, long long sy, int n,
-                                                           int mode, int tri) {
+                                                           int mode, int tri, T* ws, unsigned* ctr) {
   constexpr int R = 32 * (VEC > 1 ? VEC : 2);
   __shared__ T part[kGemvWarps][R];
+  __shared__ unsigned last_cta;
   const int b = blockIdx.y;
+  const int S = gridDim.z, sl = blockIdx.z;
   const int ntile = (n + R - 1) / R;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const T* Ab = A + b * sA;
@@ -230,9 +239,15 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
     int c0 = 0, c1 = n;
     if (tri == 1) c1 = min(n, r0 + R);
     else if (tri == 2) c0 = r0;
+    if (S > 1) {
+      const int chunk = (c1 - c0 + S - 1) / S;
+      const int a = c0 + sl * chunk;
+      c1 = min(c1, a + chunk);
+      c0 = min(a, c1);
+    }
     // 8 independent column loads in flight per warp, then the FMAs
     constexpr int U = 8;
-    constexpr int S = kGemvWarps;
+    constexpr int SW = kGemvWarps;  // column stride of a warp
     if constexpr (VEC > 1) {
       using V = typename VecOf<T, VEC>::type;
       T acc[VEC];
@@ -243,20 +258,20 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
       const T* base = Ab + r;
       int col = c0 + w;
       if (valid == VEC) {
-        for (; col + (U - 1) * S < c1; col += U * S) {
+        for (; col + (U - 1) * SW < c1; col += U * SW) {
           V a[U];
           T xv[U];
 #pragma unroll
           for (int u = 0; u < U; u++) {
-            a[u] = *reinterpret_cast<const V*>(base + (long long)(col + u * S) * ld);
-            xv[u] = xb[col + u * S];
+            a[u] = *reinterpret_cast<const V*>(base + (long long)(col + u * SW) * ld);
+            xv[u] = xb[col + u * SW];
           }
 #pragma unroll
           for (int u = 0; u < U; u++) vec_fma<T>(a[u], xv[u], acc);
         }
-        for (; col < c1; col += S) vec_fma<T>(*reinterpret_cast<const V*>(base + (long long)col * ld), xb[col], acc);
+        for (; col < c1; col += SW) vec_fma<T>(*reinterpret_cast<const V*>(base + (long long)col * ld), xb[col], acc);
       } else {
-        for (; col < c1; col += S) {
+        for (; col < c1; col += SW) {
           const T xv = xb[col];
           for (int v = 0; v < valid; v++) acc[v] += base[(long long)col * ld + v] * xv;
         }
@@ -270,14 +285,14 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
       const T* pa = Ab + (va ? ra : 0);
       const T* pb = Ab + (vb ? rb : 0);
       int col = c0 + w;
-      for (; col + (U - 1) * S < c1; col += U * S) {
+      for (; col + (U - 1) * SW < c1; col += U * SW) {
         T a0[U], a1[U], xv[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-          const long long o = (long long)(col + u * S) * ld;
+          const long long o = (long long)(col + u * SW) * ld;
           a0[u] = va ? pa[o] : T(0);
           a1[u] = vb ? pb[o] : T(0);
-          xv[u] = xb[col + u * S];
+          xv[u] = xb[col + u * SW];
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -285,7 +300,7 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
           acc1 += a1[u] * xv[u];
         }
       }
-      for (; col < c1; col += S) {
+      for (; col < c1; col += SW) {
         const T xv = xb[col];
         const long long o = (long long)col * ld;
         if (va) acc0 += pa[o] * xv;
@@ -295,12 +310,36 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
       part[w][32 + lane] = acc1;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < R; q += blockDim.x) {
-      const int r = r0 + q;
-      T s = T(0);
+    if (S == 1) {
+      for (int q = threadIdx.x; q < R; q += blockDim.x) {
+        const int r = r0 + q;
+        T s = T(0);
 #pragma unroll
-      for (int k = 0; k < kGemvWarps; k++) s += part[k][q];
-      if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+        for (int k = 0; k < kGemvWarps; k++) s += part[k][q];
+        if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+      }
+    } else {
+      const long long slot = (long long)b * ntile + tile;
+      for (int q = threadIdx.x; q < R; q += blockDim.x) {
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < kGemvWarps; k++) s += part[k][q];
+        ws[(slot * S + sl) * R + q] = s;
+      }
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) last_cta = (atomicAdd(&ctr[slot], 1u) == (unsigned)(S - 1));
+      __syncthreads();
+      if (last_cta) {
+        __threadfence();
+        for (int q = threadIdx.x; q < R; q += blockDim.x) {
+          const int r = r0 + q;
+          T s = T(0);
+          for (int k = 0; k < S; k++) s += __ldcg(ws + (slot * S + k) * R + q);
+          if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+        }
+        if (threadIdx.x == 0) ctr[slot] = 0u;
+      }
     }
     __syncthreads();
   }

@@ -126,6 +126,18 @@ class WideBand {
   DBuf<long long> ipos, irow;        // interface unknowns: block-vector position / band row
   DBuf<T> Fb, xv, yv, tv, xbt, fbt, t1, t2;
   DBuf<int> flag;
+  // setup workspaces, kept (with everything above) across setups of the
+  // same layout so that a repeated setup does not free and re-allocate
+  DBuf<T> Dw, Lw, Uw, Ww, X, Wt, S, Ws;
+
+  // device bytes this object holds
+  size_t bytes_held() const {
+    size_t b = 0;
+    for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
+                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &gws})
+      b += d->size() * sizeof(T);
+    return b;
+  }
 
   WideBand() = default;
   WideBand(const WideBand&) = delete;
@@ -161,8 +173,9 @@ class WideBand {
     bs = bs_;
     pstart_h = pstart;
     psize_h = psize;
-    cublas_check(cublasCreate(&h), "cublasCreate");
+    if (!h) cublas_check(cublasCreate(&h), "cublasCreate");
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
+    spike = false;
     math_mode(tf32);
     int maxsz = 0;
     for (int v : psize) maxsz = std::max(maxsz, v);
@@ -223,7 +236,6 @@ class WideBand {
   //   D_i <- D_i - L_{i,i-1} U_{i-1,i};  D_i = L_ii U_ii (recursive, with inverses);
   //   U_{i,i+1} = L_ii^-1 E_i;  L_{i+1,i} = F_i U_ii^-1.
   void factor(bool boost) {
-    DBuf<T> Dw, Lw, Uw, Ww;
     Dw.alloc((size_t)P * BB);
     Lw.alloc((size_t)P * BB);
     Uw.alloc((size_t)P * BB);
@@ -259,21 +271,36 @@ class WideBand {
     if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
   }
 
-  // tri: 0 full, 1 lower, 2 upper (see k_tgemv)
+  // tri: 0 full, 1 lower, 2 upper (see k_tgemv).  Grids with fewer than
+  // about 2.5 CTAs per SM split the columns over gridDim.z CTAs.
+  DBuf<T> gws;          // column-split partial sums
+  DBuf<unsigned> gctr;  // column-split arrival counters (zero between launches)
+  template <int V>
+  void gemv_launch(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y,
+                   long long sy, int m, int nbatch, int mode, int tri) {
+    constexpr int R = tgemv_rows<T, V>();
+    const int ntile = (m + R - 1) / R, pairs = (ntile + 1) / 2;
+    const long long base = (long long)pairs * nbatch;
+    int S = (int)std::min<long long>(8, (370 + base - 1) / base);
+    S = std::max(1, std::min(S, m / 256));
+    if (S > 1) {
+      const size_t need = (size_t)nbatch * ntile * S * R, nctr = (size_t)nbatch * ntile;
+      if (gws.size() < need) gws.alloc(need);
+      if (gctr.size() < nctr) {
+        gctr.alloc(nctr);
+        gctr.zero(st);
+      }
+    }
+    k_tgemv<T, V><<<dim3(pairs, nbatch, S), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri,
+                                                                     gws.get(), gctr.get());
+    SAPB_LAUNCHED();
+  }
   void gemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y, long long sy,
             int m, int nbatch, int mode, int tri) {
     constexpr int V = 16 / sizeof(T);  // 16-byte loads
     const bool vec = ld % V == 0 && sA % V == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
-    if (vec) {
-      const int ntile = (m + tgemv_rows<T, V>() - 1) / tgemv_rows<T, V>();
-      k_tgemv<T, V><<<dim3((ntile + 1) / 2, nbatch), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m,
-                                                                             mode, tri);
-    } else {
-      const int ntile = (m + tgemv_rows<T, 1>() - 1) / tgemv_rows<T, 1>();
-      k_tgemv<T, 1><<<dim3((ntile + 1) / 2, nbatch), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m,
-                                                                             mode, tri);
-    }
-    SAPB_LAUNCHED();
+    if (vec) gemv_launch<V>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri);
+    else gemv_launch<1>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri);
   }
 
   // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
@@ -371,7 +398,6 @@ class WideBand {
       pos_d.upload(pos, st);
       const int cs = std::min(ncol, cs_max);
       const long long sX = plen * cs;
-      DBuf<T> X, Wt;
       X.alloc((size_t)nI * sX);
       Wt.alloc((size_t)nI * bs * cs);
       BlockLU<T> ops;
@@ -424,7 +450,6 @@ class WideBand {
     SAPB_LAUNCHED();
     k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 1, K, ldK, sK, Cc.get());
     SAPB_LAUNCHED();
-    DBuf<T> S, Ws;
     DBuf<int> sflag;
     S.alloc((size_t)nI * sK);
     Ws.alloc((size_t)nI * sK);
