@@ -194,15 +194,21 @@ class PrecondT : public PrecBase {
     nb = wide_active ? wide->nb : 0;
   }
 
-  // Half-bandwidths from this value up are factored and applied as block
-  // tridiagonal partitions (wide_host.cuh); above 1024 that is the only
-  // path.  The environment variable SAPB_WIDE_MIN_K overrides the threshold.
-  static int wide_min_k() {
+  // Partitions are factored and applied as block tridiagonal (wide_host.cuh)
+  // when the narrow factor's window (K+1+8 band columns of 2K+1 values) does
+  // not fit in 200 KB of shared memory, where the narrow kernels fall back to
+  // a global-memory window and the block path is faster (FP64 from K ~ 108,
+  // FP32 from K ~ 155 on B200), and always above K = 1024.  The environment
+  // variable SAPB_WIDE_MIN_K sets an explicit threshold instead.
+  static bool use_wide(int kmax) {
+    if (kmax > 1024) return true;
     const char* e = std::getenv("SAPB_WIDE_MIN_K");
     const int v = e ? std::atoi(e) : 0;
-    return v > 0 ? v : 256;
+    if (v > 0) return kmax >= v;
+    constexpr int D = 8;
+    const size_t smem = ((size_t)(kmax + 1 + D) * (2 * kmax + 1) + (kmax + 1 + D)) * sizeof(T);
+    return smem > 200 * 1024;
   }
-  static bool use_wide(int kmax) { return kmax > 1024 || kmax >= wide_min_k(); }
 
   // Boosting of the band factorization (partBandedLU and its variants,
   // sap/precond.h:3882-3983): the variable-band kernels always boost; the

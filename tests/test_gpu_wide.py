@@ -163,3 +163,37 @@ def test_illegal_solver_type_is_unsupported():
     s.setup(A)
     with pytest.raises(sap.LibraryError):
         s.solve(sap.MVBanded(A), np.ones(n), np.zeros(n))
+
+
+@pytest.mark.parametrize("dtype", ["double", "float"])
+def test_narrow_kernels_forced_on_wide_band(monkeypatch, dtype):
+    # bands whose factor window exceeds shared memory go to the block path by
+    # default; the narrow kernels (global-memory factor window, chunked
+    # sweeps) stay available and correct when forced
+    monkeypatch.setenv("SAPB_WIDE_MIN_K", "100000")
+    n, K, P = 40000, 170, 8
+    band = sap.generate_band_host(n, K, 0.8, 2, seed=n + K)
+    A, s, o = setup_pair(band, n, K, P, dtype)
+    assert s.blockLayout()[0] == 0  # narrow path
+    v = np.random.default_rng(5).standard_normal(n)
+    z, zo = apply_gpu(s, v), o.apply(v)
+    assert np.linalg.norm(z - zo) / np.linalg.norm(zo) <= APPLY_TOL[dtype]
+
+
+def test_narrow_var_band_forced(monkeypatch):
+    from saplibrary_b200.problems import convection_diffusion_csr
+    monkeypatch.setenv("SAPB_WIDE_MIN_K", "100000")
+    m, P = 60, 8
+    rp, ci, v, _ = convection_diffusion_csr(m=m, fill_reach=5 * m, seed=m)
+    A = sap.CsrMatrix(rp, ci, v)
+    s = sap.Solver(P, sap.Options(dropOffFraction=1e-4, relTol=1e-10), prec="double")
+    s.setup(A)
+    assert s.blockLayout()[0] == 0 and s.getStats().bandwidth > 108
+    o = oracle.SparsePrecond(P, dtype="double", dropFrac=1e-4)
+    assert o.setup(rp, ci, v) == 0
+    x = np.random.default_rng(6).standard_normal(m * m)
+    vd = torch.tensor(x, device="cuda")
+    zd = torch.empty_like(vd)
+    s.precond(vd, zd)
+    zo = o.apply(x)
+    assert np.linalg.norm(zd.cpu().numpy() - zo) / np.linalg.norm(zo) <= 1e-10
