@@ -682,6 +682,26 @@ __global__ void k_band_from_coo_var(const int* __restrict__ rows, const int* __r
   }
 }
 
+// COO entries (band row, column, value) into the constant band (column-major,
+// 2K+1 values per column).
+template <typename T>
+__global__ void k_band_from_coo_const(const int* __restrict__ rows, const int* __restrict__ cols,
+                                      const T* __restrict__ vals, long long nz, T* __restrict__ B, int K) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nz; e += (long long)gridDim.x * blockDim.x) {
+    const int j = rows[e], l = cols[e];
+    B[(long long)l * (2 * K + 1) + K + (j - l)] = vals[e];
+  }
+}
+
+// update(): out[e] = (T)entries[src[e]] * scale[e] (Precond::update's
+// entries x scaleMap, sap/precond.h:760-768).
+template <typename T>
+__global__ void k_gather_scale(const double* __restrict__ entries, const int* __restrict__ src,
+                               const T* __restrict__ scale, long long m, T* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x)
+    out[e] = (T)entries[src[e]] * scale[e];
+}
+
 // Spike tips of the variable-band method (calculateSpikes_var + spikeSweeps,
 // sap/precond.h:5951-6202), computed exactly: V_i = the rows of
 // A_i^-1 [0; B_i] at the bottom K first-level rows of partition i, W_i = the

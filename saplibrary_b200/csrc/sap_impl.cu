@@ -145,6 +145,7 @@ class PrecBase {
   virtual void setup_sparse(const Csr& A) = 0;
   virtual void apply_band(const double* v, double* z) = 0;
   virtual void block_layout(int& bs, int& nb) const = 0;
+  virtual void update_values(const double* entries, long long nnz, bool device) = 0;
   void apply(const double* v, double* z) { apply_band(v, z); }
 
   void clamp_partitions_banded() {
@@ -187,6 +188,24 @@ class PrecondT : public PrecBase {
   DBuf<T> sin_d, cout_d;  // DB row / column scales in band order (reordered path)
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
+  // Numeric inputs of a CSR setup, on the device: the entries of the
+  // partitions' diagonal blocks (band rows / columns, values; for a constant
+  // band, all entries) and the coupling entries (index into the dense
+  // coupling blocks, values).  update() rewrites the values and reruns the
+  // numeric phase from them.
+  DBuf<int> co_row, co_col;
+  DBuf<T> co_val;
+  DBuf<long long> cp_idx;
+  DBuf<T> cp_val;
+  size_t cp_size = 0;
+  std::vector<int> iface_h;
+  // update() maps (trackReordering): the input entry of every diagonal-block
+  // and coupling entry and its DB scale factor (graph.h:1292-1330 scaleMap,
+  // bandedMatMap / offDiagMap of graph.h:795-886, 1031-1062, 1140-1184)
+  DBuf<int> co_src, cp_src;
+  DBuf<T> co_scale, cp_scale;
+  int numeric_kind = 0;  // 0: no CSR numeric phase, 1: variable band, 2: constant band
+
   std::unique_ptr<WideBand<T>> wide;  // block (GEMM) path of wide bands (buffers kept across setups)
   bool wide_active = false;           // the last setup used the block path
   void block_layout(int& bs, int& nb) const override {
@@ -244,22 +263,6 @@ class PrecondT : public PrecBase {
     return iface;
   }
 
-  // dense coupling blocks on the device from the pipeline's entries
-  void upload_coupling(const rp::Pipeline<T>& pl) {
-    offd.alloc(pl.offd_size);
-    offd.zero(st);
-    if (!pl.offd_idx.empty()) {
-      DBuf<long long> di;
-      DBuf<T> dv;
-      di.upload(pl.offd_idx, st);
-      dv.upload(pl.offd_val, st);
-      const long long m = (long long)pl.offd_idx.size();
-      k_scatter_idx<T><<<grid1d(m), 256, 0, st>>>(di.get(), dv.get(), m, offd.get());
-      SAPB_LAUNCHED();
-      SAPB_CUDA(cudaStreamSynchronize(st));
-    }
-  }
-
   void wide_init(int kmax) {
     wide_check_memory(kmax);
     std::vector<int> ps(P), pz(P);
@@ -285,6 +288,7 @@ class PrecondT : public PrecBase {
   }
 
   void setup_rowmajor(const double* A_dev, int n_, int K_) override {
+    numeric_kind = 0;
     n = n_;
     K = K_;
     clamp_partitions_banded();
@@ -300,6 +304,7 @@ class PrecondT : public PrecBase {
   void setup_csr_direct(const Csr& A, int K_) override {
     n = A.n;
     K = K_;
+    numeric_kind = 0;
     clamp_partitions_banded();
     B.alloc((size_t)(2 * K + 1) * n);
     B.zero(st);
@@ -308,7 +313,77 @@ class PrecondT : public PrecBase {
     SAPB_LAUNCHED();
     SAPB_CUDA(cudaStreamSynchronize(st));
     t_toBanded = ms_since(t1);
+    if (o.trackReordering) {
+      // band position (i, j) of every entry, scale 1 (convertToBandedMatrix
+      // of a CSR matrix, precond.h:2240-2368)
+      std::vector<int> rows(A.nnz), src(A.nnz);
+      for (int i = 0; i < n; i++)
+        for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) rows[e] = i;
+      for (int e = 0; e < A.nnz; e++) src[e] = e;
+      co_row.upload(rows, st);
+      co_col.upload(A.ci_h, st);
+      co_src.upload(src, st);
+      co_scale.upload(std::vector<T>(A.nnz, T(1)), st);
+      co_val.alloc(A.nnz);
+      cp_idx.release();
+      cp_val.release();
+      cp_src.release();
+      cp_scale.release();
+      cp_size = 0;
+      numeric_kind = 2;
+    }
     setup_from_band();
+  }
+
+  // Band from the diagonal-block entries, then the constant-band setup.
+  void numeric_const() {
+    B.alloc((size_t)(2 * K + 1) * n);
+    B.zero(st);
+    const long long m = (long long)co_row.size();
+    if (m) {
+      k_band_from_coo_const<T><<<grid1d(m), 256, 0, st>>>(co_row.get(), co_col.get(), co_val.get(), m, B.get(), K);
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    setup_from_band();
+  }
+
+  // Dense coupling blocks from the coupling entries.
+  void coupling_dense() {
+    offd.alloc(cp_size);
+    offd.zero(st);
+    const long long m = (long long)cp_idx.size();
+    if (m) {
+      k_scatter_idx<T><<<grid1d(m), 256, 0, st>>>(cp_idx.get(), cp_val.get(), m, offd.get());
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // Precond::update (sap/precond.h:751-900): values = entries x scaleMap,
+  // scattered through the maps of the setup, then the numeric phase again.
+  void update_values(const double* entries, long long nnz_in, bool device) override {
+    if (numeric_kind == 0 || co_src.size() != co_row.size())
+      throw Error(SAP_ERR_UNSUPPORTED, "update() needs a CSR setup with trackReordering");
+    DBuf<double> ev;
+    const double* e = entries;
+    if (!device) {
+      ev.upload(entries, (size_t)nnz_in, st);
+      e = ev.get();
+    }
+    const long long m1 = (long long)co_src.size(), m2 = (long long)cp_src.size();
+    if (m1) {
+      k_gather_scale<T><<<grid1d(m1), 256, 0, st>>>(e, co_src.get(), co_scale.get(), m1, co_val.get());
+      SAPB_LAUNCHED();
+    }
+    if (m2) {
+      k_gather_scale<T><<<grid1d(m2), 256, 0, st>>>(e, cp_src.get(), cp_scale.get(), m2, cp_val.get());
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    t_reorder = t_DB = t_dropOff = t_transfer = 0;
+    if (numeric_kind == 1) numeric_var();
+    else numeric_const();
   }
 
   // transformToBandedMatrix (sap/precond.h:1656-2101) and the rest of the
@@ -396,19 +471,14 @@ class PrecondT : public PrecBase {
     reordered = true;
     if (!var_band) {
       // constant band over the whole reordered matrix (assembleBandedMatrix, graph.h:1019-1091)
-      B.alloc((size_t)(2 * K + 1) * n);
-      B.zero(st);
-      DBuf<int> drp, dci;
-      DBuf<double> dv;
-      std::vector<double> mv(pl.m_val.begin(), pl.m_val.end());
-      drp.upload(pl.m_rp, st);
-      dci.upload(pl.m_ci, st);
-      dv.upload(mv, st);
-      k_band_from_csr<T><<<grid_for(n, 256), 256, 0, st>>>(drp.get(), dci.get(), dv.get(), B.get(), n, K);
-      SAPB_LAUNCHED();
-      SAPB_CUDA(cudaStreamSynchronize(st));
+      upload_coo(pl.m_rp, pl.m_ci, pl.m_val);
+      cp_idx.release();
+      cp_val.release();
+      cp_size = 0;
+      numeric_kind = 2;
+      if (o.trackReordering) build_update_maps(A, pl);
       t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
-      setup_from_band();
+      numeric_const();
       return;
     }
     // variable band: partitions with their own K_p (>= 1 for storage)
@@ -433,55 +503,127 @@ class PrecondT : public PrecBase {
     }
     parts_d.upload(parts_h, st);
     partcol_d.upload(partcol, st);
+    boff_total = off;
+    upload_coo(pl.d_rp, pl.d_ci, pl.d_val);
+    cp_idx.upload(pl.offd_idx, st);
+    cp_val.upload(pl.offd_val, st);
+    cp_size = pl.offd_size;
+    iface_h = spike ? var_iface(pl) : std::vector<int>();
+    numeric_kind = 1;
+    if (o.trackReordering) build_update_maps(A, pl);
+    t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
+    numeric_var();
+  }
+
+  long long boff_total = 0;
+
+  // device COO (band rows, columns, values) of a CSR in band order
+  void upload_coo(const std::vector<int>& rp_, const std::vector<int>& ci_, const std::vector<T>& v_) {
+    std::vector<int> rows(ci_.size());
+    for (int i = 0; i < n; i++)
+      for (int e = rp_[i]; e < rp_[i + 1]; e++) rows[e] = i;
+    co_row.upload(rows, st);
+    co_col.upload(ci_, st);
+    co_val.upload(v_, st);
+  }
+
+  // update() maps: every input entry located in the setup's numeric inputs
+  // (its position after DB, RCM, drop-off, the partition split and the
+  // second-level reordering); dropped entries and explicit zeros have none.
+  void build_update_maps(const Csr& A, const rp::Pipeline<T>& pl) {
+    const int q = n / P, rem = n % P;
+    auto part_of = [&](int x) { return x < rem * (q + 1) ? x / (q + 1) : rem + (x - rem * (q + 1)) / q; };
+    const std::vector<int>& rp_ = var_band ? pl.d_rp : pl.m_rp;
+    const std::vector<int>& ci_ = var_band ? pl.d_ci : pl.m_ci;
+    std::vector<int> csrc(ci_.size(), -1), psrc(pl.offd_idx.size(), -1);
+    std::vector<T> cscale(ci_.size(), T(1)), pscale(pl.offd_idx.size(), T(1));
+    std::vector<std::pair<long long, int>> cpl(pl.offd_idx.size());
+    for (size_t k = 0; k < cpl.size(); k++) cpl[k] = {pl.offd_idx[k], (int)k};
+    std::sort(cpl.begin(), cpl.end());
+    const long long KK = (long long)K * K;
+    for (int i = 0; i < n; i++)
+      for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) {
+        if ((T)A.v_h[e] == T(0)) continue;  // removed before reordering (precond.h:1690-1713)
+        const int j = A.ci_h[e];
+        const T sc = pl.scale ? (T)(pl.row_scale[i] * pl.col_scale[j]) : T(1);
+        const int i1 = pl.rcm_pos[pl.db_row_perm[i]], j1 = pl.rcm_pos[j];
+        const int pr = part_of(i1), pc = part_of(j1);
+        if (!var_band || pr == pc) {
+          const int r2 = var_band ? pl.second_pos[i1] : i1, c2 = var_band ? pl.second_pos[j1] : j1;
+          for (int t = rp_[r2]; t < rp_[r2 + 1]; t++)
+            if (ci_[t] == c2) {
+              csrc[t] = e;
+              cscale[t] = sc;
+              break;
+            }
+          continue;
+        }
+        long long idx = -1;
+        if (pc == pr + 1) {
+          const int row_end = q * pr + (pr < rem ? pr + q + 1 : rem + q);
+          const int col_start = q * pc + (pc < rem ? pc : rem);
+          const int a = i1 + K - row_end, c = j1 - col_start;
+          if (a >= 0 && a < K && c >= 0 && c < K) idx = pr * 2 * KK + (long long)a * K + c;
+        } else if (pr == pc + 1) {
+          const int row_start = q * pr + (pr < rem ? pr : rem);
+          const int col_end = q * pc + (pc < rem ? pc + q + 1 : rem + q);
+          const int a = i1 - row_start, c = j1 - col_end + K;
+          if (a >= 0 && a < K && c >= 0 && c < K) idx = (pc * 2 + 1) * KK + (long long)a * K + c;
+        }
+        if (idx < 0) continue;
+        auto it = std::lower_bound(cpl.begin(), cpl.end(), std::make_pair(idx, -1));
+        if (it != cpl.end() && it->first == idx) {
+          psrc[it->second] = e;
+          pscale[it->second] = sc;
+        }
+      }
+    for (int v : csrc)
+      if (v < 0) throw Error(SAP_ERR_CUDA, "update map: a band entry has no input entry");
+    for (int v : psrc)
+      if (v < 0) throw Error(SAP_ERR_CUDA, "update map: a coupling entry has no input entry");
+    co_src.upload(csrc, st);
+    co_scale.upload(cscale, st);
+    cp_src.upload(psrc, st);
+    cp_scale.upload(pscale, st);
+  }
+
+  // The numeric phase of the variable band: band (narrow) or blocks (wide)
+  // from the diagonal-block entries, factors, spike tips, reduced system.
+  void numeric_var() {
+    if (ptype == SAP_PRECOND_NONE) return;
+    auto t0 = Clock::now();
     if (use_wide(parts_maxK())) {
       wide_init(parts_maxK());
-      std::vector<int> rows(pl.d_ci.size());
-      for (int i = 0; i < n; i++)
-        for (int e = pl.d_rp[i]; e < pl.d_rp[i + 1]; e++) rows[e] = i;
-      {
-        DBuf<int> drows, dcols;
-        DBuf<T> dvals;
-        drows.upload(rows, st);
-        dcols.upload(pl.d_ci, st);
-        dvals.upload(pl.d_val, st);
-        wide->load_coo(drows.get(), dcols.get(), dvals.get(), (long long)rows.size());
-      }
-      t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
+      wide->load_coo(co_row.get(), co_col.get(), co_val.get(), (long long)co_row.size());
+      t_cpu_assemble += ms_since(t0);
       auto t2 = Clock::now();
       wide->factor(true);
       t_bandLU = ms_since(t2);
       if (spike) {
-        upload_coupling(pl);
-        wide_couple(var_iface(pl));
+        coupling_dense();
+        wide_couple(iface_h);
       }
       return;
     }
     wide.reset();
-    B.alloc((size_t)off);
+    B.alloc((size_t)boff_total);
     B.zero(st);
     {
-      std::vector<int> rows(pl.d_ci.size());
-      for (int i = 0; i < n; i++)
-        for (int e = pl.d_rp[i]; e < pl.d_rp[i + 1]; e++) rows[e] = i;
-      DBuf<int> drows, dcols;
-      DBuf<T> dvals;
-      drows.upload(rows, st);
-      dcols.upload(pl.d_ci, st);
-      dvals.upload(pl.d_val, st);
-      k_band_from_coo_var<T><<<grid_for((long long)rows.size(), 256, 148 * 32), 256, 0, st>>>(
-          drows.get(), dcols.get(), dvals.get(), (long long)rows.size(), parts_d.get(), partcol_d.get(), B.get());
+      const long long m = (long long)co_row.size();
+      k_band_from_coo_var<T><<<grid_for(m, 256, 148 * 32), 256, 0, st>>>(co_row.get(), co_col.get(), co_val.get(), m,
+                                                                         parts_d.get(), partcol_d.get(), B.get());
       SAPB_LAUNCHED();
       SAPB_CUDA(cudaStreamSynchronize(st));
     }
-    t_cpu_assemble = ms_since(t0) - t_transfer - t_DB - t_reorder - t_dropOff;
+    t_cpu_assemble += ms_since(t0);
     auto t2 = Clock::now();
     factor();
     t_bandLU = ms_since(t2);
     if (spike) {
       t2 = Clock::now();
       const size_t KK = (size_t)K * K;
-      upload_coupling(pl);
-      iface_d.upload(var_iface(pl), st);
+      coupling_dense();
+      iface_d.upload(iface_h, st);
       V.alloc(KK * (P - 1));
       W.alloc(KK * (P - 1));
       S.alloc(KK * (P - 1));
@@ -1500,8 +1642,23 @@ int sap_solver_update(sap_solver* h, const double* entries, int64_t nnz, int mem
       if (accepted) *accepted = 0;
       return SAP_OK;
     }
-    (void)memspace;
-    throw Error(SAP_ERR_UNSUPPORTED, "update() is not available yet");
+    auto t0 = Clock::now();
+    PrecBase& pc = S.pc();
+    pc.update_values(entries, nnz, memspace == SAP_DEVICE);
+    SAPB_CUDA(cudaStreamSynchronize(S.st));
+    // Solver::update statistics (sap/solver.h:440-460)
+    S.stats.timeUpdate = ms_since(t0);
+    S.stats.time_reorder = 0;
+    S.stats.time_DB = 0;
+    S.stats.time_dropOff = 0;
+    S.stats.time_cpu_assemble = pc.t_cpu_assemble;
+    S.stats.time_transfer = pc.t_transfer;
+    S.stats.time_toBanded = pc.t_toBanded;
+    S.stats.time_offDiags = pc.t_offDiags;
+    S.stats.time_bandLU = pc.t_bandLU;
+    S.stats.time_assembly = pc.t_assembly;
+    S.stats.time_fullLU = pc.t_fullLU;
+    if (accepted) *accepted = 1;
   });
 }
 
