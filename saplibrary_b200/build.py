@@ -37,7 +37,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(CSRC, os.path.splitext(src)[0] + ".o")
         cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC, *FLAGS, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj]
+            cmd = [NVCC, *FLAGS, "-Wno-deprecated-gpu-targets", "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

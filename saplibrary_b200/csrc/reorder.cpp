@@ -55,6 +55,30 @@ void csr_from_keys(int n, const std::vector<int>& key, const std::vector<int>& c
   out_rp[n] = (int)m;
 }
 
+// Rows moved as whole units: row r of (rp, ci, val) becomes row newpos[r]
+// with its entries in their order and columns relabelled through colmap
+// (none when null).  This is exactly what the stable counting sort by
+// key = newpos[row] (csr_from_keys) produces, built row-parallel.
+template <typename V>
+void permute_rows(int n, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<V>& val,
+                  const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
+                  std::vector<int>& out_ci, std::vector<V>& out_val) {
+  out_rp.assign(n + 1, 0);
+  for (int r = 0; r < n; r++) out_rp[newpos[r] + 1] = rp[r + 1] - rp[r];
+  for (int i = 0; i < n; i++) out_rp[i + 1] += out_rp[i];
+  out_ci.resize(ci.size());
+  out_val.resize(val.size());
+  const int* cm = colmap ? colmap->data() : nullptr;
+#pragma omp parallel for schedule(static, 4096)
+  for (int r = 0; r < n; r++) {
+    int d = out_rp[newpos[r]];
+    for (int e = rp[r]; e < rp[r + 1]; e++, d++) {
+      out_ci[d] = cm ? cm[ci[e]] : ci[e];
+      out_val[d] = val[e];
+    }
+  }
+}
+
 int partition_of(int r, int q, int rem) {
   int p = r / (q + 1);
   return p >= rem ? rem + (r - rem * (q + 1)) / q : p;
@@ -189,14 +213,12 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
   db_row_perm.resize(n);
   for (int c = 0; c < n; c++) db_row_perm[match[c]] = c;
   // permuted (and scaled) matrix, rows in the new order, entries stable
-  std::vector<int> key(nnz), col(in_ci);
   std::vector<T> val(nnz);
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++)
-    for (int e = Rp[i]; e < Rp[i + 1]; e++) {
-      key[e] = db_row_perm[i];
+    for (int e = Rp[i]; e < Rp[i + 1]; e++)
       val[e] = scale ? (T)(row_scale[i] * col_scale[Ci[e]]) * in_val[e] : in_val[e];
-    }
-  csr_from_keys(n, key, col, val, m_rp, m_ci, m_val);
+  permute_rows(n, Rp, Ci, val, db_row_perm, nullptr, m_rp, m_ci, m_val);
 }
 
 // Symmetrised adjacency of edges [e0, e1) without self loops (duplicates
@@ -204,20 +226,24 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
 // graph.h:1764-1809).
 static void symmetric_adjacency(const std::vector<int>& er, const std::vector<int>& ec, int e0, int e1, int nb,
                                 int ne, int n, std::vector<int>& off, std::vector<int>& adj) {
-  std::vector<int> src;
-  std::vector<int> dst;
-  src.reserve(2 * (size_t)(e1 - e0));
-  dst.reserve(2 * (size_t)(e1 - e0));
+  // each edge (r, c), r != c, contributes (r -> c) then (c -> r); a node's
+  // neighbours keep the order of these contributions
+  off.assign(n + 1, 0);
   for (int e = e0; e < e1; e++) {
     if (er[e] == ec[e]) continue;
-    src.push_back(er[e]); dst.push_back(ec[e]);
-    src.push_back(ec[e]); dst.push_back(er[e]);
+    off[er[e]]++;
+    off[ec[e]]++;
   }
-  off.assign(n + 1, 0);
-  for (int s : src) off[s]++;
   for (int i = nb + 1; i <= ne; i++) off[i] += off[i - 1];
-  adj.resize(dst.size());
-  for (size_t e = dst.size(); e-- > 0;) adj[--off[src[e]]] = dst[e];
+  for (int i = ne - 1; i >= nb; i--) off[i] = i > nb ? off[i - 1] : 0;  // exclusive starts
+  adj.resize(off[ne]);
+  std::vector<int> pos(off.begin() + nb, off.begin() + ne);
+  for (int e = e0; e < e1; e++) {
+    const int r = er[e], c = ec[e];
+    if (r == c) continue;
+    adj[pos[r - nb]++] = c;
+    adj[pos[c - nb]++] = r;
+  }
 }
 
 // One BFS of the Cuthill-McKee order from `root` over nodes [nb, ne):
@@ -227,25 +253,26 @@ static void symmetric_adjacency(const std::vector<int>& er, const std::vector<in
 static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& off, const std::vector<int>& adj,
                    const std::vector<int>* fixed_degree, std::vector<int>& pushed, std::vector<int>& level,
                    std::vector<int>& order, int& last_level) {
-  std::queue<int> fifo;
+  // FIFO as an array: every node enters at most once per trial
+  std::vector<int> fifo((size_t)(ne - nb) + 2);
+  size_t head = 0, tail = 0;
   std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree> kids;
   level[root] = 0;
   pushed[root] = trial;
-  fifo.push(root);
+  fifo[tail++] = root;
   int left = ne - nb, out = nb, scan = nb;
   while (left--) {
-    if (fifo.empty()) {
+    if (head == tail) {
       left++;
       int i = scan;
       while (i < ne && pushed[i] == trial) i++;
       if (i >= ne) return false;
-      fifo.push(i);
+      fifo[tail++] = i;
       pushed[i] = trial;
       scan = i;
       continue;
     }
-    int node = fifo.front();
-    fifo.pop();
+    int node = fifo[head++];
     order[out++] = node;
     int lv = level[node];
     for (int e = off[node]; e < off[node + 1]; e++) {
@@ -258,7 +285,7 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
       last_level = lv + 1;
     }
     while (!kids.empty()) {
-      fifo.push(kids.top().first);
+      fifo[tail++] = kids.top().first;
       kids.pop();
     }
   }
@@ -275,11 +302,13 @@ template <typename T>
 int Pipeline<T>::rcm() {
   const int nz = (int)m_ci.size();
   std::vector<int> row(nz), degree(n);
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) row[e] = i;
     degree[i] = m_rp[i + 1] - m_rp[i];
   }
   int best_bw = 0;
+#pragma omp parallel for reduction(max : best_bw) schedule(static)
   for (int e = 0; e < nz; e++) best_bw = std::max(best_bw, std::abs(row[e] - m_ci[e]));
   std::vector<int> off, adj;
   symmetric_adjacency(row, m_ci, 0, nz, 0, n, n, off, adj);
@@ -311,6 +340,7 @@ int Pipeline<T>::rcm() {
     if (!cm_bfs(root, 0, n, trial, off, adj, &degree, pushed, level, order, unused)) break;
     for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
     int bw = 0;
+#pragma omp parallel for reduction(max : bw) schedule(static)
     for (int e = 0; e < nz; e++) bw = std::max(bw, std::abs(rcm_pos[row[e]] - rcm_pos[m_ci[e]]));
     if (best_bw > bw) {
       best_bw = bw;
@@ -320,13 +350,11 @@ int Pipeline<T>::rcm() {
     if (best_bw <= 256) break;       // BANDWIDTH_THRESHOLD
   }
   for (int k = 0; k < n; k++) rcm_pos[rcm_order[k]] = k;
-  std::vector<int> key(nz), col(nz);
-  for (int e = 0; e < nz; e++) {
-    key[e] = rcm_pos[row[e]];
-    col[e] = rcm_pos[m_ci[e]];
+  {
+    const std::vector<int> rp0 = std::move(m_rp), ci0 = std::move(m_ci);
+    const std::vector<T> v0 = std::move(m_val);
+    permute_rows(n, rp0, ci0, v0, rcm_pos, &rcm_pos, m_rp, m_ci, m_val);
   }
-  std::vector<T> val = m_val;
-  csr_from_keys(n, key, col, val, m_rp, m_ci, m_val);
   return best_bw;
 }
 
@@ -337,60 +365,86 @@ int Pipeline<T>::rcm() {
 template <typename T>
 int Pipeline<T>::drop_off(T frac, int max_bw) {
   const int nz = (int)m_ci.size();
-  std::vector<int> start(n + 1, 0);
+  // The reference's bucketed list: entries ordered by distance |i - j|, rows
+  // ascending and CSR order inside a distance group.  Group d occupies
+  // [gstart[d], gstart[d+1]); only the values are needed (for the squares).
+  std::vector<int> gstart(n + 1, 0);
   for (int i = 0; i < n; i++)
-    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) start[std::abs(i - m_ci[e])]++;
-  for (int d = 0, acc = 0; d < n; d++) { int c = start[d]; start[d] = acc; acc += c; }
-  std::vector<int> br(nz), bc(nz);
+    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) gstart[std::abs(i - m_ci[e]) + 1]++;
+  for (int d = 0; d < n; d++) gstart[d + 1] += gstart[d];
   std::vector<T> bv(nz);
-  for (int i = 0; i < n; i++)
-    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) {
-      int s = start[std::abs(i - m_ci[e])]++;
-      br[s] = i; bc[s] = m_ci[e]; bv[s] = m_val[e];
-    }
+  {
+    std::vector<int> pos(gstart.begin(), gstart.end() - 1);
+    for (int i = 0; i < n; i++)
+      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[pos[std::abs(i - m_ci[e])]++] = m_val[e];
+  }
   T total = T(0);
   for (int e = 0; e < nz; e++) total = total + m_val[e] * m_val[e];
   const T keep_min = (T(1) - frac) * total;
   T kept = total;
-  // walk from the longest distance (the end of the bucketed list)
-  auto dist_at = [&](int k) { int s = nz - 1 - k; return std::abs(br[s] - bc[s]); };
-  auto sq_at = [&](int k) { int s = nz - 1 - k; return bv[s] * bv[s]; };
-  int cut = 0, probe = 0, kres = dist_at(0);
+  // walk the groups from the longest distance down, summing squares from
+  // the end of the list backwards (the reference's order)
+  auto lower = [&](int g) {
+    do g--; while (g > 0 && gstart[g] == gstart[g + 1]);
+    return g;
+  };
+  int g = n;
+  g = lower(g);  // the top non-empty group
+  int kres = g;
   {
-    int d;
-    while ((d = dist_at(probe)) > max_bw) probe++;
     T s = T(0);
-    for (int k = cut; k < probe; k++) s = s + sq_at(k);
+    while (g > max_bw) {
+      for (int p = gstart[g + 1] - 1; p >= gstart[g]; p--) s = s + bv[p] * bv[p];
+      g = lower(g);
+    }
     kept -= s;
-    cut = probe;
-    kres = d;
+    kres = g;
   }
   if (kept >= keep_min) {
     for (;;) {
-      int d = dist_at(cut);
+      const int d = g;
       if (d == 0) { kres = 0; break; }
-      do { probe++; } while (dist_at(probe) == d);
       T band = T(0);
-      for (int k = cut; k < probe; k++) band = band + sq_at(k);
+      for (int p = gstart[g + 1] - 1; p >= gstart[g]; p--) band = band + bv[p] * bv[p];
       if (kept - band < keep_min) break;
       kept -= band;
-      cut = probe;
       kres = d;
+      g = lower(g);
     }
   }
   drop_actual = T(1) - kept / total;
-  const int keep = nz - cut;
-  // rebuild sorted by row, then column: stable by column, then by row
-  std::vector<int> cstart(n + 1, 0);
-  for (int k = 0; k < keep; k++) cstart[bc[k]]++;
-  for (int d = 0, acc = 0; d < n; d++) { int c = cstart[d]; cstart[d] = acc; acc += c; }
-  std::vector<int> tr(keep), tc(keep);
-  std::vector<T> tv(keep);
-  for (int k = 0; k < keep; k++) {
-    int s = cstart[bc[k]]++;
-    tr[s] = br[k]; tc[s] = bc[k]; tv[s] = bv[k];
+  // kept: every entry within distance g, sorted by row, then column (what
+  // the reference's two stable counting sorts of the kept list give)
+  const int dkeep = g;
+  const std::vector<int> rp0 = std::move(m_rp), ci0 = std::move(m_ci);
+  const std::vector<T> v0 = std::move(m_val);
+  m_rp.assign(n + 1, 0);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    int c = 0;
+    for (int e = rp0[i]; e < rp0[i + 1]; e++) c += std::abs(i - ci0[e]) <= dkeep;
+    m_rp[i + 1] = c;
   }
-  csr_from_keys(n, tr, tc, tv, m_rp, m_ci, m_val);
+  for (int i = 0; i < n; i++) m_rp[i + 1] += m_rp[i];
+  m_ci.resize(m_rp[n]);
+  m_val.resize(m_rp[n]);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    const int a = m_rp[i];
+    int w = a;
+    for (int e = rp0[i]; e < rp0[i + 1]; e++) {
+      if (std::abs(i - ci0[e]) > dkeep) continue;
+      // insertion by column (columns of a row are distinct)
+      int t = w++;
+      while (t > a && m_ci[t - 1] > ci0[e]) {
+        m_ci[t] = m_ci[t - 1];
+        m_val[t] = m_val[t - 1];
+        t--;
+      }
+      m_ci[t] = ci0[e];
+      m_val[t] = v0[e];
+    }
+  }
   return kres;
 }
 
@@ -514,13 +568,11 @@ void Pipeline<T>::second_level(int K, int P) {
     second_pos.assign(n, 0);
     for (int p = 0; p < P; p++) part(p, true);
   }
-  std::vector<int> key(dz), col(dz);
-  for (int e = 0; e < dz; e++) {
-    key[e] = second_pos[row[e]];
-    col[e] = second_pos[d_ci[e]];
+  {
+    const std::vector<int> rp0 = std::move(d_rp), ci0 = std::move(d_ci);
+    const std::vector<T> v0 = std::move(d_val);
+    permute_rows(n, rp0, ci0, v0, second_pos, &second_pos, d_rp, d_ci, d_val);
   }
-  std::vector<T> val = d_val;
-  csr_from_keys(n, key, col, val, d_rp, d_ci, d_val);
   first_rows.assign(std::max(P - 1, 0), 0);
   int last = 0;
   for (int i = 0; i < P - 1; i++) {

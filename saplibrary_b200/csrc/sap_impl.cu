@@ -405,22 +405,36 @@ class PrecondT : public PrecBase {
     pl.max_bandwidth = o.maxBandwidth;
     pl.var_band = o.variableBandwidth != 0;
     // the matrix in the preconditioner's value type, explicit zeros removed
+    // (row-parallel: count, prefix, fill)
     pl.in_rp.assign(n + 1, 0);
-    pl.in_ci.reserve(A.nnz);
-    pl.in_val.reserve(A.nnz);
+#pragma omp parallel for schedule(static, 4096)
     for (int i = 0; i < n; i++) {
+      int c = 0;
+      for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) c += (T)A.v_h[e] != T(0);
+      pl.in_rp[i + 1] = c;
+    }
+    for (int i = 0; i < n; i++) pl.in_rp[i + 1] += pl.in_rp[i];
+    pl.in_ci.resize(pl.in_rp[n]);
+    pl.in_val.resize(pl.in_rp[n]);
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; i++) {
+      int d = pl.in_rp[i];
       for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) {
-        T a = (T)A.v_h[e];
-        if (a != T(0)) { pl.in_ci.push_back(A.ci_h[e]); pl.in_val.push_back(a); }
+        const T a = (T)A.v_h[e];
+        if (a != T(0)) {
+          pl.in_ci[d] = A.ci_h[e];
+          pl.in_val[d++] = a;
+        }
       }
-      pl.in_rp[i + 1] = (int)pl.in_ci.size();
     }
     pl.nnz = (int)pl.in_ci.size();
     std::vector<double> w, rmax;
     if (pl.do_db) {
       DBuf<int> drp;
       DBuf<double> da, dw, dmax;
-      std::vector<double> av(pl.in_val.begin(), pl.in_val.end());
+      std::vector<double> av(pl.in_val.size());
+#pragma omp parallel for schedule(static, 65536)
+      for (long long e = 0; e < (long long)av.size(); e++) av[e] = (double)pl.in_val[e];
       drp.upload(pl.in_rp, st);
       da.upload(av, st);
       dw.alloc(av.size());
