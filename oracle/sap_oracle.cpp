@@ -565,6 +565,133 @@ struct Monitor {
 
 using Apply = std::function<void(const std::vector<double>&, std::vector<double>&)>;
 
+// Monitor::finished (sap/monitor.h:134-149), the default monitor of the
+// BiCGStab and MINRES drivers.
+static bool finished_default(Monitor& mon, double r) {
+  mon.rNorm = r;
+  if (mon.code != 0) return true;
+  if (std::isnan(mon.rNorm)) mon.stop(-2, "Residual norm is NaN");
+  else if (mon.rNorm <= mon.tol()) mon.stop(1, "Converged");
+  else if (mon.it > mon.maxIt) mon.stop(-1, "Maximum number of iterations was reached");
+  return mon.code != 0;
+}
+
+// cusp::blas::axpbypcz: out = a x + b y + c z
+static void axpbypcz(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z,
+                     std::vector<double>& out, double a, double b, double c) {
+  for (size_t i = 0; i < out.size(); i++) out[i] = a * x[i] + b * y[i] + c * z[i];
+}
+
+// sap::bicgstab (sap/bicgstab.h:50-155), restated line by line.
+static void bicgstab_classic(const Apply& A, const Apply& M, std::vector<double>& x, const std::vector<double>& b,
+                             Monitor& mon) {
+  const size_t N = b.size();
+  std::vector<double> y(N), p(N), r(N), r_star(N), s(N), Mp(N), AMp(N), Ms(N), AMs(N);
+  A(x, y);
+  axpby(b, y, r, 1.0, -1.0);
+  p = r;
+  r_star = r;
+  double r_r_star_old = dot(r_star, r);
+  while (!finished_default(mon, nrm2(r))) {
+    if (r_r_star_old == 0) { mon.stop(-10, "r_r_star is zero"); break; }
+    M(p, Mp);
+    A(Mp, AMp);
+    const double tmp1 = dot(r_star, AMp);
+    if (tmp1 == 0) { mon.stop(-11, "r_star * AMp is zero"); break; }
+    const double alpha = r_r_star_old / tmp1;
+    axpby(r, AMp, s, 1.0, -alpha);
+    if (finished_default(mon, nrm2(s))) {
+      axpby(x, Mp, x, 1.0, alpha);
+      break;
+    }
+    M(s, Ms);
+    A(Ms, AMs);
+    const double tmp2 = dot(AMs, AMs);
+    if (tmp2 == 0) { mon.stop(-12, "AMs * AMs is zero"); break; }
+    const double omega = dot(AMs, s) / tmp2;
+    axpbypcz(x, Mp, Ms, x, 1.0, alpha, omega);
+    axpby(s, AMs, r, 1.0, -omega);
+    const double r_r_star_new = dot(r_star, r);
+    const double beta = (r_r_star_new / r_r_star_old) * (alpha / omega);
+    r_r_star_old = r_r_star_new;
+    axpbypcz(r, p, AMp, p, 1.0, beta, -beta * omega);
+    mon.it += 1.f;
+  }
+}
+
+// sap::minres (sap/minres.h:40-195), restated line by line.
+static void minres(const Apply& A, const Apply& P, std::vector<double>& x, const std::vector<double>& b,
+                   Monitor& mon) {
+  const double eps = std::numeric_limits<double>::epsilon();
+  const size_t n = b.size();
+  auto count = [&]() { return (size_t)(mon.it + 0.5f); };
+  std::vector<double> y(n), r1(n);
+  A(x, r1);
+  axpby(b, r1, r1, 1.0, -1.0);
+  P(r1, y);
+  double beta1 = dot(r1, y);
+  if (beta1 < 0) {
+    mon.stop(-10, "The preconditioner is not positive definite");
+    beta1 *= -1;
+  } else if (beta1 > 0) {
+    beta1 = std::sqrt(beta1);
+  }
+  double Anorm = 0, ynorm = 0, phibar = beta1;
+  double oldb = 0, beta = beta1, dbar = 0, epsln = 0, oldeps = 0;
+  double phi = 0, rhs1 = beta1, rhs2 = 0, tnorm2 = 0;
+  double cs = -1, sn = 0, gmax = 0, gmin = std::numeric_limits<double>::max();
+  double alpha = 0, gamma = 0, delta = 0, gbar = 0, z = 0;
+  std::vector<double> v(n), w(n, 0.0), w1(n, 0.0), w2(n, 0.0), r2 = r1;
+  while (!finished_default(mon, phibar)) {
+    const double s = 1 / beta;
+    for (size_t i = 0; i < n; i++) v[i] = y[i] * s;
+    A(v, y);
+    if (count() > 0) axpby(y, r1, y, 1.0, -beta / oldb);
+    alpha = dot(v, y);
+    axpby(y, r2, y, 1.0, -alpha / beta);
+    r1 = r2;
+    r2 = y;
+    P(r2, y);
+    oldb = beta;
+    beta = dot(r2, y);
+    if (beta < 0) { mon.stop(-10, "The preconditioner is not positive definite"); break; }
+    beta = std::sqrt(beta);
+    tnorm2 += alpha * alpha + oldb * oldb + beta * beta;
+    if (count() == 0 && beta / beta1 <= 10 * eps) mon.stop(10, "beta2 = 0. If M = I, b and x are eigenvectors");
+    oldeps = epsln;
+    delta = cs * dbar + sn * alpha;
+    gbar = sn * dbar - cs * alpha;
+    epsln = sn * beta;
+    dbar = -cs * beta;
+    const double root = std::sqrt(gbar * gbar + dbar * dbar);
+    gamma = std::sqrt(gbar * gbar + beta * beta);
+    gamma = std::max(gamma, eps);
+    cs = gbar / gamma;
+    sn = beta / gamma;
+    phi = cs * phibar;
+    phibar = sn * phibar;
+    const double denom = 1 / gamma;
+    w1 = w2;
+    w2 = w;
+    axpbypcz(v, w1, w2, w, denom, -oldeps * denom, -delta * denom);
+    axpby(x, w, x, 1.0, phi);
+    gmax = std::max(gmax, gamma);
+    gmin = std::min(gmin, gamma);
+    z = rhs1 / gamma;
+    rhs1 = rhs2 - delta * z;
+    rhs2 = -epsln * z;
+    Anorm = std::sqrt(tnorm2);
+    ynorm = nrm2(x);
+    if (mon.code != 10) {
+      const double test2 = root / Anorm, Acond = gmax / gmin;
+      if (Acond >= 0.1 / eps) mon.stop(11, "x has converged to an eigenvector");
+      if (Anorm * eps * ynorm >= beta1) mon.stop(12, "Reasonable accuracy achieved, given eps");
+      if (test2 <= mon.absTol) mon.stop(13, "A least-squares solution was found, given tol");
+    }
+    mon.it += 1.f;
+  }
+}
+
 // bicgstabl<..., L> (sap/bicgstab2.h:32-360), restated line by line.
 static void bicgstabl(const Apply& A, const Apply& P, std::vector<double>& x,
                       const std::vector<double>& b, Monitor& mon, int L) {
@@ -841,7 +968,10 @@ int orc_solve(void* h, int n, int K, const double* band, const int* rp, const in
   orc::Apply Pm = [&](const std::vector<double>& in, std::vector<double>& out) {
     H->visit([&](auto& pc) { orc::apply(pc, in.data(), out.data()); return 0; });
   };
-  orc::bicgstabl(A, Pm, xv, bv, mon, L);
+  // L >= 1: BiCGStab(L); L == 0: sap::bicgstab; L == -1: sap::minres
+  if (L >= 1) orc::bicgstabl(A, Pm, xv, bv, mon, L);
+  else if (L == 0) orc::bicgstab_classic(A, Pm, xv, bv, mon);
+  else orc::minres(A, Pm, xv, bv, mon);
   std::copy(xv.begin(), xv.end(), x);
   res->code = mon.code; res->iterations = mon.it; res->rhs_norm = mon.rhsNorm;
   res->res_norm = mon.rNorm; res->rel_res_norm = mon.rNorm / mon.rhsNorm;

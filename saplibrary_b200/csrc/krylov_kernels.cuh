@@ -118,4 +118,12 @@ k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ c
   }
 }
 
+
+// out = a x + b y + c z (cusp::blas::axpbypcz); out may alias an input
+static __global__ void k_axpbypcz(int n, double a, const double* x, double b, const double* y, double c,
+                                  const double* z, double* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = a * x[i] + b * y[i] + c * z[i];
+}
+
 }  // namespace sapb

@@ -1145,10 +1145,139 @@ class Solver {
     SAPB_CUDA(cudaStreamSynchronize(st));
   }
 
-  // The Krylov method of the options: BiCGStab(L) or flexible GMRES(50).
+  // Monitor::finished (sap/monitor.h:134-149): the default monitor of the
+  // BiCGStab and MINRES drivers.
+  bool finished_default(double r) {
+    mon.rNorm = r;
+    if (mon.code != 0) return true;
+    if (std::isnan(r)) mon.stop(-2, "Residual norm is NaN");
+    else if (r <= mon.tol()) mon.stop(1, "Converged");
+    else if (mon.it > mon.maxIt) mon.stop(-1, "Maximum number of iterations was reached");
+    return mon.code != 0;
+  }
+  void axpbypcz(const double* x, const double* y, const double* z, double* out, double a, double b, double c) {
+    k_axpbypcz<<<grid_for(n, 256), 256, 0, st>>>(n, a, x, b, y, c, z, out);
+    SAPB_LAUNCHED();
+  }
+
+  // sap::bicgstab (sap/bicgstab.h:50-155)
+  void bicgstab_classic(const Spmv& A, double* x, const double* b) {
+    double *y = wsv(70), *p = wsv(71), *r = wsv(72), *rs = wsv(73), *s = wsv(74), *Mp = wsv(75), *AMp = wsv(76),
+           *Ms = wsv(77), *AMs = wsv(78);
+    A.apply(x, y, st);
+    axpby(b, y, r, 1.0, -1.0);
+    copy(r, p);
+    copy(r, rs);
+    double rr_old = dot(rs, r);
+    while (!finished_default(nrm2(r))) {
+      if (rr_old == 0) { mon.stop(-10, "r_r_star is zero"); break; }
+      pcp->apply(p, Mp);
+      A.apply(Mp, AMp, st);
+      const double t1 = dot(rs, AMp);
+      if (t1 == 0) { mon.stop(-11, "r_star * AMp is zero"); break; }
+      const double alpha = rr_old / t1;
+      axpby(r, AMp, s, 1.0, -alpha);
+      if (finished_default(nrm2(s))) {
+        axpby(x, Mp, x, 1.0, alpha);
+        break;
+      }
+      pcp->apply(s, Ms);
+      A.apply(Ms, AMs, st);
+      const double t2 = dot(AMs, AMs);
+      if (t2 == 0) { mon.stop(-12, "AMs * AMs is zero"); break; }
+      const double omega = dot(AMs, s) / t2;
+      axpbypcz(x, Mp, Ms, x, 1.0, alpha, omega);
+      axpby(s, AMs, r, 1.0, -omega);
+      const double rr_new = dot(rs, r);
+      const double beta = (rr_new / rr_old) * (alpha / omega);
+      rr_old = rr_new;
+      axpbypcz(r, p, AMp, p, 1.0, beta, -beta * omega);
+      mon.it += 1.f;
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // sap::minres (sap/minres.h:40-195): preconditioned Lanczos with Givens
+  // rotations, stop codes 10-13 and -10 as in the reference.
+  void minres(const Spmv& A, double* x, const double* b) {
+    const double eps = std::numeric_limits<double>::epsilon();
+    auto count = [&]() { return (size_t)(mon.it + 0.5f); };
+    double *y = wsv(80), *r1 = wsv(81), *v = wsv(82), *w = wsv(83), *w1 = wsv(84), *w2 = wsv(85), *r2 = wsv(86);
+    A.apply(x, r1, st);
+    axpby(b, r1, r1, 1.0, -1.0);
+    pcp->apply(r1, y);
+    double beta1 = dot(r1, y);
+    if (beta1 < 0) {
+      mon.stop(-10, "The preconditioner is not positive definite");
+      beta1 *= -1;
+    } else if (beta1 > 0) {
+      beta1 = std::sqrt(beta1);
+    }
+    double Anorm = 0, ynorm = 0, phibar = beta1;
+    double oldb = 0, beta = beta1, dbar = 0, epsln = 0, oldeps = 0;
+    double phi = 0, rhs1 = beta1, rhs2 = 0, tnorm2 = 0;
+    double cs = -1, sn = 0, gmax = 0, gmin = std::numeric_limits<double>::max();
+    double alpha = 0, gamma = 0, delta = 0, gbar = 0, z = 0;
+    for (double* q : {w, w1, w2}) SAPB_CUDA(cudaMemsetAsync(q, 0, (size_t)n * sizeof(double), st));
+    copy(r1, r2);
+    while (!finished_default(phibar)) {
+      const double s = 1 / beta;
+      axpby(y, y, v, s, 0.0);
+      A.apply(v, y, st);
+      if (count() > 0) axpby(y, r1, y, 1.0, -beta / oldb);
+      alpha = dot(v, y);
+      axpby(y, r2, y, 1.0, -alpha / beta);
+      copy(r2, r1);
+      copy(y, r2);
+      pcp->apply(r2, y);
+      oldb = beta;
+      beta = dot(r2, y);
+      if (beta < 0) { mon.stop(-10, "The preconditioner is not positive definite"); break; }
+      beta = std::sqrt(beta);
+      tnorm2 += alpha * alpha + oldb * oldb + beta * beta;
+      if (count() == 0 && beta / beta1 <= 10 * eps) mon.stop(10, "beta2 = 0. If M = I, b and x are eigenvectors");
+      oldeps = epsln;
+      delta = cs * dbar + sn * alpha;
+      gbar = sn * dbar - cs * alpha;
+      epsln = sn * beta;
+      dbar = -cs * beta;
+      const double root = std::sqrt(gbar * gbar + dbar * dbar);
+      gamma = std::sqrt(gbar * gbar + beta * beta);
+      gamma = std::max(gamma, eps);
+      cs = gbar / gamma;
+      sn = beta / gamma;
+      phi = cs * phibar;
+      phibar = sn * phibar;
+      const double denom = 1 / gamma;
+      copy(w2, w1);
+      copy(w, w2);
+      axpbypcz(v, w1, w2, w, denom, -oldeps * denom, -delta * denom);
+      axpby(x, w, x, 1.0, phi);
+      gmax = std::max(gmax, gamma);
+      gmin = std::min(gmin, gamma);
+      z = rhs1 / gamma;
+      rhs1 = rhs2 - delta * z;
+      rhs2 = -epsln * z;
+      Anorm = std::sqrt(tnorm2);
+      ynorm = nrm2(x);
+      if (mon.code != 10) {
+        const double test2 = root / Anorm, Acond = gmax / gmin;
+        if (Acond >= 0.1 / eps) mon.stop(11, "x has converged to an eigenvector");
+        if (Anorm * eps * ynorm >= beta1) mon.stop(12, "Reasonable accuracy achieved, given eps");
+        if (test2 <= mon.absTol) mon.stop(13, "A least-squares solution was found, given tol");
+      }
+      mon.it += 1.f;
+    }
+    SAPB_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // The Krylov method of the options: L > 0 BiCGStab(L), L == 0 flexible
+  // GMRES(50), L == -1 sap::bicgstab, L == -2 sap::minres.
   void krylov(const Spmv& A, double* x, const double* b, int L) {
     if (L > 0) bicgstabl(A, x, b, L);
-    else fgmres(A, x, b, 50);
+    else if (L == 0) fgmres(A, x, b, 50);
+    else if (L == -1) bicgstab_classic(A, x, b);
+    else minres(A, x, b);
   }
 
   // FP64 iterative refinement around bicgstabl (options.refinementSweeps):
@@ -1685,8 +1814,10 @@ int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, 
     int L = 0;
     if (S.opts.solverType == SAP_BICGSTAB2) L = 2;
     else if (S.opts.solverType == SAP_BICGSTAB1) L = 1;
+    else if (S.opts.solverType == SAP_BICGSTAB) L = -1;
+    else if (S.opts.solverType == SAP_MINRES) L = -2;
     else if (S.opts.solverType != SAP_FGMRES)
-      throw Error(SAP_ERR_UNSUPPORTED, "only BiCGStab1 / BiCGStab2 and the FGMRES extension are provided");
+      throw Error(SAP_ERR_UNSUPPORTED, "the CUSP solvers (BiCGStab_C, GMRES_C, CG_C, CR_C) are not provided");
     auto t0 = Clock::now();
     const size_t bytes = (size_t)S.n * sizeof(double);
     S.bvec.alloc(S.n);

@@ -80,3 +80,16 @@ def band_to_csr(band, n, K):
     rp = np.zeros(n + 1, np.int64)
     np.add.at(rp, rows + 1, 1)
     return np.cumsum(rp).astype(np.int32), cols.astype(np.int32), vals
+
+
+def spd_band(n, K, seed):
+    """Row-major band (n x (2K+1)) of a symmetric, strictly diagonally
+    dominant matrix with a positive diagonal (hence SPD)."""
+    rng = np.random.default_rng(seed)
+    band = np.zeros((n, 2 * K + 1))
+    for d in range(1, K + 1):
+        vals = rng.uniform(-1.0, 1.0, n - d)
+        band[: n - d, K + d] = vals   # A(i, i+d)
+        band[d:, K - d] = vals        # A(i+d, i)
+    band[:, K] = 1.2 * np.abs(band).sum(axis=1)
+    return band.ravel()

@@ -154,11 +154,11 @@ def test_fgmres_narrow_band_matches_direct():
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) <= 1e-8
 
 
-def test_illegal_solver_type_is_unsupported():
+def test_cusp_solver_type_is_unsupported():
     n, K = 2000, 4
     band = sap.generate_band_host(n, K, 1.0, 1, seed=2)
     A = sap.BandedMatrix.from_array(band, n, K)
-    opts = sap.Options(solverType=sap.MINRES, performReorder=False, variableBandwidth=False, applyScaling=False)
+    opts = sap.Options(solverType=sap.CG_C, performReorder=False, variableBandwidth=False, applyScaling=False)
     s = sap.Solver(2, opts, prec="double")
     s.setup(A)
     with pytest.raises(sap.LibraryError):

@@ -109,3 +109,17 @@ def test_unit_test_float_preconditioner_stagnates(unit_test_problem):
     x, res = pc.solve(b, csr=(rp, ci, v), L=2, maxit=100, reltol=1e-13)
     assert res.code == -3
     assert res.rel_res_norm < 1e-6
+
+
+def test_oracle_classic_bicgstab_and_minres_converge():
+    from tests.helpers import spd_band
+    n, K, P = 3000, 6, 3
+    band = spd_band(n, K, seed=3)
+    xt = np.linspace(1.0, 2.0, n)
+    b = oracle.spmv_banded(band, n, K, xt)
+    for L in (0, -1):
+        o = oracle.Precond(P, fact=1, ptype=1, dtype="double")
+        assert o.setup_banded(band, n, K) == 0
+        x, res = o.solve(b, band=band, K=K, L=L, maxit=200, reltol=1e-10)
+        assert res.code > 0, (L, res.code)
+        assert np.linalg.norm(x - xt) / np.linalg.norm(xt) <= 1e-8
