@@ -257,6 +257,20 @@ int64_t sap_library_call_count(void);
 int sap_profile_select(const char* kernel_name);
 int sap_profile_read(double* total_ms, int64_t* launches);
 
+/* ---- Matrix Market input ---------------------------------------------------
+ * Replaces cusp::io::read_matrix_market_file of the reference drivers
+ * (examples/driver_mm.cu).  Matrices: coordinate real / integer / pattern,
+ * general / symmetric / skew-symmetric, returned as CSR (rows and columns
+ * sorted, duplicates summed).  Call once with row_offsets / col_indices /
+ * values NULL to get the sizes, then again with arrays of n_rows + 1 and nnz
+ * elements.  Vectors: array (one column) or coordinate; call with values
+ * NULL for the length.  Errors return SAP_ERR_INVALID_ARGUMENT with the
+ * reason in sap_mm_last_error(). */
+int sap_mm_read_csr(const char* path, int* n_rows, int* n_cols, int64_t* nnz, int* row_offsets, int* col_indices,
+                    double* values);
+int sap_mm_read_vector(const char* path, int64_t* n, double* values);
+const char* sap_mm_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

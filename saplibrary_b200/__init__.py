@@ -89,6 +89,10 @@ _sig = {
     "sap_last_error": (ctypes.c_char_p, []),
     "sap_kernel_launch_count": (ctypes.c_int64, []),
     "sap_library_call_count": (ctypes.c_int64, []),
+    "sap_mm_read_csr": (_i, [ctypes.c_char_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_int64),
+                             _vp, _vp, _vp]),
+    "sap_mm_read_vector": (_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), _vp]),
+    "sap_mm_last_error": (ctypes.c_char_p, []),
     "sap_solver_block_layout": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_options_default": (_i, [ctypes.POINTER(_COptions)]),
     "sap_banded_create": (_i, [_i, _i, _vp, _i, _pp]),
@@ -155,6 +159,40 @@ def _ptr(a):
 def kernel_launch_count() -> int:
     """Number of kernels this library has enqueued since it was loaded."""
     return int(_lib.sap_kernel_launch_count())
+
+
+def read_matrix_market(path: str):
+    """CSR arrays (row_offsets int32, column_indices int32, values float64) and
+    the shape of a Matrix Market coordinate matrix (the reference drivers'
+    cusp::io::read_matrix_market_file); duplicates summed, rows and columns
+    sorted.  Host-side only: pass the arrays to CsrMatrix for the device."""
+    m, n, nnz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+    bp = path.encode()
+    code = _lib.sap_mm_read_csr(bp, ctypes.byref(m), ctypes.byref(n), ctypes.byref(nnz), None, None, None)
+    if code:
+        raise LibraryError(code, (_lib.sap_mm_last_error() or b"").decode())
+    rp = np.empty(m.value + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    v = np.empty(nnz.value, np.float64)
+    code = _lib.sap_mm_read_csr(bp, ctypes.byref(m), ctypes.byref(n), ctypes.byref(nnz), rp.ctypes.data,
+                                ci.ctypes.data, v.ctypes.data)
+    if code:
+        raise LibraryError(code, (_lib.sap_mm_last_error() or b"").decode())
+    return rp, ci, v, (m.value, n.value)
+
+
+def read_matrix_market_vector(path: str) -> np.ndarray:
+    """A Matrix Market vector (array or one-column coordinate) as float64."""
+    n = ctypes.c_int64()
+    bp = path.encode()
+    code = _lib.sap_mm_read_vector(bp, ctypes.byref(n), None)
+    if code:
+        raise LibraryError(code, (_lib.sap_mm_last_error() or b"").decode())
+    out = np.empty(n.value, np.float64)
+    code = _lib.sap_mm_read_vector(bp, ctypes.byref(n), out.ctypes.data)
+    if code:
+        raise LibraryError(code, (_lib.sap_mm_last_error() or b"").decode())
+    return out
 
 
 def library_call_count() -> int:
