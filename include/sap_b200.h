@@ -257,6 +257,26 @@ int64_t sap_library_call_count(void);
 int sap_profile_select(const char* kernel_name);
 int sap_profile_read(double* total_ms, int64_t* launches);
 
+/* ---- learned solver settings (no counterpart in the reference) -------------
+ * A multilayer perceptron in -> h1 -> h2 -> out (ReLU hidden layers, softmax
+ * output) mapping matrix features to a choice of solver settings, trained and
+ * evaluated on the GPU by this library's kernels (FP32, deterministic).
+ * Parameters are one flat float array: W1 [h1][in], b1, W2 [h2][h1], b2,
+ * W3 [out][h2], b3.  Features, labels and outputs are host arrays. */
+typedef struct sap_mlp sap_mlp;
+int sap_mlp_create(int in, int h1, int h2, int out, uint64_t seed, sap_mlp** mlp);
+int sap_mlp_destroy(sap_mlp* mlp);
+int sap_mlp_num_params(const sap_mlp* mlp);
+int sap_mlp_get_params(sap_mlp* mlp, float* params);
+int sap_mlp_set_params(sap_mlp* mlp, const float* params);
+/* logits[batch][out] of features x[batch][in] */
+int sap_mlp_forward(sap_mlp* mlp, const float* x, int batch, float* logits);
+/* mean softmax cross-entropy over the batch and its gradient (flat layout) */
+int sap_mlp_gradients(sap_mlp* mlp, const float* x, const int* labels, int batch, float* grads, float* loss);
+/* `epochs` full-batch Adam steps (beta 0.9 / 0.999); final mean loss */
+int sap_mlp_train(sap_mlp* mlp, const float* x, const int* labels, int batch, int epochs, float lr, float* loss);
+const char* sap_mlp_last_error(void);
+
 /* ---- Matrix Market input ---------------------------------------------------
  * Replaces cusp::io::read_matrix_market_file of the reference drivers
  * (examples/driver_mm.cu).  Matrices: coordinate real / integer / pattern,

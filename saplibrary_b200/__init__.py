@@ -93,6 +93,15 @@ _sig = {
                              _vp, _vp, _vp]),
     "sap_mm_read_vector": (_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), _vp]),
     "sap_mm_last_error": (ctypes.c_char_p, []),
+    "sap_mlp_create": (_i, [_i, _i, _i, _i, ctypes.c_uint64, _pp]),
+    "sap_mlp_destroy": (_i, [_vp]),
+    "sap_mlp_num_params": (_i, [_vp]),
+    "sap_mlp_get_params": (_i, [_vp, _vp]),
+    "sap_mlp_set_params": (_i, [_vp, _vp]),
+    "sap_mlp_forward": (_i, [_vp, _vp, _i, _vp]),
+    "sap_mlp_gradients": (_i, [_vp, _vp, _vp, _i, _vp, ctypes.POINTER(ctypes.c_float)]),
+    "sap_mlp_train": (_i, [_vp, _vp, _vp, _i, _i, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]),
+    "sap_mlp_last_error": (ctypes.c_char_p, []),
     "sap_solver_block_layout": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_options_default": (_i, [ctypes.POINTER(_COptions)]),
     "sap_banded_create": (_i, [_i, _i, _vp, _i, _pp]),

@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
-SOURCES = ["sap_impl.cu", "dots_noalloc.cu", "gen.cpp", "reorder.cpp", "mmio.cpp"]
+SOURCES = ["sap_impl.cu", "dots_noalloc.cu", "mlp.cu", "gen.cpp", "reorder.cpp", "mmio.cpp"]
 
 
 def _newest_source_mtime() -> float:

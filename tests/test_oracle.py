@@ -123,3 +123,19 @@ def test_oracle_classic_bicgstab_and_minres_converge():
         x, res = o.solve(b, band=band, K=K, L=L, maxit=200, reltol=1e-10)
         assert res.code > 0, (L, res.code)
         assert np.linalg.norm(x - xt) / np.linalg.norm(xt) <= 1e-8
+
+
+def test_mlp_oracle_gradient_matches_central_differences():
+    from oracle import mlp_oracle
+    rng = np.random.default_rng(2)
+    shape = (16, 8, 8, 7)
+    n = 8 * 16 + 8 + 8 * 8 + 8 + 7 * 8 + 7
+    p = rng.standard_normal(n) * 0.3
+    X = rng.standard_normal((30, 16))
+    y = rng.integers(0, 7, 30)
+    _, g = mlp_oracle.loss_and_grad(p, shape, X, y)
+    for k in range(0, n, 17):
+        e = np.zeros(n)
+        e[k] = 1e-6
+        d = (mlp_oracle.loss_and_grad(p + e, shape, X, y)[0] - mlp_oracle.loss_and_grad(p - e, shape, X, y)[0]) / 2e-6
+        assert abs(d - g[k]) <= 1e-6 + 1e-5 * abs(g[k])
