@@ -257,6 +257,25 @@ int64_t sap_library_call_count(void);
 int sap_profile_select(const char* kernel_name);
 int sap_profile_read(double* total_ms, int64_t* launches);
 
+/* ---- batched solve (no counterpart in the reference) -----------------------
+ * Solves m independent banded systems A_i x_i = b_i (row-major bands of
+ * n_i x (2 k_i + 1) values, host arrays) with the options' Krylov method and
+ * preconditioner type.  Systems of equal half-bandwidth are solved together
+ * as one block-diagonal system, every system's rows scaled by 1/||b_i||, to
+ * the absolute residual opts->relTol, which gives each system
+ * ||b_i - A_i x_i|| <= relTol ||b_i|| (opts->absTol is not used).  x_i are
+ * the initial guesses' storage (overwritten; the solve starts from zero).
+ * results[i]: the system's relative residual, the iterations of its stack
+ * and whether it met relTol; seconds: wall time of the whole batch. */
+typedef struct sap_batch_result {
+  double rel_residual;
+  float iterations;
+  int converged;
+} sap_batch_result;
+int sap_batch_banded_solve(int m, const int* n, const int* k, const double* const* bands, const double* const* b,
+                           double* const* x, int num_partitions, const sap_options* opts, int prec_dtype,
+                           sap_batch_result* results, double* seconds);
+
 /* ---- learned solver settings (no counterpart in the reference) -------------
  * A multilayer perceptron in -> h1 -> h2 -> out (ReLU hidden layers, softmax
  * output) mapping matrix features to a choice of solver settings, trained and

@@ -93,6 +93,8 @@ _sig = {
                              _vp, _vp, _vp]),
     "sap_mm_read_vector": (_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), _vp]),
     "sap_mm_last_error": (ctypes.c_char_p, []),
+    "sap_batch_banded_solve": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_void_p, _i, _vp,
+                                    ctypes.POINTER(ctypes.c_double)]),
     "sap_mlp_create": (_i, [_i, _i, _i, _i, ctypes.c_uint64, _pp]),
     "sap_mlp_destroy": (_i, [_vp]),
     "sap_mlp_num_params": (_i, [_vp]),
@@ -202,6 +204,36 @@ def read_matrix_market_vector(path: str) -> np.ndarray:
     if code:
         raise LibraryError(code, (_lib.sap_mm_last_error() or b"").decode())
     return out
+
+
+class _BatchResult(ctypes.Structure):
+    _fields_ = [("rel_residual", ctypes.c_double), ("iterations", ctypes.c_float), ("converged", ctypes.c_int)]
+
+
+def solve_batch(bands, ks, bs, num_partitions: int, opts: "Options", prec: str = "float"):
+    """Solve independent banded systems (row-major bands as numpy arrays,
+    half-bandwidths ks, right-hand sides bs) in one batched call; systems of
+    equal half-bandwidth are solved together as one block-diagonal system to
+    ||b_i - A_i x_i|| <= opts.relTol ||b_i|| each.  Returns (xs, results,
+    seconds) with results[i] = (relative residual, iterations, converged)."""
+    m = len(bands)
+    ns = [len(b) for b in bs]
+    bands = [np.ascontiguousarray(a, np.float64) for a in bands]
+    bs = [np.ascontiguousarray(b, np.float64) for b in bs]
+    xs = [np.zeros(n) for n in ns]
+    n_arr = np.asarray(ns, np.int32)
+    k_arr = np.asarray(ks, np.int32)
+    pa = (ctypes.c_void_p * m)(*[a.ctypes.data for a in bands])
+    pb = (ctypes.c_void_p * m)(*[b.ctypes.data for b in bs])
+    px = (ctypes.c_void_p * m)(*[x.ctypes.data for x in xs])
+    res = (_BatchResult * m)()
+    sec = ctypes.c_double()
+    copts = opts._c()
+    _check(_lib.sap_batch_banded_solve(m, n_arr.ctypes.data, k_arr.ctypes.data, ctypes.cast(pa, ctypes.c_void_p),
+                                       ctypes.cast(pb, ctypes.c_void_p), ctypes.cast(px, ctypes.c_void_p),
+                                       int(num_partitions), ctypes.cast(ctypes.pointer(copts), ctypes.c_void_p),
+                                       _PREC[prec], ctypes.cast(res, ctypes.c_void_p), ctypes.byref(sec)))
+    return xs, [(r.rel_residual, r.iterations, bool(r.converged)) for r in res], sec.value
 
 
 def library_call_count() -> int:

@@ -1477,6 +1477,35 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
 
 }  // namespace sapb
 
+// One system of a batch stack: row-major band rows scaled by `scale`,
+// entries outside the system's columns [0, n) zeroed.
+static __global__ void k_stack_rows(double* __restrict__ A, int n, int K, double scale) {
+  const long long W = 2LL * K + 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * W;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / W;
+    const long long c = r + (e - r * W) - K;
+    A[e] = (c >= 0 && c < n) ? A[e] * scale : 0.0;
+  }
+}
+
+// Per-segment sums of squares: out[s] = sum over rows [seg[s], seg[s+1]) of
+// r^2, one CTA per segment, fixed-order reduction.
+static __global__ void k_seg_sumsq(const double* __restrict__ r, const long long* __restrict__ seg,
+                                   double* __restrict__ out) {
+  __shared__ double red[256];
+  const long long a = seg[blockIdx.x], b = seg[blockIdx.x + 1];
+  double s = 0;
+  for (long long i = a + threadIdx.x; i < b; i += blockDim.x) s += r[i] * r[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
 // ===========================================================================
 // C ABI
 using namespace sapb;
@@ -1847,6 +1876,117 @@ int sap_precond_apply(sap_solver* h, const double* v, double* z) {
     if (!S.setup_done) throw Error(SAP_ILLEGAL_SOLVE, "preconditioner used before setup().");
     S.pc().apply(v, z);
     SAPB_CUDA(cudaStreamSynchronize(S.st));
+  });
+}
+
+// Batched solve of independent banded systems (no reference counterpart).
+// Systems with the same half-bandwidth are stacked into one block-diagonal
+// banded system (entries of a system never reach another: its band rows
+// have zeros outside its own columns), each system's rows scaled by
+// 1/||b_i|| so that the stacked right-hand side has unit blocks; the stack
+// is set up and solved once, to the absolute residual relTol, which bounds
+// every block: ||r_i|| <= relTol ||b_i||.  The partition count of a stack is
+// the sum of the systems' own counts.
+int sap_batch_banded_solve(int m, const int* n, const int* k, const double* const* bands, const double* const* b,
+                           double* const* x, int num_partitions, const sap_options* opts, int prec_dtype,
+                           sap_batch_result* results, double* seconds) {
+  SAP_TRY({
+    SAP_REQUIRE(m > 0 && n && k && bands && b && x && opts && results, "null or empty batch");
+    for (int i = 0; i < m; i++) SAP_REQUIRE(n[i] > 0 && k[i] >= 0 && k[i] < n[i] && bands[i] && b[i] && x[i], "bad system");
+    auto t0 = Clock::now();
+    std::vector<int> order(m);
+    for (int i = 0; i < m; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return k[a] < k[c]; });
+    size_t g0 = 0;
+    while (g0 < order.size()) {
+      size_t g1 = g0;
+      const int K = k[order[g0]];
+      while (g1 < order.size() && k[order[g1]] == K) g1++;
+      // stack the group
+      long long ntot = 0;
+      int Ptot = 0;
+      std::vector<long long> seg{0};
+      std::vector<double> scale;
+      for (size_t q = g0; q < g1; q++) {
+        const int i = order[q];
+        ntot += n[i];
+        seg.push_back(ntot);
+        double bn = 0;
+        for (int r = 0; r < n[i]; r++) bn += b[i][r] * b[i][r];
+        bn = std::sqrt(bn);
+        scale.push_back(bn > 0 ? 1.0 / bn : 1.0);
+        Ptot += std::max(1, std::min(num_partitions, n[i] / std::max(K + 1, 2 * K)));
+      }
+      SAP_REQUIRE(ntot < 2147483647LL, "stacked system too large");
+      const size_t W = 2 * (size_t)K + 1;
+      std::vector<double> bb((size_t)ntot), xx((size_t)ntot, 0.0);
+      // the stack on the device: every system copied into its rows, then
+      // scaled, with the entries outside its own columns dropped so that no
+      // system reaches into its neighbours
+      auto Ah = std::make_unique<sap_banded>();
+      Ah->b.n = (int)ntot;
+      Ah->b.K = K;
+      Ah->b.A.alloc((size_t)ntot * W);
+      for (size_t q = g0; q < g1; q++) {
+        const int i = order[q];
+        const long long off = seg[q - g0];
+        SAPB_CUDA(cudaMemcpy(Ah->b.A.get() + (size_t)off * W, bands[i], sizeof(double) * (size_t)n[i] * W,
+                             cudaMemcpyHostToDevice));
+        k_stack_rows<<<grid_for((long long)n[i] * (long long)W, 256), 256>>>(Ah->b.A.get() + (size_t)off * W, n[i], K,
+                                                                             scale[q - g0]);
+        SAPB_LAUNCHED();
+        const double sc = scale[q - g0];
+        for (int r = 0; r < n[i]; r++) bb[off + r] = b[i][r] * sc;
+      }
+      SAPB_CUDA(cudaDeviceSynchronize());
+      sap_options o = *opts;
+      o.absTol = opts->relTol;
+      o.relTol = 0;
+      o.performReorder = 0;
+      o.variableBandwidth = 0;
+      o.applyScaling = 0;
+      sap_banded* A = Ah.release();
+      sap_spmv* op = nullptr;
+      sap_solver* sv = nullptr;
+      int rc = sap_spmv_banded_create(A, &op);
+      if (rc == SAP_OK) rc = sap_solver_create(Ptot, &o, prec_dtype, &sv);
+      if (rc == SAP_OK) rc = sap_solver_setup_banded(sv, A);
+      int conv = 0;
+      if (rc == SAP_OK) rc = sap_solver_solve(sv, op, bb.data(), xx.data(), SAP_HOST, &conv);
+      if (rc == SAP_OK) {
+        // per-system residual norms of the scaled stack = relative residuals
+        Solver& S = *sv->s;
+        DBuf<double> xd, rd, sq;
+        DBuf<long long> segd;
+        xd.upload(xx, S.st);
+        rd.alloc((size_t)ntot);
+        sq.alloc(g1 - g0);
+        segd.upload(seg, S.st);
+        op->op.apply(xd.get(), rd.get(), S.st);
+        DBuf<double> bd;
+        bd.upload(bb, S.st);
+        k_axpby<<<grid_for(ntot, 256), 256, 0, S.st>>>((int)ntot, 1.0, bd.get(), -1.0, rd.get(), rd.get());
+        SAPB_LAUNCHED();
+        k_seg_sumsq<<<(int)(g1 - g0), 256, 0, S.st>>>(rd.get(), segd.get(), sq.get());
+        SAPB_LAUNCHED();
+        std::vector<double> sqh;
+        sq.download(sqh, S.st);
+        SAPB_CUDA(cudaStreamSynchronize(S.st));
+        for (size_t q = g0; q < g1; q++) {
+          const int i = order[q];
+          results[i].rel_residual = std::sqrt(sqh[q - g0]);
+          results[i].iterations = S.stats.numIterations;
+          results[i].converged = results[i].rel_residual <= opts->relTol ? 1 : 0;
+          std::memcpy(x[i], xx.data() + seg[q - g0], sizeof(double) * n[i]);
+        }
+      }
+      if (sv) sap_solver_destroy(sv);
+      if (op) sap_spmv_destroy(op);
+      if (A) sap_banded_destroy(A);
+      if (rc != SAP_OK) return rc;
+      g0 = g1;
+    }
+    if (seconds) *seconds = ms_since(t0) / 1e3;
   });
 }
 
