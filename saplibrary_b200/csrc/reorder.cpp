@@ -95,7 +95,9 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
   const std::vector<int>& Rp = in_rp;
   const std::vector<int>& Ci = in_ci;
   std::vector<double> u(n, 0.0), v(n, kInf);
-  std::vector<int> match(n, 0), rev_match(nnz, 0);
+  std::vector<int> match(n, 0);
+  std::vector<int>& rev_match = ws_i0;
+  rev_match.assign(nnz, 0);
   std::vector<char> row_done(n, 0), col_done(n, 0);
   // initial duals: u = per-row minimum weight (reduce_by_key over CSR rows)
   for (int i = 0; i < n; i++) {
@@ -213,7 +215,8 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
   db_row_perm.resize(n);
   for (int c = 0; c < n; c++) db_row_perm[match[c]] = c;
   // permuted (and scaled) matrix, rows in the new order, entries stable
-  std::vector<T> val(nnz);
+  std::vector<T>& val = ws_t0;
+  val.resize(nnz);
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++)
     for (int e = Rp[i]; e < Rp[i + 1]; e++)
@@ -301,7 +304,9 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
 template <typename T>
 int Pipeline<T>::rcm() {
   const int nz = (int)m_ci.size();
-  std::vector<int> row(nz), degree(n);
+  std::vector<int>& row = ws_i0;
+  row.resize(nz);
+  std::vector<int> degree(n);
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) row[e] = i;
@@ -310,7 +315,8 @@ int Pipeline<T>::rcm() {
   int best_bw = 0;
 #pragma omp parallel for reduction(max : best_bw) schedule(static)
   for (int e = 0; e < nz; e++) best_bw = std::max(best_bw, std::abs(row[e] - m_ci[e]));
-  std::vector<int> off, adj;
+  std::vector<int>& off = ws_off;
+  std::vector<int>& adj = ws_adj;
   symmetric_adjacency(row, m_ci, 0, nz, 0, n, n, off, adj);
   rcm_order.resize(n);
   for (int i = 0; i < n; i++) rcm_order[i] = i;
@@ -350,11 +356,10 @@ int Pipeline<T>::rcm() {
     if (best_bw <= 256) break;       // BANDWIDTH_THRESHOLD
   }
   for (int k = 0; k < n; k++) rcm_pos[rcm_order[k]] = k;
-  {
-    const std::vector<int> rp0 = std::move(m_rp), ci0 = std::move(m_ci);
-    const std::vector<T> v0 = std::move(m_val);
-    permute_rows(n, rp0, ci0, v0, rcm_pos, &rcm_pos, m_rp, m_ci, m_val);
-  }
+  tmp_rp.swap(m_rp);
+  tmp_ci.swap(m_ci);
+  tmp_val.swap(m_val);
+  permute_rows(n, tmp_rp, tmp_ci, tmp_val, rcm_pos, &rcm_pos, m_rp, m_ci, m_val);
   return best_bw;
 }
 
@@ -368,13 +373,16 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   // The reference's bucketed list: entries ordered by distance |i - j|, rows
   // ascending and CSR order inside a distance group.  Group d occupies
   // [gstart[d], gstart[d+1]); only the values are needed (for the squares).
-  std::vector<int> gstart(n + 1, 0);
+  std::vector<int>& gstart = ws_i1;
+  gstart.assign(n + 1, 0);
   for (int i = 0; i < n; i++)
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) gstart[std::abs(i - m_ci[e]) + 1]++;
   for (int d = 0; d < n; d++) gstart[d + 1] += gstart[d];
-  std::vector<T> bv(nz);
+  std::vector<T>& bv = ws_t0;
+  bv.resize(nz);
   {
-    std::vector<int> pos(gstart.begin(), gstart.end() - 1);
+    std::vector<int>& pos = ws_i2;
+    pos.assign(gstart.begin(), gstart.end() - 1);
     for (int i = 0; i < n; i++)
       for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[pos[std::abs(i - m_ci[e])]++] = m_val[e];
   }
@@ -416,8 +424,12 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   // kept: every entry within distance g, sorted by row, then column (what
   // the reference's two stable counting sorts of the kept list give)
   const int dkeep = g;
-  const std::vector<int> rp0 = std::move(m_rp), ci0 = std::move(m_ci);
-  const std::vector<T> v0 = std::move(m_val);
+  tmp_rp.swap(m_rp);
+  tmp_ci.swap(m_ci);
+  tmp_val.swap(m_val);
+  const std::vector<int>& rp0 = tmp_rp;
+  const std::vector<int>& ci0 = tmp_ci;
+  const std::vector<T>& v0 = tmp_val;
   m_rp.assign(n + 1, 0);
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
@@ -499,7 +511,8 @@ template <typename T>
 void Pipeline<T>::second_level(int K, int P) {
   const int q = n / P, rem = n % P;
   const int dz = (int)d_ci.size();
-  std::vector<int> row(dz);
+  std::vector<int>& row = ws_i0;
+  row.resize(dz);
   for (int i = 0; i < n; i++)
     for (int e = d_rp[i]; e < d_rp[i + 1]; e++) row[e] = i;
   second_order.assign(n, 0);
@@ -568,11 +581,10 @@ void Pipeline<T>::second_level(int K, int P) {
     second_pos.assign(n, 0);
     for (int p = 0; p < P; p++) part(p, true);
   }
-  {
-    const std::vector<int> rp0 = std::move(d_rp), ci0 = std::move(d_ci);
-    const std::vector<T> v0 = std::move(d_val);
-    permute_rows(n, rp0, ci0, v0, second_pos, &second_pos, d_rp, d_ci, d_val);
-  }
+  tmp_rp.swap(d_rp);
+  tmp_ci.swap(d_ci);
+  tmp_val.swap(d_val);
+  permute_rows(n, tmp_rp, tmp_ci, tmp_val, second_pos, &second_pos, d_rp, d_ci, d_val);
   first_rows.assign(std::max(P - 1, 0), 0);
   int last = 0;
   for (int i = 0; i < P - 1; i++) {

@@ -57,6 +57,11 @@ class Pipeline {
   std::vector<T> m_val, d_val;
   std::vector<char> couples_right;
 
+  // scratch kept across runs of the same object (a repeated setup reuses
+  // its memory instead of allocating and page-faulting it again)
+  std::vector<int> ws_i0, ws_i1, ws_i2, ws_off, ws_adj, tmp_rp, tmp_ci;
+  std::vector<T> ws_t0, tmp_val;
+
   // wall time of the stages of run(), in order (ms)
   std::vector<std::pair<const char*, double>> stage_ms;
   double stage(const char* name) const {

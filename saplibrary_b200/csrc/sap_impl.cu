@@ -396,7 +396,8 @@ class PrecondT : public PrecBase {
     wide_active = false;
     auto t0 = Clock::now();
     n = A.n;
-    rp::Pipeline<T> pl;
+    if (!pipe) pipe = std::make_unique<rp::Pipeline<T>>();
+    rp::Pipeline<T>& pl = *pipe;
     pl.n = n;
     pl.P_req = P_req;
     pl.do_db = o.performDB != 0;
@@ -428,11 +429,15 @@ class PrecondT : public PrecBase {
       }
     }
     pl.nnz = (int)pl.in_ci.size();
-    std::vector<double> w, rmax;
+    std::vector<double>& w = db_w;
+    std::vector<double>& rmax = db_rmax;
+    w.clear();
+    rmax.clear();
     if (pl.do_db) {
       DBuf<int> drp;
       DBuf<double> da, dw, dmax;
-      std::vector<double> av(pl.in_val.size());
+      std::vector<double>& av = db_av;
+      av.resize(pl.in_val.size());
 #pragma omp parallel for schedule(static, 65536)
       for (long long e = 0; e < (long long)av.size(); e++) av[e] = (double)pl.in_val[e];
       drp.upload(pl.in_rp, st);
@@ -530,10 +535,15 @@ class PrecondT : public PrecBase {
   }
 
   long long boff_total = 0;
+  // host state kept across setups (its memory is reused, not re-faulted)
+  std::unique_ptr<rp::Pipeline<T>> pipe;
+  std::vector<double> db_w, db_rmax, db_av;
+  std::vector<int> coo_rows;
 
   // device COO (band rows, columns, values) of a CSR in band order
   void upload_coo(const std::vector<int>& rp_, const std::vector<int>& ci_, const std::vector<T>& v_) {
-    std::vector<int> rows(ci_.size());
+    std::vector<int>& rows = coo_rows;
+    rows.resize(ci_.size());
     for (int i = 0; i < n; i++)
       for (int e = rp_[i]; e < rp_[i + 1]; e++) rows[e] = i;
     co_row.upload(rows, st);
