@@ -89,6 +89,15 @@ __global__ void k_sub_copy(const T* __restrict__ src, int lds, long long ss, T* 
       dst[b * sd + (long long)c * ldd + r] = scale * src[b * ss + (long long)c * lds + r];
 }
 
+// Batched fill of an m x n sub-matrix with a value.
+template <typename T>
+__global__ void k_sub_fill(T* __restrict__ dst, int ldd, long long sd, int m, int n, T value) {
+  const int b = blockIdx.z;
+  for (int c = blockIdx.y; c < n; c += gridDim.y)
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x)
+      dst[b * sd + (long long)c * ldd + r] = value;
+}
+
 // Leaf of the recursive LU: an n x n (n <= 32) diagonal block factored in
 // place without pivoting (the reference's boosting rule when `boost`), and
 // its L^-1 (unit lower) and U^-1 (upper) written to Li / Ui.  One CTA of 32

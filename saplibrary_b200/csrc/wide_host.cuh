@@ -74,6 +74,82 @@ class BlockLU {
     SAPB_LAUNCHED();
   }
 
+  void fill(Mat<T> dst, int m, int n, T value) {
+    if (m <= 0 || n <= 0) return;
+    dim3 g((m + 255) / 256, std::min(n, 1024), batch);
+    k_sub_fill<T><<<g, 256, 0, st>>>(dst.p, dst.ld, dst.s, m, n, value);
+    SAPB_LAUNCHED();
+  }
+
+  // Products with triangular operands, recursing on halves and skipping the
+  // structurally zero quarter (the skipped terms are exact zeros, so the
+  // results equal the full products up to summation order).  Below `cut`
+  // a full GEMM.  C never aliases A or B.  L: lower, U: upper, F: full.
+  int cut = 384;  // WideBand sets it: recursion pays off for compute-bound FP64 / FP32, not for TF32
+  static int half(int n) { return std::max(32, ((n / 2 + 31) / 32) * 32); }
+  // C (n x m) = alpha L B + beta C
+  void prod_LF(int n, int m, T alpha, Mat<T> L, Mat<T> B, T beta, Mat<T> C) {
+    if (n <= cut) return gemm(n, m, n, alpha, L, B, beta, C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_LF(n1, m, alpha, L, B, beta, C);
+    gemm(n2, m, n1, alpha, L.at(n1, 0), B, beta, C.at(n1, 0));
+    prod_LF(n2, m, alpha, L.at(n1, n1), B.at(n1, 0), T(1), C.at(n1, 0));
+  }
+  // C (n x m) = alpha U B + beta C
+  void prod_UF(int n, int m, T alpha, Mat<T> U, Mat<T> B, T beta, Mat<T> C) {
+    if (n <= cut) return gemm(n, m, n, alpha, U, B, beta, C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_UF(n1, m, alpha, U, B, beta, C);
+    gemm(n1, m, n2, alpha, U.at(0, n1), B.at(n1, 0), T(1), C);
+    prod_UF(n2, m, alpha, U.at(n1, n1), B.at(n1, 0), beta, C.at(n1, 0));
+  }
+  // C (m x n) = alpha A U + beta C
+  void prod_FU(int m, int n, T alpha, Mat<T> A, Mat<T> U, T beta, Mat<T> C) {
+    if (n <= cut) return gemm(m, n, n, alpha, A, U, beta, C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_FU(m, n1, alpha, A, U, beta, C);
+    gemm(m, n2, n1, alpha, A, U.at(0, n1), beta, C.at(0, n1));
+    prod_FU(m, n2, alpha, A.at(0, n1), U.at(n1, n1), T(1), C.at(0, n1));
+  }
+  // C (m x n) = alpha A L + beta C
+  void prod_FL(int m, int n, T alpha, Mat<T> A, Mat<T> L, T beta, Mat<T> C) {
+    if (n <= cut) return gemm(m, n, n, alpha, A, L, beta, C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_FL(m, n1, alpha, A, L, beta, C);
+    gemm(m, n1, n2, alpha, A.at(0, n1), L.at(n1, 0), T(1), C);
+    prod_FL(m, n2, alpha, A.at(0, n1), L.at(n1, n1), beta, C.at(0, n1));
+  }
+  // C (lower, n x n) = alpha A B, A and B lower; C's upper part set to zero
+  void prod_LL(int n, T alpha, Mat<T> A, Mat<T> B, Mat<T> C) {
+    if (n <= cut) return gemm(n, n, n, alpha, A, B, T(0), C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_LL(n1, alpha, A, B, C);
+    fill(C.at(0, n1), n1, n2, T(0));
+    prod_FL(n2, n1, alpha, A.at(n1, 0), B, T(0), C.at(n1, 0));
+    prod_LF(n2, n1, alpha, A.at(n1, n1), B.at(n1, 0), T(1), C.at(n1, 0));
+    prod_LL(n2, alpha, A.at(n1, n1), B.at(n1, n1), C.at(n1, n1));
+  }
+  // C (upper, n x n) = alpha A B, A and B upper; C's lower part set to zero
+  void prod_UU(int n, T alpha, Mat<T> A, Mat<T> B, Mat<T> C) {
+    if (n <= cut) return gemm(n, n, n, alpha, A, B, T(0), C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_UU(n1, alpha, A, B, C);
+    prod_UF(n1, n2, alpha, A, B.at(0, n1), T(0), C.at(0, n1));
+    prod_FU(n1, n2, alpha, A.at(0, n1), B.at(n1, n1), T(1), C.at(0, n1));
+    fill(C.at(n1, 0), n2, n1, T(0));
+    prod_UU(n2, alpha, A.at(n1, n1), B.at(n1, n1), C.at(n1, n1));
+  }
+  // C (n x n) += alpha A B, A upper, B lower
+  void prod_UL_acc(int n, T alpha, Mat<T> A, Mat<T> B, Mat<T> C) {
+    if (n <= cut) return gemm(n, n, n, alpha, A, B, T(1), C);
+    const int n1 = half(n), n2 = n - n1;
+    prod_UL_acc(n1, alpha, A, B, C);
+    gemm(n1, n1, n2, alpha, A.at(0, n1), B.at(n1, 0), T(1), C);
+    prod_FL(n1, n2, alpha, A.at(0, n1), B.at(n1, n1), T(1), C.at(0, n1));
+    prod_UF(n2, n1, alpha, A.at(n1, n1), B.at(n1, 0), T(1), C.at(n1, 0));
+    prod_UL_acc(n2, alpha, A.at(n1, n1), B.at(n1, n1), C.at(n1, n1));
+  }
+
   // M (n x n at M) = L U in place; Li = L^-1, Ui = U^-1 (both pre-zeroed).
   void rec(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n) {
     if (n <= kLeaf) {
@@ -87,17 +163,17 @@ class BlockLU {
     const int n2 = n - n1;
     rec(M, Li, Ui, n1);
     // U12 = L11^-1 A12 ; L21 = A21 U11^-1 ; A22 -= L21 U12
-    gemm(n1, n2, n1, T(1), Li, M.at(0, n1), T(0), W);
+    prod_LF(n1, n2, T(1), Li, M.at(0, n1), T(0), W);
     copy(W, M.at(0, n1), n1, n2);
-    gemm(n2, n1, n1, T(1), M.at(n1, 0), Ui, T(0), W);
+    prod_FU(n2, n1, T(1), M.at(n1, 0), Ui, T(0), W);
     copy(W, M.at(n1, 0), n2, n1);
     gemm(n2, n2, n1, T(-1), M.at(n1, 0), M.at(0, n1), T(1), M.at(n1, n1));
     rec(M.at(n1, n1), Li.at(n1, n1), Ui.at(n1, n1), n2);
     // (L^-1)21 = -L22^-1 L21 L11^-1 ; (U^-1)12 = -U11^-1 U12 U22^-1
-    gemm(n2, n1, n1, T(1), M.at(n1, 0), Li, T(0), W);
-    gemm(n2, n1, n2, T(-1), Li.at(n1, n1), W, T(0), Li.at(n1, 0));
-    gemm(n1, n2, n2, T(1), M.at(0, n1), Ui.at(n1, n1), T(0), W);
-    gemm(n1, n2, n1, T(-1), Ui, W, T(0), Ui.at(0, n1));
+    prod_FL(n2, n1, T(1), M.at(n1, 0), Li, T(0), W);
+    prod_LF(n2, n1, T(-1), Li.at(n1, n1), W, T(0), Li.at(n1, 0));
+    prod_FU(n1, n2, T(1), M.at(0, n1), Ui.at(n1, n1), T(0), W);
+    prod_UF(n1, n2, T(-1), Ui, W, T(0), Ui.at(0, n1));
   }
 };
 
@@ -248,20 +324,24 @@ class WideBand {
     lu.batch = P;
     lu.boost = boost;
     lu.flag = flag.get();
+    lu.cut = tf32 ? (1 << 30) : 384;
     const Mat<T> D{Dw.get(), bs, BB}, L{Lw.get(), bs, BB}, U{Uw.get(), bs, BB}, Wm{Ww.get(), bs, BB};
     lu.W = Wm;
     for (int i = 0; i < nb; i++) {
       lu.copy(blk(Linv, nb, i), D, bs, bs);
-      if (i > 0) lu.gemm(bs, bs, bs, T(-1), blk(Loff, nb - 1, i - 1), blk(Uoff, nb - 1, i - 1), T(1), D);
+      // D_i -= L_{i,i-1} U_{i-1,i}: upper times lower
+      if (i > 0) lu.prod_UL_acc(bs, T(-1), blk(Loff, nb - 1, i - 1), blk(Uoff, nb - 1, i - 1), D);
       Lw.zero(st);
       Uw.zero(st);
       lu.rec(D, L, U, bs);
       lu.copy(L, blk(Linv, nb, i), bs, bs);
       lu.copy(U, blk(Uinv, nb, i), bs, bs);
       if (i < nb - 1) {
-        lu.gemm(bs, bs, bs, T(1), L, blk(Uoff, nb - 1, i), T(0), Wm);
+        // U_{i,i+1} = L_ii^-1 E_i (lower times lower: E_i has no entries above
+        // its diagonal), L_{i+1,i} = F_i U_ii^-1 (upper times upper)
+        lu.prod_LL(bs, T(1), L, blk(Uoff, nb - 1, i), Wm);
         lu.copy(Wm, blk(Uoff, nb - 1, i), bs, bs);
-        lu.gemm(bs, bs, bs, T(1), blk(Loff, nb - 1, i), U, T(0), Wm);
+        lu.prod_UU(bs, T(1), blk(Loff, nb - 1, i), U, Wm);
         lu.copy(Wm, blk(Loff, nb - 1, i), bs, bs);
       }
     }
@@ -404,6 +484,7 @@ class WideBand {
       ops.h = h;
       ops.st = st;
       ops.batch = nI;
+      ops.cut = 1 << 30;  // measured: the slab products are fastest as plain GEMMs
       const Mat<T> Wm{Wt.get(), bs, (long long)bs * cs};
       const int ib0 = std::max(0, minpos) / bs;
       auto Xb = [&](int i) { return Mat<T>{X.get() + (long long)i * bs, (int)plen, sX}; };
@@ -418,14 +499,16 @@ class WideBand {
         k_spike_rhs<T><<<dim3(w, nI), kt, 0, st>>>(offd, which, K, cols_d.get(), ncol, j0, pos_d.get(), X.get(), sX,
                                                     plen);
         SAPB_LAUNCHED();
+        // forward with L_{i,i-1} (upper) and L_ii^-1 (lower), backward with
+        // U_{i,i+1} (lower) and U_ii^-1 (upper)
         for (int i = ib0; i < nb; i++) {
-          if (i > ib0) ops.gemm(bs, w, bs, T(-1), Fk(Loff, nb - 1, i - 1), Xb(i - 1), T(1), Xb(i));
-          ops.gemm(bs, w, bs, T(1), Fk(Linv, nb, i), Xb(i), T(0), Wm);
+          if (i > ib0) ops.prod_UF(bs, w, T(-1), Fk(Loff, nb - 1, i - 1), Xb(i - 1), T(1), Xb(i));
+          ops.prod_LF(bs, w, T(1), Fk(Linv, nb, i), Xb(i), T(0), Wm);
           ops.copy(Wm, Xb(i), bs, w);
         }
         for (int i = nb - 1; i >= ib0; i--) {
-          if (i < nb - 1) ops.gemm(bs, w, bs, T(-1), Fk(Uoff, nb - 1, i), Xb(i + 1), T(1), Xb(i));
-          ops.gemm(bs, w, bs, T(1), Fk(Uinv, nb, i), Xb(i), T(0), Wm);
+          if (i < nb - 1) ops.prod_LF(bs, w, T(-1), Fk(Uoff, nb - 1, i), Xb(i + 1), T(1), Xb(i));
+          ops.prod_UF(bs, w, T(1), Fk(Uinv, nb, i), Xb(i), T(0), Wm);
           ops.copy(Wm, Xb(i), bs, w);
         }
         k_spike_tips<T><<<dim3(w, nI), kt, 0, st>>>(X.get(), sX, plen, cols_d.get(), ncol, j0, pos_d.get(), K, ldK,
