@@ -219,8 +219,20 @@ class WideBand {
   WideBand(const WideBand&) = delete;
   WideBand& operator=(const WideBand&) = delete;
   ~WideBand() {
+    if (fgraph) cudaGraphExecDestroy(fgraph);
     if (h) cublasDestroy(h);
   }
+
+  // The factorization's launch sequence (about a thousand small GEMMs,
+  // copies and leaf LUs per block row) as a CUDA graph: the first setup of a
+  // layout runs it directly, the second captures it, later ones replay it
+  // (every buffer it touches is kept across setups of the layout).
+  cudaGraphExec_t fgraph = nullptr;
+  long long fgraph_key = -1;
+  int fgraph_runs = 0;
+  bool fgraph_failed = false;
+  int64_t fgraph_launches = 0, fgraph_lib_calls = 0;
+  DBuf<unsigned char> cublas_ws;  // fixed cuBLAS workspace (no allocation inside a capture)
 
   // Block size bs >= the largest half-bandwidth, a multiple of the leaf size.
   static int block_size(int kmax) { return std::max(kLeaf, ((kmax + kLeaf - 1) / kLeaf) * kLeaf); }
@@ -251,6 +263,8 @@ class WideBand {
     psize_h = psize;
     if (!h) cublas_check(cublasCreate(&h), "cublasCreate");
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
+    if (cublas_ws.size() == 0) cublas_ws.alloc((size_t)64 << 20);
+    cublas_check(cublasSetWorkspace(h, cublas_ws.get(), cublas_ws.size()), "cublasSetWorkspace");
     spike = false;
     math_mode(tf32);
     int maxsz = 0;
@@ -317,6 +331,52 @@ class WideBand {
     Uw.alloc((size_t)P * BB);
     Ww.alloc((size_t)P * BB);
     flag.alloc(1);
+    const long long key = (((long long)P * 65537 + bs) * 65537 + nb) * 4 + (boost ? 2 : 0) + (tf32 ? 1 : 0);
+    if (key != fgraph_key) {
+      if (fgraph) cudaGraphExecDestroy(fgraph);
+      fgraph = nullptr;
+      fgraph_key = key;
+      fgraph_runs = 0;
+    }
+    if (fgraph) {
+      SAPB_CUDA(cudaGraphLaunch(fgraph, st));
+      count_launch((int)fgraph_launches);
+      g_lib_calls.fetch_add(fgraph_lib_calls, std::memory_order_relaxed);
+    } else if (fgraph_runs >= 1 && !fgraph_failed) {
+      const int64_t l0 = g_launches.load(), c0 = g_lib_calls.load();
+      cudaGraph_t g = nullptr;
+      bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        try {
+          enqueue_factor(boost);
+        } catch (...) {
+          ok = false;
+        }
+        ok = (cudaStreamEndCapture(st, &g) == cudaSuccess) && ok && g;
+      }
+      if (ok) ok = cudaGraphInstantiate(&fgraph, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      (void)cudaGetLastError();
+      fgraph_launches = g_launches.load() - l0;
+      fgraph_lib_calls = g_lib_calls.load() - c0;
+      if (ok) {
+        SAPB_CUDA(cudaGraphLaunch(fgraph, st));
+      } else {
+        fgraph = nullptr;
+        fgraph_failed = true;  // run directly from now on
+        enqueue_factor(boost);
+      }
+    } else {
+      enqueue_factor(boost);
+      fgraph_runs++;
+    }
+    int hf = 0;
+    SAPB_CUDA(cudaMemcpyAsync(&hf, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
+  }
+
+  void enqueue_factor(bool boost) {
     flag.zero(st);
     BlockLU<T> lu;
     lu.h = h;
@@ -345,10 +405,6 @@ class WideBand {
         lu.copy(Wm, blk(Loff, nb - 1, i), bs, bs);
       }
     }
-    int hf = 0;
-    SAPB_CUDA(cudaMemcpyAsync(&hf, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
-    SAPB_CUDA(cudaStreamSynchronize(st));
-    if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
   }
 
   // tri: 0 full, 1 lower, 2 upper (see k_tgemv).  Grids with fewer than
