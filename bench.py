@@ -48,6 +48,11 @@ HEADLINE = "tf32_fgmres"
 DEFAULT_FORMS = "tf32_fgmres,fp64"
 # rows of the CPU band-LU timing sample (about 5 s at K ~ 3000)
 LU_SAMPLE_ROWS = 400
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) over the
+# algorithmic bytes of one block-sweep k_tgemv launch, measured with ncu on
+# this workload at grid side 310 (block size 3168, the FP32 block size at
+# the full size); a launch's traffic scales with its triangle's bytes
+TGEMV_TRAFFIC_RATIO = {4: 1.051}
 
 
 def measured_peaks():
@@ -354,10 +359,12 @@ def main():
     roofline = None
     if "block_sweep" in head:
         bsw = head["block_sweep"]
+        ratio = TGEMV_TRAFFIC_RATIO.get(head["value_bytes"])
         roofline = {"kernel": "k_tgemv (one block_sweep = 4*nb-2 launches)", "bound": "hbm", "achieved": bsw["gbs"],
                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": bsw["gbs"] / peaks["hbm_gbs"],
-                    "traffic": None, "peak_source": peak_kind, "avg_sweep_ms": bsw["avg_ms"],
-                    "bytes_per_sweep": bsw["bytes"]}
+                    "traffic": int(ratio * bsw["bytes"]) if ratio else None,
+                    "traffic_source": "ncu ratio of one block-sweep launch at grid side 310, scaled" if ratio else None,
+                    "peak_source": peak_kind, "avg_sweep_ms": bsw["avg_ms"], "bytes_per_sweep": bsw["bytes"]}
 
     line = {
         "metric": "time_to_solution", "value": head["tts_s"], "unit": "s", "n_gpus": ws, "steps": args.steps,
