@@ -127,6 +127,24 @@ def set_grid(m: int) -> None:
         WORKLOAD["name"] = WORKLOAD["name"].replace("m1000", f"m{m}")
 
 
+def max_over_ranks(value: float, ws: int) -> float:
+    """The maximum of a per-rank value over all ranks (timings are reported
+    as max over ranks); the reduction runs on the process group's device."""
+    if ws <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(rank: int) -> int:
+    """Every rank solves its own system (replicas): seed of rank r's problem."""
+    return 1 + rank
+
+
 def make_problem(seed: int):
     from saplibrary_b200.problems import convection_diffusion_csr
     w = WORKLOAD
@@ -237,7 +255,7 @@ def main():
 
     w = WORKLOAD
     warm = max(3, args.warmup)
-    rp, ci, v, b_np = make_problem(seed=1 + rank)
+    rp, ci, v, b_np = make_problem(seed=rank_seed(rank))
     n = len(rp) - 1
     A = sap.CsrMatrix(rp, ci, v)
     spmv = sap.SpmvCusp(A)
@@ -291,11 +309,7 @@ def main():
         sap.profile_select(None)
         launches = sap.kernel_launch_count() - launches0
         lib_calls = sap.library_call_count() - lib0
-        ms_step = ev0.elapsed_time(ev1) / steps
-        if ws > 1:
-            t = torch.tensor([ms_step], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_step = float(t.item())
+        ms_step = max_over_ranks(ev0.elapsed_time(ev1) / steps, ws)
         st = solver.getStats()
         bs, nb, vb = solver.blockLayout()
         _, K, P = solver.info()
@@ -346,11 +360,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(args.steps):
             step_e2e()
-        e2e_s = (time.perf_counter() - t0) / args.steps
-        if ws > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, ws)
         h2d = rp.nbytes + ci.nbytes + v.nbytes + 2 * n * 8
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": n * 8}
         del solver_h

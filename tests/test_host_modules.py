@@ -1,0 +1,30 @@
+"""Host-side pieces of the learned settings and the batched ensemble (no GPU)."""
+import numpy as np
+
+import saplibrary_b200 as sap
+from saplibrary_b200 import ensemble, learned
+
+
+def test_band_features_are_finite_and_scale_aware():
+    f1 = learned.band_features(sap.generate_band_host(20000, 20, 1.0, 1, seed=1), 20000, 20)
+    f2 = learned.band_features(sap.generate_band_host(20000, 80, 0.6, 2, seed=1), 20000, 80)
+    assert f1.shape == (learned.NUM_FEATURES,) and np.all(np.isfinite(f1)) and np.all(np.isfinite(f2))
+    assert f2[1] > f1[1]          # log10 K
+    assert f2[4] < f1[4]          # mean dominance follows d
+    assert f1[15] <= 1.0 and f2[15] > 0.9  # rows below dominance 1
+
+
+def test_gain_and_labels_from_a_time_table():
+    T = np.array([[3.0, 1.0, 2.0, 9, 9, 9, 9], [1.0, 2.0, 3.0, 9, 9, 9, 9], [np.inf, 4.0, 5.0, 9, 9, 9, 9]])
+    assert list(learned.labels_from_times(T)) == [1, 0, 1]
+    g = learned.gain(T, np.array([1, 0, 1]))
+    assert g["total_chosen_s"] == 6.0 and g["total_default_s"] == 10.0 and g["picked_best"] == 1.0
+
+
+def test_ensemble_generator_shapes_and_seeds():
+    bands, ks, bs = ensemble.make_ensemble(12, seed=4, n_min=2000, n_max=8000, ks=(8, 16))
+    assert len(bands) == len(ks) == len(bs) == 12
+    for band, K, b in zip(bands, ks, bs):
+        assert K in (8, 16) and 2000 <= len(b) <= 8000 and band.size == len(b) * (2 * K + 1)
+    again = ensemble.make_ensemble(12, seed=4, n_min=2000, n_max=8000, ks=(8, 16))
+    assert all(np.array_equal(a, c) for a, c in zip(bands, again[0]))
