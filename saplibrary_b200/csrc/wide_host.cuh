@@ -210,7 +210,7 @@ class WideBand {
   size_t bytes_held() const {
     size_t b = 0;
     for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
-                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &gws})
+                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &gws[0], &gws[1]})
       b += d->size() * sizeof(T);
     return b;
   }
@@ -221,6 +221,12 @@ class WideBand {
   ~WideBand() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
     if (h) cublasDestroy(h);
+    if (st2) {
+      cudaStreamSynchronize(st2);
+      cudaStreamDestroy(st2);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   // The factorization's launch sequence (about a thousand small GEMMs,
@@ -262,6 +268,11 @@ class WideBand {
     pstart_h = pstart;
     psize_h = psize;
     if (!h) cublas_check(cublasCreate(&h), "cublasCreate");
+    if (!st2) {
+      SAPB_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+      SAPB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+      SAPB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    }
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
     if (cublas_ws.size() == 0) cublas_ws.alloc((size_t)64 << 20);
     cublas_check(cublasSetWorkspace(h, cublas_ws.get(), cublas_ws.size()), "cublasSetWorkspace");
@@ -409,11 +420,20 @@ class WideBand {
 
   // tri: 0 full, 1 lower, 2 upper (see k_tgemv).  Grids with fewer than
   // about 2.5 CTAs per SM split the columns over gridDim.z CTAs.
-  DBuf<T> gws;          // column-split partial sums
-  DBuf<unsigned> gctr;  // column-split arrival counters (zero between launches)
+  // Two lanes (streams) for the block sweeps: each takes half of the
+  // partitions, so one lane's launch tails overlap the other's streaming.
+  // Each lane has its own column-split scratch.
+  DBuf<T> gws[2];          // column-split partial sums
+  DBuf<unsigned> gctr[2];  // column-split arrival counters (zero between launches)
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t lane_stream(int lane) const { return lane ? st2 : st; }
   template <int V>
   void gemv_launch(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y,
-                   long long sy, int m, int nbatch, int mode, int tri) {
+                   long long sy, int m, int nbatch, int mode, int tri, int lane) {
+    cudaStream_t ls = lane_stream(lane);
+    DBuf<T>& ws_ = gws[lane];
+    DBuf<unsigned>& ct = gctr[lane];
     constexpr int R = tgemv_rows<T, V>();
     const int ntile = (m + R - 1) / R, pairs = (ntile + 1) / 2;
     const long long base = (long long)pairs * nbatch;
@@ -421,50 +441,70 @@ class WideBand {
     S = std::max(1, std::min(S, m / 256));
     if (S > 1) {
       const size_t need = (size_t)nbatch * ntile * S * R, nctr = (size_t)nbatch * ntile;
-      if (gws.size() < need) gws.alloc(need);
-      if (gctr.size() < nctr) {
-        gctr.alloc(nctr);
-        gctr.zero(st);
+      if (ws_.size() < need) ws_.alloc(need);
+      if (ct.size() < nctr) {
+        SAPB_CUDA(cudaStreamSynchronize(ls));
+        ct.alloc(nctr);
+        ct.zero(ls);
       }
     }
-    k_tgemv<T, V><<<dim3(pairs, nbatch, S), kGemvWarps * 32, 0, st>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri,
-                                                                     gws.get(), gctr.get());
+    k_tgemv<T, V><<<dim3(pairs, nbatch, S), kGemvWarps * 32, 0, ls>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri,
+                                                                     ws_.get(), ct.get());
     SAPB_LAUNCHED();
   }
   void gemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y, long long sy,
-            int m, int nbatch, int mode, int tri) {
+            int m, int nbatch, int mode, int tri, int lane = 0) {
     constexpr int V = 16 / sizeof(T);  // 16-byte loads
     const bool vec = ld % V == 0 && sA % V == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
-    if (vec) gemv_launch<V>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri);
-    else gemv_launch<1>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri);
+    if (vec) gemv_launch<V>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane);
+    else gemv_launch<1>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane);
   }
 
   // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
   // and U_{i,i+1} = L_ii^-1 E_i are lower triangular, U_ii^-1 and
   // L_{i+1,i} = F_i U_ii^-1 upper triangular (the band fits in one block).
   void solve_blocks(T* x) {
-    T* y = yv.get();
-    T* t = tv.get();
+    const int lanes = (P >= 4 && st2) ? 2 : 1;
+    if (lanes == 2) {
+      SAPB_CUDA(cudaEventRecord(ev_fork, st));
+      SAPB_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
+    }
+    const int half = P / 2;
+    for (int lane = 0; lane < lanes; lane++) {
+      const int p0 = lanes == 2 ? lane * half : 0;
+      const int np = lanes == 2 ? (lane ? P - half : half) : P;
+      const long long vo = (long long)p0 * plen;
+      solve_blocks_part(x + vo, yv.get() + vo, tv.get() + vo, p0, np, lane);
+    }
+    if (lanes == 2) {
+      SAPB_CUDA(cudaEventRecord(ev_join, st2));
+      SAPB_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+    }
+  }
+
+  // the block sweeps of partitions [p0, p0+np) on one lane
+  void solve_blocks_part(T* x, T* y, T* t, int p0, int np, int lane) {
     const long long sv = plen;
+    const long long od = (long long)p0 * nb * BB, oo = (long long)p0 * (nb - 1) * BB;
     for (int i = 0; i < nb; i++) {  // y_i = L_ii^-1 (x_i - L_{i,i-1} y_{i-1})
       const T* rhs = x + (long long)i * bs;
       if (i > 0) {
-        gemv(Loff.get() + (long long)(i - 1) * BB, bs, (long long)(nb - 1) * BB, y + (long long)(i - 1) * bs, sv,
-             x + (long long)i * bs, sv, t, sv, bs, P, 1, 2);
+        gemv(Loff.get() + oo + (long long)(i - 1) * BB, bs, (long long)(nb - 1) * BB, y + (long long)(i - 1) * bs, sv,
+             x + (long long)i * bs, sv, t, sv, bs, np, 1, 2, lane);
         rhs = t;
       }
-      gemv(Linv.get() + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, y + (long long)i * bs, sv, bs,
-           P, 0, 1);
+      gemv(Linv.get() + od + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, y + (long long)i * bs, sv,
+           bs, np, 0, 1, lane);
     }
     for (int i = nb - 1; i >= 0; i--) {  // x_i = U_ii^-1 (y_i - U_{i,i+1} x_{i+1})
       const T* rhs = y + (long long)i * bs;
       if (i < nb - 1) {
-        gemv(Uoff.get() + (long long)i * BB, bs, (long long)(nb - 1) * BB, x + (long long)(i + 1) * bs, sv,
-             y + (long long)i * bs, sv, t, sv, bs, P, 1, 1);
+        gemv(Uoff.get() + oo + (long long)i * BB, bs, (long long)(nb - 1) * BB, x + (long long)(i + 1) * bs, sv,
+             y + (long long)i * bs, sv, t, sv, bs, np, 1, 1, lane);
         rhs = t;
       }
-      gemv(Uinv.get() + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, x + (long long)i * bs, sv, bs,
-           P, 0, 2);
+      gemv(Uinv.get() + od + (long long)i * BB, bs, (long long)nb * BB, rhs, sv, nullptr, 0, x + (long long)i * bs, sv,
+           bs, np, 0, 2, lane);
     }
   }
 
