@@ -13,11 +13,14 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <limits>
 #include <queue>
 #include <utility>
+
+#include <omp.h>
 
 namespace sapb {
 namespace rp {
@@ -100,19 +103,31 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
   rev_match.assign(nnz, 0);
   std::vector<char> row_done(n, 0), col_done(n, 0);
   // initial duals: u = per-row minimum weight (reduce_by_key over CSR rows)
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     double m = 0;
     for (int e = Rp[i]; e < Rp[i + 1]; e++) m = (e == Rp[i]) ? weight[e] : std::min(m, weight[e]);
     u[i] = m;
   }
-  // greedy initial matching (init_reduced_cval, graph.h:1890-1918)
+  // greedy initial matching (init_reduced_cval, graph.h:1890-1918): every
+  // column's smallest reduced weight and its entry are independent of the
+  // others (parallel); the claims are then made in column order
+  std::vector<int>& best_e = ws_i1;
+  best_e.assign(n, -1);
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     int best = -1;
+    double vi = kInf;
     for (int e = Rp[i]; e < Rp[i + 1]; e++) {
       if (weight[e] > kInf / 2.0) continue;
       double red = weight[e] - u[Ci[e]];
-      if (v[i] > red) { v[i] = red; best = e; }
+      if (vi > red) { vi = red; best = e; }
     }
+    v[i] = vi;
+    best_e[i] = best;
+  }
+  for (int i = 0; i < n; i++) {
+    const int best = best_e[i];
     if (best >= 0 && !row_done[Ci[best]]) {
       col_done[i] = 1;
       row_done[Ci[best]] = 1;
@@ -210,8 +225,11 @@ void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double
     if (!row_done[i]) throw Error(SAP_MATRIX_SINGULAR, "Singular matrix found");
   col_scale.resize(n);
   row_scale.resize(n);
-  for (int i = 0; i < n; i++) col_scale[i] = std::exp(u[i]);
-  for (int i = 0; i < n; i++) row_scale[i] = std::exp(v[i]) / rowmax[i];
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    col_scale[i] = std::exp(u[i]);
+    row_scale[i] = std::exp(v[i]) / rowmax[i];
+  }
   db_row_perm.resize(n);
   for (int c = 0; c < n; c++) db_row_perm[match[c]] = c;
   // permuted (and scaled) matrix, rows in the new order, entries stable
@@ -246,6 +264,74 @@ static void symmetric_adjacency(const std::vector<int>& er, const std::vector<in
     if (r == c) continue;
     adj[pos[r - nb]++] = c;
     adj[pos[c - nb]++] = r;
+  }
+}
+
+// The same adjacency for a whole CSR matrix (rows rp, columns ci), built in
+// parallel.  Node x's list in the serial builder's order is: the rows r < x
+// of the entries (r, x) in entry order, then row x's own columns, then the
+// rows r > x of the entries (r, x).  The column lists are a stable transpose:
+// every thread counts the columns of its block of rows, the counts are
+// turned into per-(column, thread) offsets, and each thread places its rows
+// in order, so every column lists its rows in entry order without sorting.
+static void symmetric_adjacency_csr(int n, const std::vector<int>& rp, const std::vector<int>& ci,
+                                    std::vector<int>& off, std::vector<int>& adj, std::vector<int>& cnt,
+                                    std::vector<int>& cstart, std::vector<int>& tr) {
+  const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
+  cnt.resize((size_t)nt * n);
+  cstart.assign(n + 1, 0);
+  off.assign(n + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num(), nth = omp_get_num_threads();
+    const int r0 = (int)((long long)n * t / nth), r1 = (int)((long long)n * (t + 1) / nth);
+    int* c = cnt.data() + (size_t)t * n;
+    std::fill(c, c + n, 0);
+    for (int r = r0; r < r1; r++) {
+      int own = 0;
+      for (int e = rp[r]; e < rp[r + 1]; e++)
+        if (ci[e] != r) {
+          own++;
+          c[ci[e]]++;
+        }
+      off[r + 1] = own;
+    }
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int x = 0; x < n; x++) {
+      int sum = 0;
+      for (int u = 0; u < nth; u++) {
+        int& v = cnt[(size_t)u * n + x];
+        const int k = v;
+        v = sum;
+        sum += k;
+      }
+      cstart[x + 1] = sum;
+    }
+#pragma omp single
+    {
+      for (int i = 0; i < n; i++) {
+        off[i + 1] += off[i] + cstart[i + 1];
+        cstart[i + 1] += cstart[i];
+      }
+      tr.resize(cstart[n]);
+      adj.resize(off[n]);
+    }
+    for (int r = r0; r < r1; r++)
+      for (int e = rp[r]; e < rp[r + 1]; e++) {
+        const int x = ci[e];
+        if (x != r) tr[cstart[x] + c[x]++] = r;
+      }
+#pragma omp barrier
+#pragma omp for schedule(static)
+    for (int x = 0; x < n; x++) {
+      int w = off[x], k = cstart[x];
+      const int k1 = cstart[x + 1];
+      for (; k < k1 && tr[k] < x; k++) adj[w++] = tr[k];
+      for (int e = rp[x]; e < rp[x + 1]; e++)
+        if (ci[e] != x) adj[w++] = ci[e];
+      for (; k < k1; k++) adj[w++] = tr[k];
+    }
   }
 }
 
@@ -295,6 +381,132 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
   return true;
 }
 
+// cm_bfs over the whole graph (nodes [0, n), degrees fixed), level by
+// level and in parallel, with the same result.  The FIFO is consumed in
+// batches: a batch is everything queued while the previous batch was
+// scanned.  A node queued from a batch belongs to the first node of the
+// batch, in FIFO order, that meets it unqueued (smallest claim), and every
+// claimer queues its nodes through the same degree heap in its adjacency
+// order, so the concatenation equals the serial queue.  Small batches are
+// scanned serially.  claim[] is INT_MAX everywhere on entry and on return.
+static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& off, const std::vector<int>& adj,
+                          const std::vector<int>& degree, std::vector<int>& pushed, std::vector<int>& level,
+                          std::vector<int>& order, std::vector<int>& claim, std::vector<int>& meta) {
+  constexpr int kSerialBatch = 384;
+  const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
+  int h0 = 0, t0 = 1, scan = 0, total = 0;
+  bool ok = true;
+  level[root] = 0;
+  pushed[root] = trial;
+  order[0] = root;
+  meta.resize(3 * ((size_t)n + 1));  // per batch position: thread, start in its buffer, count
+  int* cl = claim.data();
+  std::vector<std::vector<int>> bufs(nt);
+  using Kids = std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree>;
+#pragma omp parallel num_threads(nt)
+  {
+    Kids kids;
+    const int tid = omp_get_thread_num();
+    std::vector<int>& buf = bufs[tid];
+    for (;;) {
+      const int m = t0 - h0;  // shared, stable between barriers
+      if (m == 0) break;
+      if (m < kSerialBatch) {
+#pragma omp single
+        {
+          int tail = t0;
+          for (int k = h0; k < t0; k++) {
+            const int u = order[k], lv = level[u];
+            for (int e = off[u]; e < off[u + 1]; e++) {
+              const int t = adj[e];
+              if (pushed[t] == trial) continue;
+              pushed[t] = trial;
+              kids.push(std::make_pair(t, degree[t]));
+              level[t] = lv + 1;
+            }
+            while (!kids.empty()) {
+              order[tail++] = kids.top().first;
+              kids.pop();
+            }
+          }
+          total = tail - t0;
+        }
+      } else {
+        // claims: the smallest batch position meeting the node
+#pragma omp for schedule(dynamic, 64)
+        for (int k = h0; k < t0; k++) {
+          const int u = order[k];
+          for (int e = off[u]; e < off[u + 1]; e++) {
+            const int t = adj[e];
+            if (pushed[t] == trial) continue;
+            int cur = __atomic_load_n(cl + t, __ATOMIC_RELAXED);
+            while (k < cur && !__atomic_compare_exchange_n(cl + t, &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+            }
+          }
+        }
+        // every claimer takes its nodes (each once) through the heap into
+        // its thread's buffer
+        buf.clear();
+#pragma omp for schedule(dynamic, 64)
+        for (int k = h0; k < t0; k++) {
+          const int u = order[k], lv = level[u];
+          for (int e = off[u]; e < off[u + 1]; e++) {
+            const int t = adj[e];
+            if (__atomic_load_n(cl + t, __ATOMIC_RELAXED) != k) continue;
+            __atomic_store_n(cl + t, INT_MAX, __ATOMIC_RELAXED);
+            pushed[t] = trial;
+            level[t] = lv + 1;
+            kids.push(std::make_pair(t, degree[t]));
+          }
+          int* md = meta.data() + 3 * (size_t)(k - h0);
+          md[0] = tid;
+          md[1] = (int)buf.size();
+          while (!kids.empty()) {
+            buf.push_back(kids.top().first);
+            kids.pop();
+          }
+          md[2] = (int)buf.size() - md[1];
+        }
+#pragma omp single
+        {
+          int run = 0;
+          for (int k = 0; k < m; k++) {
+            int* md = meta.data() + 3 * (size_t)k;
+            const int c = md[2];
+            md[2] = run;  // now: position in the next batch
+            run += c;
+          }
+          total = run;
+        }
+#pragma omp for schedule(static)
+        for (int k = 0; k < m; k++) {
+          const int* md = meta.data() + 3 * (size_t)k;
+          const int end = k + 1 < m ? md[5] : total;
+          std::copy(bufs[md[0]].begin() + md[1], bufs[md[0]].begin() + md[1] + (end - md[2]), order.begin() + t0 + md[2]);
+        }
+      }
+#pragma omp single
+      {
+        h0 = t0;
+        t0 += total;
+        if (t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
+          int i = scan;
+          while (i < n && pushed[i] == trial) i++;
+          if (i >= n) {
+            ok = false;
+          } else {
+            order[t0++] = i;
+            pushed[i] = trial;
+            scan = i;
+          }
+        }
+        if (t0 == n) h0 = t0;  // every node queued: the rest adds nothing
+      }
+    }
+  }
+  return ok;
+}
+
 // RCM on the DB-reordered matrix (graph.h:1371-1584).  As in the reference:
 // BFS priority is the CSR row length; the trial loop stops after the second
 // trial (its level bookkeeping never advances); a later trial starts from
@@ -317,12 +529,12 @@ int Pipeline<T>::rcm() {
   for (int e = 0; e < nz; e++) best_bw = std::max(best_bw, std::abs(row[e] - m_ci[e]));
   std::vector<int>& off = ws_off;
   std::vector<int>& adj = ws_adj;
-  symmetric_adjacency(row, m_ci, 0, nz, 0, n, n, off, adj);
+  symmetric_adjacency_csr(n, m_rp, m_ci, off, adj, ws_cnt, ws_i1, ws_i2);
   rcm_order.resize(n);
   for (int i = 0; i < n; i++) rcm_order[i] = i;
   rcm_pos.assign(n, 0);
   std::vector<char> tried(n, 0);
-  std::vector<int> pushed(n, -1), level(n, 0), order(n);
+  std::vector<int> pushed(n, -1), level(n, 0), order(n), claim(n, INT_MAX);
   const int tracked_level = 0;  // never advanced (graph.h:1413-1414)
   for (int trial = 0; trial < 5; trial++) {
     int root;
@@ -342,8 +554,7 @@ int Pipeline<T>::rcm() {
       while (tried[root]) root = (root + 1) % n;
     }
     tried[root] = 1;
-    int unused = 0;
-    if (!cm_bfs(root, 0, n, trial, off, adj, &degree, pushed, level, order, unused)) break;
+    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, ws_i2)) break;
     for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
     int bw = 0;
 #pragma omp parallel for reduction(max : bw) schedule(static)
@@ -373,18 +584,46 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   // The reference's bucketed list: entries ordered by distance |i - j|, rows
   // ascending and CSR order inside a distance group.  Group d occupies
   // [gstart[d], gstart[d+1]); only the values are needed (for the squares).
+  // Built in parallel as a stable bucket sort: every thread counts the
+  // distances of its block of rows, the counts become per-(distance, thread)
+  // offsets, and each thread places its rows' values in order.
+  int dmax = 0;
+#pragma omp parallel for schedule(static, 4096) reduction(max : dmax)
+  for (int i = 0; i < n; i++)
+    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) dmax = std::max(dmax, std::abs(i - m_ci[e]));
+  const int nd = dmax + 1;
   std::vector<int>& gstart = ws_i1;
   gstart.assign(n + 1, 0);
-  for (int i = 0; i < n; i++)
-    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) gstart[std::abs(i - m_ci[e]) + 1]++;
-  for (int d = 0; d < n; d++) gstart[d + 1] += gstart[d];
   std::vector<T>& bv = ws_t0;
   bv.resize(nz);
+  const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
+  std::vector<int>& cnt = ws_cnt;
+  cnt.resize((size_t)nt * nd);
+#pragma omp parallel num_threads(nt)
   {
-    std::vector<int>& pos = ws_i2;
-    pos.assign(gstart.begin(), gstart.end() - 1);
-    for (int i = 0; i < n; i++)
-      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[pos[std::abs(i - m_ci[e])]++] = m_val[e];
+    const int t = omp_get_thread_num(), nth = omp_get_num_threads();
+    const int r0 = (int)((long long)n * t / nth), r1 = (int)((long long)n * (t + 1) / nth);
+    int* c = cnt.data() + (size_t)t * nd;
+    std::fill(c, c + nd, 0);
+    for (int i = r0; i < r1; i++)
+      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) c[std::abs(i - m_ci[e])]++;
+#pragma omp barrier
+#pragma omp single
+    {
+      int run = 0;
+      for (int d = 0; d < nd; d++) {
+        gstart[d] = run;
+        for (int u = 0; u < nth; u++) {
+          int& v = cnt[(size_t)u * nd + d];
+          const int k = v;
+          v = run;
+          run += k;
+        }
+      }
+      for (int d = nd; d <= n; d++) gstart[d] = run;
+    }
+    for (int i = r0; i < r1; i++)
+      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[c[std::abs(i - m_ci[e])]++] = m_val[e];
   }
   T total = T(0);
   for (int e = 0; e < nz; e++) total = total + m_val[e] * m_val[e];
@@ -470,36 +709,61 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
   const int q = n / P, rem = n % P;
   const size_t KK = (size_t)K * K;
   offd_size = 2 * KK * (P - 1);
-  offd_idx.clear();
-  offd_val.clear();
   couples_right.assign(n, 0);
   d_rp.assign(n + 1, 0);
-  d_ci.clear();
-  d_val.clear();
+  // per row: entries inside its partition (d_rp) and coupling entries
+  // (ocnt), then row offsets, then the entries in row order
+  std::vector<int>& ocnt = ws_i1;
+  ocnt.assign(n + 1, 0);
+#pragma omp parallel for schedule(static)
   for (int j = 0; j < n; j++) {
     const int pr = partition_of(j, q, rem);
+    int dc = 0, oc = 0;
+    char right = 0;
+    for (int e = m_rp[j]; e < m_rp[j + 1]; e++) {
+      const int pc = partition_of(m_ci[e], q, rem);
+      if (pc == pr) {
+        dc++;
+      } else {
+        oc++;
+        right |= (char)(pc > pr);
+      }
+    }
+    d_rp[j + 1] = dc;
+    ocnt[j + 1] = oc;
+    couples_right[j] = right;
+  }
+  for (int i = 0; i < n; i++) {
+    d_rp[i + 1] += d_rp[i];
+    ocnt[i + 1] += ocnt[i];
+  }
+  d_ci.resize(d_rp[n]);
+  d_val.resize(d_rp[n]);
+  offd_idx.resize(ocnt[n]);
+  offd_val.resize(ocnt[n]);
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < n; j++) {
+    const int pr = partition_of(j, q, rem);
+    int dw = d_rp[j], ow = ocnt[j];
     for (int e = m_rp[j]; e < m_rp[j + 1]; e++) {
       const int l = m_ci[e];
       const int pc = partition_of(l, q, rem);
       if (pc == pr) {
-        d_ci.push_back(l);
-        d_val.push_back(m_val[e]);
-        d_rp[j + 1]++;
+        d_ci[dw] = l;
+        d_val[dw++] = m_val[e];
       } else if (pc > pr) {
-        couples_right[j] = 1;
         const int row_end = q * pr + (pr < rem ? pr + q + 1 : rem + q);
         const int col_start = q * pc + (pc < rem ? pc : rem);
-        offd_idx.push_back((long long)(pr * 2 * KK + (size_t)(j + K - row_end) * K + (l - col_start)));
-        offd_val.push_back(m_val[e]);
+        offd_idx[ow] = (long long)(pr * 2 * KK + (size_t)(j + K - row_end) * K + (l - col_start));
+        offd_val[ow++] = m_val[e];
       } else {
         const int row_start = q * pr + (pr < rem ? pr : rem);
         const int col_end = q * pc + (pc < rem ? pc + q + 1 : rem + q);
-        offd_idx.push_back((long long)((pc * 2 + 1) * KK + (size_t)(j - row_start) * K + (l - col_end + K)));
-        offd_val.push_back(m_val[e]);
+        offd_idx[ow] = (long long)((pc * 2 + 1) * KK + (size_t)(j - row_start) * K + (l - col_end + K));
+        offd_val[ow++] = m_val[e];
       }
     }
   }
-  for (int i = 0; i < n; i++) d_rp[i + 1] += d_rp[i];
 }
 
 // Second-level reordering (secondLevelReordering + partitionedRCM,
@@ -513,6 +777,7 @@ void Pipeline<T>::second_level(int K, int P) {
   const int dz = (int)d_ci.size();
   std::vector<int>& row = ws_i0;
   row.resize(dz);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++)
     for (int e = d_rp[i]; e < d_rp[i + 1]; e++) row[e] = i;
   second_order.assign(n, 0);
@@ -601,12 +866,19 @@ template <typename T>
 void Pipeline<T>::assemble_var_band(int P) {
   const int q = n / P, rem = n % P;
   part_k.assign(P, 0);
-  for (int j = 0; j < n; j++)
-    for (int e = d_rp[j]; e < d_rp[j + 1]; e++) {
-      int l = d_ci[e];
-      int p = partition_of(l, q, rem);
-      part_k[p] = std::max(part_k[p], std::abs(l - j));
-    }
+#pragma omp parallel
+  {
+    std::vector<int> kp(P, 0);
+#pragma omp for schedule(static) nowait
+    for (int j = 0; j < n; j++)
+      for (int e = d_rp[j]; e < d_rp[j + 1]; e++) {
+        const int l = d_ci[e];
+        const int p = partition_of(l, q, rem);
+        kp[p] = std::max(kp[p], std::abs(l - j));
+      }
+#pragma omp critical
+    for (int p = 0; p < P; p++) part_k[p] = std::max(part_k[p], kp[p]);
+  }
 }
 
 // The whole sparse setup of transformToBandedMatrix (precond.h:1656-2101)
@@ -629,9 +901,11 @@ void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<doubl
     row_scale.assign(n, 1.0);
     col_scale.assign(n, 1.0);
   }
-  k_db = 0;
+  int kdb = 0;
+#pragma omp parallel for schedule(static) reduction(max : kdb)
   for (int i = 0; i < n; i++)
-    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) k_db = std::max(k_db, std::abs(i - m_ci[e]));
+    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) kdb = std::max(kdb, std::abs(i - m_ci[e]));
+  k_db = kdb;
   lap("db");
   if (max_bandwidth > 64) {
     k_reorder = rcm();
@@ -667,8 +941,11 @@ void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<doubl
   // and input column of band column k
   final_pos.resize(n);
   final_order.resize(n);
-  for (int k = 0; k < n; k++) final_order[k] = rcm_order[second_order[k]];
-  for (int i = 0; i < n; i++) final_pos[i] = second_pos[rcm_pos[db_row_perm[i]]];
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; k++) {
+    final_order[k] = rcm_order[second_order[k]];
+    final_pos[k] = second_pos[rcm_pos[db_row_perm[k]]];
+  }
   lap("compose");
 }
 

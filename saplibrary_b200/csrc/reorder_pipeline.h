@@ -59,7 +59,7 @@ class Pipeline {
 
   // scratch kept across runs of the same object (a repeated setup reuses
   // its memory instead of allocating and page-faulting it again)
-  std::vector<int> ws_i0, ws_i1, ws_i2, ws_off, ws_adj, tmp_rp, tmp_ci;
+  std::vector<int> ws_i0, ws_i1, ws_i2, ws_off, ws_adj, ws_cnt, tmp_rp, tmp_ci;
   std::vector<T> ws_t0, tmp_val;
 
   // wall time of the stages of run(), in order (ms)

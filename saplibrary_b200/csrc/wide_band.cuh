@@ -7,8 +7,8 @@
 // These are exactly the L and U factors of the band LU (the LU without
 // pivoting is unique), computed as dense block operations: the diagonal block
 // LU is recursive and also returns L_ii^-1 and U_ii^-1, so every step except
-// a 32x32 leaf is a matrix product.  The apply then reduces to batched
-// matrix-vector products per block row:
+// the leaves (one CTA each, see k_leaf_lu) is a matrix product.  The apply
+// then reduces to batched matrix-vector products per block row:
 //     y_i = L_ii^-1 (f_i - L_{i,i-1} y_{i-1}),  x_i = U_ii^-1 (y_i - U_{i,i+1} x_{i+1}).
 // Blocks are column-major (element (r, c) at c*bs + r); vectors are padded to
 // nb*bs rows per partition, padding rows carry an identity diagonal.
@@ -98,65 +98,144 @@ __global__ void k_sub_fill(T* __restrict__ dst, int ldd, long long sd, int m, in
       dst[b * sd + (long long)c * ldd + r] = value;
 }
 
-// Leaf of the recursive LU: an n x n (n <= 32) diagonal block factored in
-// place without pivoting (the reference's boosting rule when `boost`), and
-// its L^-1 (unit lower) and U^-1 (upper) written to Li / Ui.  One CTA of 32
-// threads per batch element; thread r owns row r.
-template <typename T>
-__global__ void __launch_bounds__(32) k_leaf_lu(T* __restrict__ M, T* __restrict__ Li, T* __restrict__ Ui, int ld,
-                                                long long stride, int n, int boost, int* __restrict__ zero_flag) {
-  __shared__ T a[kLeaf][kLeaf + 1];
-  __shared__ T li[kLeaf][kLeaf + 1];
-  __shared__ T ui[kLeaf][kLeaf + 1];
-  const int r = threadIdx.x;
-  T* Mb = M + blockIdx.x * stride;
+// Leaf of the recursive block LU: one CTA per batch element factors an n x n
+// block (n <= NL) without pivoting (pivots boosted as in the band LU when
+// `boost`, else a pivot below 1e-7 raises zero_flag) and writes L^-1 (unit
+// lower) to Li and U^-1 (upper) to Ui; M is only read.  Both inverses come
+// out of the elimination loop itself (Gauss-Jordan):
+//   * eliminating below the pivot in [A | I] turns I into L^-1, stored in
+//     place of the multipliers (step j sets G[r][j] = -l_r and updates the
+//     columns c < j like the trailing ones);
+//   * eliminating below the diagonal of [U^T | I] (row j of U is final at
+//     step j) turns I into E with U^-T = diag(U)^-1 E, so U^-1 = E^T diag(U)^-1.
+// The working matrix G and E live in registers: thread (ty, tx) of the RY x
+// 32 CTA owns rows ty + RY*i and columns tx + 32*k.  Each step the owners of
+// pivot row j and pivot column j publish them to shared memory (two buffers,
+// so one barrier per step); rows r <= j are skipped per warp.
+template <typename T, int NL, int RY>
+__global__ void __launch_bounds__(RY * 32) k_leaf_lu(const T* __restrict__ M, T* __restrict__ Li, T* __restrict__ Ui,
+                                                     int ld, long long stride, int n, int boost,
+                                                     int* __restrict__ zero_flag) {
+  constexpr int TM = NL / RY, TN = NL / 32, NT = RY * 32, SP = NL + 1;
+  static_assert(NL % RY == 0 && NL % 32 == 0, "leaf tiling");
+  extern __shared__ __align__(16) unsigned char leaf_smem[];
+  T* S = reinterpret_cast<T*>(leaf_smem);  // NL x SP staging (row-major)
+  T* colj = S + NL * SP;                   // [2][NL] pivot column
+  T* rowj = colj + 2 * NL;                 // [2][NL] pivot row of G
+  T* erow = rowj + 2 * NL;                 // [2][NL] pivot row of E
+  T* piv = erow + 2 * NL;                  // [NL] pivots as used
+  const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
+  const T* Mb = M + blockIdx.x * stride;
   T* Lb = Li + blockIdx.x * stride;
   T* Ub = Ui + blockIdx.x * stride;
-  for (int c = 0; c < n; c++) a[r][c] = (r < n) ? Mb[(long long)c * ld + r] : T(0);
-  __syncwarp();
+  for (int idx = t; idx < n * n; idx += NT) {
+    const int c = idx / n, r = idx - c * n;
+    S[r * SP + c] = Mb[(long long)c * ld + r];
+  }
+  __syncthreads();
+  T g[TM][TN], e[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int k = 0; k < TN; k++) {
+      const int r = ty + RY * i, c = tx + 32 * k;
+      g[i][k] = (r < n && c < n) ? S[r * SP + c] : (r == c ? T(1) : T(0));
+      e[i][k] = r == c ? T(1) : T(0);
+    }
   for (int j = 0; j < n; j++) {
-    T p = a[j][j];
+    const int b = (j & 1) * NL;
+    if (tx == (j & 31)) {  // owners of column j
+      const int kj = j >> 5;
+#pragma unroll
+      for (int i = 0; i < TM; i++) {
+        T v = g[i][0];
+#pragma unroll
+        for (int k = 1; k < TN; k++)
+          if (kj == k) v = g[i][k];
+        colj[b + ty + RY * i] = v;
+      }
+    }
+    if (ty == j % RY) {  // owners of row j
+      const int ij = j / RY;
+#pragma unroll
+      for (int k = 0; k < TN; k++) {
+        T v = g[0][k], w = e[0][k];
+#pragma unroll
+        for (int i = 1; i < TM; i++)
+          if (ij == i) {
+            v = g[i][k];
+            w = e[i][k];
+          }
+        rowj[b + tx + 32 * k] = v;
+        erow[b + tx + 32 * k] = w;
+      }
+    }
+    __syncthreads();
+    T p = rowj[b + j];
     if (boost) p = boost_pivot(p);
-    else if (r == 0 && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
-    __syncwarp();
-    if (r == j) a[j][j] = p;
-    if (r > j && r < n) {
-      const T l = a[r][j] / p;
-      a[r][j] = l;
-      for (int c = j + 1; c < n; c++) a[r][c] -= l * a[j][c];
+    if (t == 0) {
+      piv[j] = p;
+      if (!boost && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
     }
-    __syncwarp();
-  }
-  // inverses: column r of L^-1 by forward substitution, row r of U^-1 by
-  // backward substitution (each thread independent)
-  if (r < n) {
-    for (int i = 0; i < n; i++) li[i][r] = (i == r) ? T(1) : T(0);
-    for (int i = r + 1; i < n; i++) {
-      T s = T(0);
-      for (int k = r; k < i; k++) s += a[i][k] * li[k][r];
-      li[i][r] = -s;
+    const T inv = T(1) / p;
+    T xr[TN], xe[TN];
+#pragma unroll
+    for (int k = 0; k < TN; k++) {
+      xr[k] = rowj[b + tx + 32 * k];
+      xe[k] = erow[b + tx + 32 * k];
     }
-    for (int c = 0; c < n; c++) ui[r][c] = T(0);
-  }
-  __syncwarp();
-  // U^-1 column by column: column c solved by thread c
-  if (r < n) {
-    const int c = r;
-    ui[c][c] = T(1) / a[c][c];
-    for (int i = c - 1; i >= 0; i--) {
-      T s = T(0);
-      for (int k = i + 1; k <= c; k++) s += a[i][k] * ui[k][c];
-      ui[i][c] = -s / a[i][i];
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+      const int r = ty + RY * i;
+      if (r > j) {  // uniform across the warp
+        const T l = colj[b + r] * inv, m = rowj[b + r] * inv;
+#pragma unroll
+        for (int k = 0; k < TN; k++) {
+          const int c = tx + 32 * k;
+          g[i][k] = (c == j) ? -l : g[i][k] - l * xr[k];
+          if (c <= j) e[i][k] -= m * xe[k];
+        }
+      }
     }
   }
-  __syncwarp();
-  if (r < n)
-    for (int c = 0; c < n; c++) {
-      Mb[(long long)c * ld + r] = a[r][c];
-      Lb[(long long)c * ld + r] = li[r][c];
-      Ub[(long long)c * ld + r] = ui[r][c];
+  __syncthreads();
+  // L^-1: unit diagonal, strict lower part of G
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int k = 0; k < TN; k++) {
+      const int r = ty + RY * i, c = tx + 32 * k;
+      S[r * SP + c] = r > c ? g[i][k] : (r == c ? T(1) : T(0));
     }
+  __syncthreads();
+  for (int idx = t; idx < n * n; idx += NT) {
+    const int c = idx / n, r = idx - c * n;
+    Lb[(long long)c * ld + r] = S[r * SP + c];
+  }
+  __syncthreads();
+  // U^-1 (row c, column r) = E[r][c] / u_rr for c <= r
+#pragma unroll
+  for (int i = 0; i < TM; i++)
+#pragma unroll
+    for (int k = 0; k < TN; k++) {
+      const int r = ty + RY * i, c = tx + 32 * k;
+      S[c * SP + r] = (c <= r && r < n) ? e[i][k] / piv[r] : T(0);
+    }
+  __syncthreads();
+  for (int idx = t; idx < n * n; idx += NT) {
+    const int c = idx / n, r = idx - c * n;
+    Ub[(long long)c * ld + r] = S[r * SP + c];
+  }
 }
+
+// Leaf size and CTA rows of k_leaf_lu per value type (register budget:
+// 2 * TM * TN values per thread).
+template <typename T>
+struct LeafShape {
+  static constexpr int NL = sizeof(T) == 4 ? 128 : 64;
+  static constexpr int RY = 16;
+  static constexpr size_t smem = (size_t)(NL * (NL + 1) + 7 * NL) * sizeof(T);
+};
 
 // Batched dense matrix-vector product with an n x n column-major block:
 //   y = A x            (mode 0)

@@ -63,7 +63,7 @@ class BlockLU {
   int batch = 0;
   bool boost = true;
   int* flag = nullptr;
-  Mat<T> W;  // workspace, >= n x n per batch element
+  Mat<T> W;  // workspace, >= n x n per batch element (the inverse-block temporaries of rec)
 
   void gemm(int m, int n, int k, T alpha, Mat<T> A, Mat<T> B, T beta, Mat<T> C) {
     Gemm<T>::run(h, m, n, k, alpha, A.p, A.ld, A.s, B.p, B.ld, B.s, beta, C.p, C.ld, C.s, batch);
@@ -151,30 +151,92 @@ class BlockLU {
     prod_UL_acc(n2, alpha, A.at(n1, n1), B.at(n1, n1), C.at(n1, n1));
   }
 
-  // M (n x n at M) = L U in place; Li = L^-1, Ui = U^-1 (both pre-zeroed).
-  void rec(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n) {
-    if (n <= kLeaf) {
+  // Second lane: the two independent products of every recursion step (the
+  // U12 / L21 panels, then the two off-diagonal inverse blocks) run on it
+  // concurrently with the first; it has its own cuBLAS handle and workspace.
+  cublasHandle_t h2 = nullptr;
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+  void fork() {
+    if (!st2) return;
+    SAPB_CUDA(cudaEventRecord(ev_a, st));
+    SAPB_CUDA(cudaStreamWaitEvent(st2, ev_a, 0));
+  }
+  void join() {
+    if (!st2) return;
+    SAPB_CUDA(cudaEventRecord(ev_b, st2));
+    SAPB_CUDA(cudaStreamWaitEvent(st, ev_b, 0));
+  }
+  template <class F>
+  void lane2(F&& f) {
+    if (!st2) return f();
+    struct Swap {
+      BlockLU* b;
+      explicit Swap(BlockLU* b_) : b(b_) { flip(); }
+      ~Swap() { flip(); }
+      void flip() {
+        std::swap(b->h, b->h2);
+        std::swap(b->st, b->st2);
+      }
+    } guard(this);
+    f();
+  }
+
+  // Recursion workspace: every step keeps its U12 and L21 panels until its
+  // inverse blocks are formed; rw holds them level by level (rec_ws(n)
+  // values per batch element for an n x n factorization, batch stride rws).
+  T* rw = nullptr;
+  long long rws = 0;
+  static int split(int n) {
+    int n1 = ((n / 2 + kLeaf - 1) / kLeaf) * kLeaf;
+    if (n1 >= n) n1 = n - kLeaf;
+    return n1;
+  }
+  static constexpr int kNL = LeafShape<T>::NL;  // largest leaf of the recursion
+  static long long rec_ws(int n) {
+    if (n <= kNL) return 0;
+    const int n1 = split(n), n2 = n - n1;
+    return std::max(rec_ws(n1), 2LL * n1 * n2 + rec_ws(n2));
+  }
+
+  // Li = L^-1, Ui = U^-1 of M = L U (n x n at M; Li, Ui pre-zeroed).  M's
+  // trailing blocks are overwritten by the Schur complements.  wo: this
+  // level's offset into rw.
+  void rec(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n, long long wo = 0) {
+    if (n <= kNL) {
       if (M.s != Li.s || Li.s != Ui.s) throw Error(SAP_ERR_INVALID_ARGUMENT, "leaf strides differ");
-      k_leaf_lu<T><<<batch, 32, 0, st>>>(M.p, Li.p, Ui.p, M.ld, M.s, n, boost ? 1 : 0, flag);
+      using LS = LeafShape<T>;
+      static bool smem_set = false;  // first call runs outside any graph capture
+      if (!smem_set) {
+        SAPB_CUDA(cudaFuncSetAttribute(k_leaf_lu<T, LS::NL, LS::RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)LS::smem));
+        smem_set = true;
+      }
+      k_leaf_lu<T, LS::NL, LS::RY><<<batch, LS::RY * 32, LS::smem, st>>>(M.p, Li.p, Ui.p, M.ld, M.s, n, boost ? 1 : 0,
+                                                                          flag);
       SAPB_LAUNCHED();
       return;
     }
-    int n1 = ((n / 2 + kLeaf - 1) / kLeaf) * kLeaf;
-    if (n1 >= n) n1 = n - kLeaf;
-    const int n2 = n - n1;
-    rec(M, Li, Ui, n1);
-    // U12 = L11^-1 A12 ; L21 = A21 U11^-1 ; A22 -= L21 U12
-    prod_LF(n1, n2, T(1), Li, M.at(0, n1), T(0), W);
-    copy(W, M.at(0, n1), n1, n2);
-    prod_FU(n2, n1, T(1), M.at(n1, 0), Ui, T(0), W);
-    copy(W, M.at(n1, 0), n2, n1);
-    gemm(n2, n2, n1, T(-1), M.at(n1, 0), M.at(0, n1), T(1), M.at(n1, n1));
-    rec(M.at(n1, n1), Li.at(n1, n1), Ui.at(n1, n1), n2);
-    // (L^-1)21 = -L22^-1 L21 L11^-1 ; (U^-1)12 = -U11^-1 U12 U22^-1
-    prod_FL(n2, n1, T(1), M.at(n1, 0), Li, T(0), W);
-    prod_LF(n2, n1, T(-1), Li.at(n1, n1), W, T(0), Li.at(n1, 0));
-    prod_FU(n1, n2, T(1), M.at(0, n1), Ui.at(n1, n1), T(0), W);
-    prod_UF(n1, n2, T(-1), Ui, W, T(0), Ui.at(0, n1));
+    const int n1 = split(n), n2 = n - n1;
+    rec(M, Li, Ui, n1, wo);
+    // U12 = L11^-1 A12, L21 = A21 U11^-1 (independent); A22 -= L21 U12
+    const Mat<T> U12{rw + wo, n1, rws}, L21{rw + wo + (long long)n1 * n2, n2, rws};
+    fork();
+    prod_LF(n1, n2, T(1), Li, M.at(0, n1), T(0), U12);
+    lane2([&] { prod_FU(n2, n1, T(1), M.at(n1, 0), Ui, T(0), L21); });
+    join();
+    gemm(n2, n2, n1, T(-1), L21, U12, T(1), M.at(n1, n1));
+    rec(M.at(n1, n1), Li.at(n1, n1), Ui.at(n1, n1), n2, wo + 2LL * n1 * n2);
+    // (L^-1)21 = -L22^-1 L21 L11^-1, (U^-1)12 = -U11^-1 U12 U22^-1 (independent)
+    const Mat<T> Tl{W.p, n2, W.s}, Tu{W.p + (long long)n1 * n2, n1, W.s};
+    fork();
+    prod_FL(n2, n1, T(1), L21, Li, T(0), Tl);
+    prod_LF(n2, n1, T(-1), Li.at(n1, n1), Tl, T(0), Li.at(n1, 0));
+    lane2([&] {
+      prod_FU(n1, n2, T(1), U12, Ui.at(n1, n1), T(0), Tu);
+      prod_UF(n1, n2, T(-1), Ui, Tu, T(0), Ui.at(0, n1));
+    });
+    join();
   }
 };
 
@@ -206,12 +268,13 @@ class WideBand {
   // setup workspaces, kept (with everything above) across setups of the
   // same layout so that a repeated setup does not free and re-allocate
   DBuf<T> Dw, Lw, Uw, Ww, X, Wt, S, Ws;
+  DBuf<T> Rw, Rs;  // recursion workspaces of the partition factors / the reduced system
 
   // device bytes this object holds
   size_t bytes_held() const {
     size_t b = 0;
     for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
-                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &gws[0], &gws[1]})
+                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1]})
       b += d->size() * sizeof(T);
     return b;
   }
@@ -221,11 +284,10 @@ class WideBand {
   WideBand& operator=(const WideBand&) = delete;
   ~WideBand() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
+    if (st2) cudaStreamSynchronize(st2);
     if (h) cublasDestroy(h);
-    if (st2) {
-      cudaStreamSynchronize(st2);
-      cudaStreamDestroy(st2);
-    }
+    if (h2) cublasDestroy(h2);
+    if (st2) cudaStreamDestroy(st2);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
   }
@@ -236,19 +298,22 @@ class WideBand {
   // (every buffer it touches is kept across setups of the layout).
   cudaGraphExec_t fgraph = nullptr;
   long long fgraph_key = -1;
+  int fgraph_cut = 0;
   int fgraph_runs = 0;
   bool fgraph_failed = false;
   int64_t fgraph_launches = 0, fgraph_lib_calls = 0;
-  DBuf<unsigned char> cublas_ws;  // fixed cuBLAS workspace (no allocation inside a capture)
+  DBuf<unsigned char> cublas_ws, cublas_ws2;  // fixed cuBLAS workspaces (no allocation inside a capture)
+  cublasHandle_t h2 = nullptr;                  // bound to st2 (second lane of the factorization)
 
   // Block size bs >= the largest half-bandwidth, a multiple of the leaf size.
   static int block_size(int kmax) { return std::max(kLeaf, ((kmax + kLeaf - 1) / kLeaf) * kLeaf); }
 
-  // Device bytes of the factors for n rows in P partitions (for the memory check).
+  // Device bytes of the factors and the factorization workspaces for n rows
+  // in P partitions (for the memory check).
   static double factor_bytes(int n, int P, int kmax) {
     const double b = block_size(kmax);
     const double nbp = std::ceil((double)(n / P + 1) / b);
-    return 4.0 * P * nbp * b * b * sizeof(T);
+    return (4.0 * nbp + 5.0) * P * b * b * sizeof(T);
   }
 
   // tf32: FP32 block products on the tensor cores (TF32 inputs, FP32
@@ -263,8 +328,23 @@ class WideBand {
     if (e && std::atoi(e) > 0) return std::atoi(e);
     return tf32 ? (1 << 30) : 384;
   }
+  // the same cut-off for the products of the partition factorization;
+  // SAPB_FACTOR_CUT overrides
+  int factor_cut() const {
+    const char* e = std::getenv("SAPB_FACTOR_CUT");
+    if (e && std::atoi(e) > 0) return std::atoi(e);
+    return tf32 ? (1 << 30) : 384;
+  }
   void math_mode(bool fast) {
-    cublas_check(cublasSetMathMode(h, fast ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_PEDANTIC_MATH), "cublasSetMathMode");
+    for (cublasHandle_t x : {h, h2})
+      cublas_check(cublasSetMathMode(x, fast ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_PEDANTIC_MATH), "cublasSetMathMode");
+  }
+  // the second lane of a recursive factorization
+  void lanes(BlockLU<T>& lu) {
+    lu.h2 = h2;
+    lu.st2 = st2;
+    lu.ev_a = ev_fork;
+    lu.ev_b = ev_join;
   }
 
   void init(cudaStream_t s, int n_, int bs_, const std::vector<int>& pstart, const std::vector<int>& psize,
@@ -285,6 +365,12 @@ class WideBand {
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
     if (cublas_ws.size() == 0) cublas_ws.alloc((size_t)64 << 20);
     cublas_check(cublasSetWorkspace(h, cublas_ws.get(), cublas_ws.size()), "cublasSetWorkspace");
+    if (!h2) {
+      cublas_check(cublasCreate(&h2), "cublasCreate");
+      cublas_check(cublasSetStream(h2, st2), "cublasSetStream");
+      cublas_ws2.alloc((size_t)32 << 20);
+      cublas_check(cublasSetWorkspace(h2, cublas_ws2.get(), cublas_ws2.size()), "cublasSetWorkspace");
+    }
     spike = false;
     math_mode(tf32);
     int maxsz = 0;
@@ -350,9 +436,11 @@ class WideBand {
     Lw.alloc((size_t)P * BB);
     Uw.alloc((size_t)P * BB);
     Ww.alloc((size_t)P * BB);
+    Rw.alloc((size_t)P * std::max(1LL, BlockLU<T>::rec_ws(bs)));
     flag.alloc(1);
     const long long key = (((long long)P * 65537 + bs) * 65537 + nb) * 4 + (boost ? 2 : 0) + (tf32 ? 1 : 0);
-    if (key != fgraph_key) {
+    if (key != fgraph_key || factor_cut() != fgraph_cut) {
+      fgraph_cut = factor_cut();
       if (fgraph) cudaGraphExecDestroy(fgraph);
       fgraph = nullptr;
       fgraph_key = key;
@@ -404,7 +492,10 @@ class WideBand {
     lu.batch = P;
     lu.boost = boost;
     lu.flag = flag.get();
-    lu.cut = tf32 ? (1 << 30) : 384;
+    lu.cut = factor_cut();
+    lanes(lu);
+    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(bs));
+    lu.rw = Rw.get();
     const Mat<T> D{Dw.get(), bs, BB}, L{Lw.get(), bs, BB}, U{Uw.get(), bs, BB}, Wm{Ww.get(), bs, BB};
     lu.W = Wm;
     for (int i = 0; i < nb; i++) {
@@ -656,6 +747,10 @@ class WideBand {
     lu.boost = boost;
     lu.flag = sflag.get();
     lu.W = Mat<T>{Ws.get(), ldK, sK};
+    lanes(lu);
+    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(K));
+    Rs.alloc((size_t)nI * lu.rws);
+    lu.rw = Rs.get();
     const Mat<T> Sm{S.get(), ldK, sK};
     lu.gemm(K, K, K, T(-1), Mat<T>{Wc.get(), ldK, sK}, Mat<T>{Vc.get(), ldK, sK}, T(1), Sm);
     lu.rec(Sm, Mat<T>{SLi.get(), ldK, sK}, Mat<T>{SUi.get(), ldK, sK}, K);
