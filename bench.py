@@ -42,6 +42,7 @@ WORKLOAD = dict(name="cd2d_m1000_conv0.3_fill2x5000_rowperm_p16_drop1e-4", m=100
 FORMS = {
     "tf32_refine": dict(prec="tf32", solver="BiCGStab2", refinementSweeps=6),
     "tf32_fgmres": dict(prec="tf32", solver="FGMRES", refinementSweeps=0),
+    "tf32f16_fgmres": dict(prec="tf32_f16", solver="FGMRES", refinementSweeps=0),
     "fp64": dict(prec="double", solver="BiCGStab2", refinementSweeps=0),
 }
 HEADLINE = "tf32_fgmres"
@@ -221,10 +222,13 @@ def sweep_bytes(bs: int, nb: int, P: int, vbytes: int) -> int:
     the 4*nb-2 triangles of bs(bs+1)/2 factor values it must read (L_ii^-1,
     U_ii^-1, and the off-diagonal factor blocks, whose other triangle is
     structurally zero), the right-hand side and carry vectors read and the
-    result written, for P partitions."""
+    result written, for P partitions.  vbytes 2: FP16 factor values with FP32
+    vectors and one FP32 column scale per factor column."""
     tri = bs * (bs + 1) // 2
     mats = (4 * nb - 2) * tri
     vecs = (4 * nb - 2) * 2 * bs + (2 * nb - 2) * bs
+    if vbytes == 2:
+        return P * (mats * 2 + vecs * 4 + (4 * nb - 2) * bs * 4)
     return P * (mats + vecs) * vbytes
 
 

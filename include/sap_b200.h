@@ -64,7 +64,7 @@ enum { SAP_LU_UL = 0, SAP_LU_ONLY = 1 };
 enum { SAP_PRECOND_SPIKE = 0, SAP_PRECOND_BLOCK = 1, SAP_PRECOND_NONE = 2 };
 /* Preconditioner value type: the Solver's PrecValueType template argument
  * (sap/solver.h:153). */
-enum { SAP_PREC_FLOAT = 0, SAP_PREC_DOUBLE = 1, SAP_PREC_TF32 = 2 };
+enum { SAP_PREC_FLOAT = 0, SAP_PREC_DOUBLE = 1, SAP_PREC_TF32 = 2, SAP_PREC_TF32_F16 = 3 };
 
 /* sap::Options (sap/solver.h:52-81); same fields, same defaults
  * (sap/solver.h:233-256).  Booleans are ints (0/1). */
@@ -198,7 +198,10 @@ int sap_blas_dots_noalloc(int n, int nq, const double* const* x, const double* c
 /* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297).  prec_dtype
  * is the preconditioner's PrecValueType: SAP_PREC_FLOAT or SAP_PREC_DOUBLE,
  * or SAP_PREC_TF32 (FP32 storage whose wide-band block products run on the
- * tensor cores in TF32 with FP32 accumulation; narrow bands as FP32). */
+ * tensor cores in TF32 with FP32 accumulation; narrow bands as FP32), or
+ * SAP_PREC_TF32_F16 (as SAP_PREC_TF32, and the wide-band block sweeps of the
+ * apply read FP16 copies of the factor blocks scaled by a power of two per
+ * column: half the bytes; extensions, no reference counterpart). */
 int sap_solver_create(int num_partitions, const sap_options* opts, int prec_dtype,
                       sap_solver** out);
 int sap_solver_destroy(sap_solver* s);
@@ -244,7 +247,8 @@ int sap_solver_get_reorder(const sap_solver* s, int which, int* out, int64_t* co
 void* sap_solver_stream(const sap_solver* s);
 /* Layout of the wide-band block path after setup: the block size and the
  * number of blocks per partition (both 0 when the narrow band kernels are
- * used), and the bytes of one preconditioner value (4 or 8). */
+ * used), and the bytes of one factor value read by the apply's sweeps (8, 4,
+ * or 2 for the FP16 copies of SAP_PREC_TF32_F16). */
 int sap_solver_block_layout(const sap_solver* s, int* block_size, int* blocks_per_partition, int* value_bytes);
 /* Number of this library's own kernels enqueued since load (all handles). */
 int64_t sap_kernel_launch_count(void);

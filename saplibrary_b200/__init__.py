@@ -271,7 +271,7 @@ def generate_band_host(n: int, k: int, d: float, dist: int = 1, seed: int = 0) -
 
 
 # ---- Options / Stats ------------------------------------------------------------
-_PREC = {"float": 0, "double": 1, "tf32": 2}
+_PREC = {"float": 0, "double": 1, "tf32": 2, "tf32_f16": 3}
 
 
 @dataclass
@@ -496,8 +496,9 @@ class Solver:
         return n.value, k.value, p.value
 
     def blockLayout(self):
-        """(block size, blocks per partition, bytes per preconditioner value) of
-        the wide-band block path; (0, 0, bytes) for the narrow band kernels."""
+        """(block size, blocks per partition, bytes per factor value read by the
+        sweeps) of the wide-band block path; (0, 0, bytes) for the narrow band
+        kernels."""
         bs, nb, vb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(_lib.sap_solver_block_layout(self._h, ctypes.byref(bs), ctypes.byref(nb), ctypes.byref(vb)))
         return bs.value, nb.value, vb.value

@@ -41,6 +41,8 @@ static ProfState g_prof;
 ProfScope::ProfScope(const char* name, cudaStream_t st) {
   std::lock_guard<std::mutex> lk(g_prof.mu);
   if (g_prof.name.empty() || g_prof.name != name) return;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return;
   on = true;
   s = st;
   cudaEventCreate(&a);
@@ -120,6 +122,7 @@ class PrecBase {
   int n = 0, K = 0, P = 1;
   bool spike = false, lu_ul = false;
   bool tf32 = false;  // wide-band block products in TF32 (FP32 storage)
+  bool h16 = false;   // wide-band block sweeps over FP16 block-scaled copies
   int ptype = SAP_PRECOND_SPIKE;
   std::vector<PartDev> parts_h;
   DBuf<PartDev> parts_d;
@@ -243,7 +246,7 @@ class PrecondT : public PrecBase {
     size_t fr = 0, tot = 0;
     SAPB_CUDA(cudaMemGetInfo(&fr, &tot));
     if (wide) fr += wide->bytes_held();  // reused (or released) by the new setup
-    const double need = WideBand<T>::factor_bytes(n, P, kmax);
+    const double need = WideBand<T>::factor_bytes(n, P, kmax, h16 && sizeof(T) == 4);
     if (need > 0.92 * (double)fr)
       throw Error(SAP_ERR_OUT_OF_MEMORY, "wide-band factors need " + std::to_string(need / 1e9) + " GB, " +
                                              std::to_string((double)fr / 1e9) + " GB free");
@@ -271,7 +274,7 @@ class PrecondT : public PrecBase {
       pz[p] = parts_h[p].size;
     }
     if (!wide) wide = std::make_unique<WideBand<T>>();
-    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz, tf32);
+    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz, tf32, h16);
     wide_active = true;
   }
 
@@ -1014,7 +1017,8 @@ class Solver {
     SAPB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     if (dtype == SAP_PREC_DOUBLE) pcp = std::make_unique<PrecondT<double>>();
     else pcp = std::make_unique<PrecondT<float>>();
-    pcp->tf32 = dtype == SAP_PREC_TF32;
+    pcp->tf32 = dtype == SAP_PREC_TF32 || dtype == SAP_PREC_TF32_F16;
+    pcp->h16 = dtype == SAP_PREC_TF32_F16;
     pcp->o = o;
     pcp->P_req = P;
     pcp->st = st;
@@ -1741,7 +1745,8 @@ int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y,
 int sap_solver_create(int P, const sap_options* opts, int prec_dtype, sap_solver** out) {
   SAP_TRY({
     SAP_REQUIRE(out && opts && P >= 1, "invalid solver arguments");
-    SAP_REQUIRE(prec_dtype == SAP_PREC_FLOAT || prec_dtype == SAP_PREC_DOUBLE || prec_dtype == SAP_PREC_TF32,
+    SAP_REQUIRE(prec_dtype == SAP_PREC_FLOAT || prec_dtype == SAP_PREC_DOUBLE || prec_dtype == SAP_PREC_TF32 ||
+                    prec_dtype == SAP_PREC_TF32_F16,
                 "invalid preconditioner type");
     SAP_REQUIRE(opts->refinementSweeps >= 0, "refinementSweeps must be >= 0");
     auto h = std::make_unique<sap_solver>();
@@ -2032,7 +2037,8 @@ int sap_solver_block_layout(const sap_solver* h, int* block_size, int* blocks_pe
     pc.block_layout(bs, nb);
     if (block_size) *block_size = bs;
     if (blocks_per_partition) *blocks_per_partition = nb;
-    if (value_bytes) *value_bytes = h->s->prec_dtype == SAP_PREC_DOUBLE ? 8 : 4;
+    if (value_bytes)
+      *value_bytes = h->s->prec_dtype == SAP_PREC_DOUBLE ? 8 : (h->s->prec_dtype == SAP_PREC_TF32_F16 && bs > 0 ? 2 : 4);
   });
 }
 

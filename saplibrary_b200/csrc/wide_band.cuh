@@ -14,6 +14,8 @@
 // nb*bs rows per partition, padding rows carry an identity diagonal.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <type_traits>
 
 #include "common.cuh"
@@ -113,9 +115,9 @@ __global__ void k_sub_fill(T* __restrict__ dst, int ldd, long long sd, int m, in
 // pivot row j and pivot column j publish them to shared memory (two buffers,
 // so one barrier per step); rows r <= j are skipped per warp.
 template <typename T, int NL, int RY>
-__global__ void __launch_bounds__(RY * 32) k_leaf_lu(const T* __restrict__ M, T* __restrict__ Li, T* __restrict__ Ui,
-                                                     int ld, long long stride, int n, int boost,
-                                                     int* __restrict__ zero_flag) {
+__global__ void __launch_bounds__(RY * 32) k_leaf_lu(const T* __restrict__ M, int ldm, long long sm,
+                                                     T* __restrict__ Li, T* __restrict__ Ui, int ld, long long stride,
+                                                     int n, int boost, int* __restrict__ zero_flag) {
   constexpr int TM = NL / RY, TN = NL / 32, NT = RY * 32, SP = NL + 1;
   static_assert(NL % RY == 0 && NL % 32 == 0, "leaf tiling");
   extern __shared__ __align__(16) unsigned char leaf_smem[];
@@ -125,12 +127,12 @@ __global__ void __launch_bounds__(RY * 32) k_leaf_lu(const T* __restrict__ M, T*
   T* erow = rowj + 2 * NL;                 // [2][NL] pivot row of E
   T* piv = erow + 2 * NL;                  // [NL] pivots as used
   const int t = threadIdx.x, tx = t & 31, ty = t >> 5;
-  const T* Mb = M + blockIdx.x * stride;
+  const T* Mb = M + blockIdx.x * sm;
   T* Lb = Li + blockIdx.x * stride;
   T* Ub = Ui + blockIdx.x * stride;
   for (int idx = t; idx < n * n; idx += NT) {
     const int c = idx / n, r = idx - c * n;
-    S[r * SP + c] = Mb[(long long)c * ld + r];
+    S[r * SP + c] = Mb[(long long)c * ldm + r];
   }
   __syncthreads();
   T g[TM][TN], e[TM][TN];
@@ -280,6 +282,15 @@ __global__ void __launch_bounds__(256) k_bgemv(const T* A, int ld, long long sA,
 // warp) and reduce in shared memory in a fixed order.  Tiles are paired j
 // with (T-1-j) so triangular work is the same for every CTA.  Batch b uses
 // A + b*sA, x + b*sx, c + b*sc, y + b*sy.
+// The matrix may be stored as FP16 (MT = __half, 8 rows per 16-byte load)
+// with a power-of-two scale per column (see k_blocks_to_half): the kernel
+// then reads x_c * cs[b*scs + c] in place of x_c and accumulates in T.
+// Chains of these launches are programmatic dependent launches: every CTA
+// first lets the next launch of its stream be scheduled
+// (griddepcontrol.launch_dependents), then waits for the previous launch to
+// complete with its writes visible (griddepcontrol.wait) before it touches
+// x, c, y or the column-split scratch; the factor blocks it streams are not
+// written by any launch of the apply.
 constexpr int kGemvWarps = 16;
 template <typename T, int VEC>
 struct VecOf;
@@ -287,6 +298,11 @@ template <>
 struct VecOf<double, 2> { using type = double2; };
 template <>
 struct VecOf<float, 4> { using type = float4; };
+template <>
+struct VecOf<__half, 8> { using type = uint4; };
+template <typename T>
+__device__ __forceinline__ T as_acc(T v) { return v; }
+__device__ __forceinline__ float as_acc(__half v) { return __half2float(v); }
 template <typename T>
 __device__ __forceinline__ void vec_fma(const double2& a, T xv, T* acc) {
   acc[0] += a.x * xv;
@@ -299,6 +315,16 @@ __device__ __forceinline__ void vec_fma(const float4& a, T xv, T* acc) {
   acc[2] += a.z * xv;
   acc[3] += a.w * xv;
 }
+template <typename T>
+__device__ __forceinline__ void vec_fma(const uint4& a, T xv, T* acc) {  // 8 x FP16
+  const __half2* h = reinterpret_cast<const __half2*>(&a);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float2 f = __half22float2(h[q]);
+    acc[2 * q] += f.x * xv;
+    acc[2 * q + 1] += f.y * xv;
+  }
+}
 
 //
 // Column split (gridDim.z = S > 1, for grids with few tiles): CTA s takes
@@ -307,10 +333,12 @@ __device__ __forceinline__ void vec_fma(const float4& a, T xv, T* acc) {
 // arrives last at the tile's counter (ctr, zero between launches) adds the S
 // slices in order s = 0..S-1, writes y and resets the counter.  No CTA waits
 // for another.
-template <typename T, int VEC>
-__global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, long long sA, const T* x, long long sx,
+// (three CTAs per SM for the vector forms: 16 warps each, <= 42 registers)
+template <typename T, int VEC, typename MT = T>
+__global__ void __launch_bounds__(kGemvWarps * 32, VEC > 1 ? 3 : 1) k_tgemv(const MT* A, int ld, long long sA, const T* x, long long sx,
                                                            const T* c, long long sc, T* y, long long sy, int n,
-                                                           int mode, int tri, T* ws, unsigned* ctr) {
+                                                           int mode, int tri, T* ws, unsigned* ctr,
+                                                           const T* cs = nullptr, long long scs = 0) {
   constexpr int R = 32 * (VEC > 1 ? VEC : 2);
   __shared__ T part[kGemvWarps][R];
   __shared__ unsigned last_cta;
@@ -318,8 +346,16 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
   const int S = gridDim.z, sl = blockIdx.z;
   const int ntile = (n + R - 1) / R;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const T* Ab = A + b * sA;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const MT* Ab = A + b * sA;
   const T* xb = x + b * sx;
+  const T* csb = cs + b * scs;
+  // x_c, times the column scale for a scaled FP16 matrix
+  auto xs = [&](int col) -> T {
+    if constexpr (std::is_same<MT, T>::value) return xb[col];
+    else return xb[col] * csb[col];
+  };
   for (int half = 0; half < 2; half++) {
     const int tile = half == 0 ? (int)blockIdx.x : ntile - 1 - (int)blockIdx.x;
     if (half == 1 && tile <= (int)blockIdx.x) break;
@@ -337,13 +373,13 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
     constexpr int U = 8;
     constexpr int SW = kGemvWarps;  // column stride of a warp
     if constexpr (VEC > 1) {
-      using V = typename VecOf<T, VEC>::type;
+      using V = typename VecOf<MT, VEC>::type;
       T acc[VEC];
 #pragma unroll
       for (int v = 0; v < VEC; v++) acc[v] = T(0);
       const int r = r0 + VEC * lane;
       const int valid = min(VEC, max(0, n - r));
-      const T* base = Ab + r;
+      const MT* base = Ab + r;
       int col = c0 + w;
       if (valid == VEC) {
         for (; col + (U - 1) * SW < c1; col += U * SW) {
@@ -352,16 +388,16 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
 #pragma unroll
           for (int u = 0; u < U; u++) {
             a[u] = *reinterpret_cast<const V*>(base + (long long)(col + u * SW) * ld);
-            xv[u] = xb[col + u * SW];
+            xv[u] = xs(col + u * SW);
           }
 #pragma unroll
           for (int u = 0; u < U; u++) vec_fma<T>(a[u], xv[u], acc);
         }
-        for (; col < c1; col += SW) vec_fma<T>(*reinterpret_cast<const V*>(base + (long long)col * ld), xb[col], acc);
+        for (; col < c1; col += SW) vec_fma<T>(*reinterpret_cast<const V*>(base + (long long)col * ld), xs(col), acc);
       } else {
         for (; col < c1; col += SW) {
-          const T xv = xb[col];
-          for (int v = 0; v < valid; v++) acc[v] += base[(long long)col * ld + v] * xv;
+          const T xv = xs(col);
+          for (int v = 0; v < valid; v++) acc[v] += as_acc(base[(long long)col * ld + v]) * xv;
         }
       }
 #pragma unroll
@@ -370,17 +406,17 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
       T acc0 = T(0), acc1 = T(0);
       const int ra = r0 + lane, rb = r0 + 32 + lane;
       const bool va = ra < n, vb = rb < n;
-      const T* pa = Ab + (va ? ra : 0);
-      const T* pb = Ab + (vb ? rb : 0);
+      const MT* pa = Ab + (va ? ra : 0);
+      const MT* pb = Ab + (vb ? rb : 0);
       int col = c0 + w;
       for (; col + (U - 1) * SW < c1; col += U * SW) {
         T a0[U], a1[U], xv[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
           const long long o = (long long)(col + u * SW) * ld;
-          a0[u] = va ? pa[o] : T(0);
-          a1[u] = vb ? pb[o] : T(0);
-          xv[u] = xb[col + u * SW];
+          a0[u] = va ? as_acc(pa[o]) : T(0);
+          a1[u] = vb ? as_acc(pb[o]) : T(0);
+          xv[u] = xs(col + u * SW);
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -389,10 +425,10 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
         }
       }
       for (; col < c1; col += SW) {
-        const T xv = xb[col];
+        const T xv = xs(col);
         const long long o = (long long)col * ld;
-        if (va) acc0 += pa[o] * xv;
-        if (vb) acc1 += pb[o] * xv;
+        if (va) acc0 += as_acc(pa[o]) * xv;
+        if (vb) acc1 += as_acc(pb[o]) * xv;
       }
       part[w][lane] = acc0;
       part[w][32 + lane] = acc1;
@@ -436,6 +472,35 @@ __global__ void __launch_bounds__(kGemvWarps * 32) k_tgemv(const T* A, int ld, l
 // rows per tile of k_tgemv<T, VEC>
 template <typename T, int VEC>
 constexpr int tgemv_rows() { return 32 * (VEC > 1 ? VEC : 2); }
+
+// FP16 copies of n x n column-major blocks (block b at A + b*BB) for the
+// apply, as block floating point: column c is stored as A[:, c] * 2^k_c with
+// its largest magnitude in [2^14, 2^15) and cs[b*n + c] = 2^-k_c (a zero
+// column gets scale 1).  Only the rows k_tgemv reads for the block's
+// triangle are written: tri 1 (lower) rows from the start of the R-row tile
+// holding row c, tri 2 (upper) rows up to the end of that tile.  One warp
+// per column.
+template <typename T, int R>
+__global__ void k_blocks_to_half(const T* __restrict__ A, __half* __restrict__ H, T* __restrict__ cs, int n,
+                                 long long BB, int tri) {
+  const int c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (c >= n) return;
+  const long long o = (long long)blockIdx.y * BB + (long long)c * n;
+  const int t0 = (c / R) * R;
+  const int r0 = tri == 1 ? t0 : 0, r1 = tri == 2 ? min(n, t0 + R) : n;
+  float m = 0.f;
+  for (int r = r0 + lane; r < r1; r += 32) m = fmaxf(m, fabsf((float)A[o + r]));
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, d));
+  int e = 0;
+  if (m > 0.f) {
+    frexpf(m, &e);  // m = f * 2^e, f in [0.5, 1)
+    e = max(e, -100);
+  }
+  const float up = m > 0.f ? ldexpf(1.f, 15 - e) : 1.f;
+  for (int r = r0 + lane; r < r1; r += 32) H[o + r] = __float2half_rn((float)A[o + r] * up);
+  if (lane == 0) cs[(long long)blockIdx.y * n + c] = m > 0.f ? (T)ldexpf(1.f, e - 15) : T(1);
+}
 
 // Nonzero columns of the coupling blocks: flag[blk][c] = any row of column c
 // of row-major K x K block blk (blk = 2t + which) is nonzero.

@@ -204,7 +204,7 @@ class BlockLU {
   // level's offset into rw.
   void rec(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n, long long wo = 0) {
     if (n <= kNL) {
-      if (M.s != Li.s || Li.s != Ui.s) throw Error(SAP_ERR_INVALID_ARGUMENT, "leaf strides differ");
+      if (Li.s != Ui.s || Li.ld != Ui.ld) throw Error(SAP_ERR_INVALID_ARGUMENT, "leaf inverse layouts differ");
       using LS = LeafShape<T>;
       static bool smem_set = false;  // first call runs outside any graph capture
       if (!smem_set) {
@@ -212,8 +212,9 @@ class BlockLU {
                                        (int)LS::smem));
         smem_set = true;
       }
-      k_leaf_lu<T, LS::NL, LS::RY><<<batch, LS::RY * 32, LS::smem, st>>>(M.p, Li.p, Ui.p, M.ld, M.s, n, boost ? 1 : 0,
-                                                                          flag);
+      SAPB_PROF("wb_leaf", st);
+      k_leaf_lu<T, LS::NL, LS::RY><<<batch, LS::RY * 32, LS::smem, st>>>(M.p, M.ld, M.s, Li.p, Ui.p, Li.ld, Li.s, n,
+                                                                          boost ? 1 : 0, flag);
       SAPB_LAUNCHED();
       return;
     }
@@ -267,15 +268,17 @@ class WideBand {
   DBuf<int> flag;
   // setup workspaces, kept (with everything above) across setups of the
   // same layout so that a repeated setup does not free and re-allocate
-  DBuf<T> Dw, Lw, Uw, Ww, X, Wt, S, Ws;
+  DBuf<T> Dw, Ww, X, Wt, S, Ws;
   DBuf<T> Rw, Rs;  // recursion workspaces of the partition factors / the reduced system
 
   // device bytes this object holds
   size_t bytes_held() const {
     size_t b = 0;
     for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
-                             &t1, &t2, &Dw, &Lw, &Uw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1]})
+                             &t1, &t2, &Dw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1], &csL, &csU,
+                             &csLo, &csUo})
       b += d->size() * sizeof(T);
+    for (const DBuf<__half>* d : {&Lh, &Uh, &Loh, &Uoh}) b += d->size() * sizeof(__half);
     return b;
   }
 
@@ -299,6 +302,11 @@ class WideBand {
   cudaGraphExec_t fgraph = nullptr;
   long long fgraph_key = -1;
   int fgraph_cut = 0;
+  // SAPB_FACTOR_GRAPH=0 runs the factorization's launches directly every time
+  static bool graph_enabled() {
+    const char* e = std::getenv("SAPB_FACTOR_GRAPH");
+    return !(e && std::atoi(e) == 0);
+  }
   int fgraph_runs = 0;
   bool fgraph_failed = false;
   int64_t fgraph_launches = 0, fgraph_lib_calls = 0;
@@ -308,18 +316,50 @@ class WideBand {
   // Block size bs >= the largest half-bandwidth, a multiple of the leaf size.
   static int block_size(int kmax) { return std::max(kLeaf, ((kmax + kLeaf - 1) / kLeaf) * kLeaf); }
 
-  // Device bytes of the factors and the factorization workspaces for n rows
-  // in P partitions (for the memory check).
-  static double factor_bytes(int n, int P, int kmax) {
+  // Device bytes of the factors, their FP16 copies (h16) and the
+  // factorization workspaces for n rows in P partitions (for the memory check).
+  static double factor_bytes(int n, int P, int kmax, bool h16 = false) {
     const double b = block_size(kmax);
     const double nbp = std::ceil((double)(n / P + 1) / b);
-    return (4.0 * nbp + 5.0) * P * b * b * sizeof(T);
+    return ((4.0 * nbp + 3.0) * sizeof(T) + (h16 ? 4.0 * nbp * 2.0 : 0.0)) * P * b * b;
   }
 
   // tf32: FP32 block products on the tensor cores (TF32 inputs, FP32
   // accumulation) for the partition factors and spikes; the reduced system
   // keeps full FP32 products.
   bool tf32 = false;
+  // h16: the block sweeps of the apply read FP16 copies of the factor
+  // blocks with a power-of-two scale per column (half the bytes of FP32);
+  // the setup keeps computing in FP32 / TF32.  FP32 storage only.
+  bool h16 = false;
+  DBuf<__half> Lh, Uh, Loh, Uoh;   // copies of Linv, Uinv, Loff, Uoff
+  DBuf<T> csL, csU, csLo, csUo;    // their column scales ([block][bs])
+  void make_half() {
+    if (!h16) return;
+    const long long nd = (long long)P * nb, no = (long long)P * (nb - 1);
+    Lh.alloc((size_t)(nd * BB));
+    Uh.alloc((size_t)(nd * BB));
+    csL.alloc((size_t)(nd * bs));
+    csU.alloc((size_t)(nd * bs));
+    if (nb > 1) {
+      Loh.alloc((size_t)(no * BB));
+      Uoh.alloc((size_t)(no * BB));
+      csLo.alloc((size_t)(no * bs));
+      csUo.alloc((size_t)(no * bs));
+    }
+    constexpr int R = tgemv_rows<T, 8>();  // rows per tile of the FP16 sweep kernel
+    auto conv = [&](const T* A, __half* H, T* cs, long long nblk, int tri) {
+      if (nblk <= 0) return;
+      k_blocks_to_half<T, R><<<dim3((bs + 7) / 8, (unsigned)nblk), 256, 0, st>>>(A, H, cs, bs, BB, tri);
+      SAPB_LAUNCHED();
+    };
+    conv(Linv.get(), Lh.get(), csL.get(), nd, 1);
+    conv(Uinv.get(), Uh.get(), csU.get(), nd, 2);
+    if (nb > 1) {
+      conv(Loff.get(), Loh.get(), csLo.get(), no, 2);
+      conv(Uoff.get(), Uoh.get(), csUo.get(), no, 1);
+    }
+  }
   // recursion cut-off of the spike slab products: structure-aware for the
   // compute-bound FP64 / FP32 products (FP64 spikes 0.99 -> 0.62 s on the
   // 1M-row workload), plain GEMMs for TF32; SAPB_SPIKE_CUT overrides
@@ -348,9 +388,10 @@ class WideBand {
   }
 
   void init(cudaStream_t s, int n_, int bs_, const std::vector<int>& pstart, const std::vector<int>& psize,
-            bool tf32_ = false) {
+            bool tf32_ = false, bool h16_ = false) {
     st = s;
     tf32 = tf32_ && sizeof(T) == 4;
+    h16 = h16_ && sizeof(T) == 4;
     n = n_;
     P = (int)pstart.size();
     bs = bs_;
@@ -433,8 +474,6 @@ class WideBand {
   //   U_{i,i+1} = L_ii^-1 E_i;  L_{i+1,i} = F_i U_ii^-1.
   void factor(bool boost) {
     Dw.alloc((size_t)P * BB);
-    Lw.alloc((size_t)P * BB);
-    Uw.alloc((size_t)P * BB);
     Ww.alloc((size_t)P * BB);
     Rw.alloc((size_t)P * std::max(1LL, BlockLU<T>::rec_ws(bs)));
     flag.alloc(1);
@@ -450,7 +489,7 @@ class WideBand {
       SAPB_CUDA(cudaGraphLaunch(fgraph, st));
       count_launch((int)fgraph_launches);
       g_lib_calls.fetch_add(fgraph_lib_calls, std::memory_order_relaxed);
-    } else if (fgraph_runs >= 1 && !fgraph_failed) {
+    } else if (fgraph_runs >= 1 && !fgraph_failed && graph_enabled()) {
       const int64_t l0 = g_launches.load(), c0 = g_lib_calls.load();
       cudaGraph_t g = nullptr;
       bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
@@ -482,6 +521,7 @@ class WideBand {
     SAPB_CUDA(cudaMemcpyAsync(&hf, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     SAPB_CUDA(cudaStreamSynchronize(st));
     if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
+    make_half();
   }
 
   void enqueue_factor(bool boost) {
@@ -496,27 +536,41 @@ class WideBand {
     lanes(lu);
     lu.rws = std::max(1LL, BlockLU<T>::rec_ws(bs));
     lu.rw = Rw.get();
-    const Mat<T> D{Dw.get(), bs, BB}, L{Lw.get(), bs, BB}, U{Uw.get(), bs, BB}, Wm{Ww.get(), bs, BB};
+    const Mat<T> D{Dw.get(), bs, BB}, Wm{Ww.get(), bs, BB};
     lu.W = Wm;
     for (int i = 0; i < nb; i++) {
-      lu.copy(blk(Linv, nb, i), D, bs, bs);
-      // D_i -= L_{i,i-1} U_{i-1,i}: upper times lower
-      if (i > 0) lu.prod_UL_acc(bs, T(-1), blk(Loff, nb - 1, i - 1), blk(Uoff, nb - 1, i - 1), D);
-      Lw.zero(st);
-      Uw.zero(st);
-      lu.rec(D, L, U, bs);
-      lu.copy(L, blk(Linv, nb, i), bs, bs);
-      lu.copy(U, blk(Uinv, nb, i), bs, bs);
+      const Mat<T> Li = blk(Linv, nb, i), Ui = blk(Uinv, nb, i);
+      {
+        SAPB_PROF("wb_copy", st);
+        lu.copy(Li, D, bs, bs);  // D_i (loaded into the L_ii^-1 slot)
+        lu.fill(Li, bs, bs, T(0));
+        lu.fill(Ui, bs, bs, T(0));
+      }
+      if (i > 0) {  // D_i -= L_{i,i-1} U_{i-1,i}: upper times lower
+        SAPB_PROF("wb_schur", st);
+        lu.prod_UL_acc(bs, T(-1), blk(Loff, nb - 1, i - 1), blk(Uoff, nb - 1, i - 1), D);
+      }
+      {
+        SAPB_PROF("wb_rec", st);
+        lu.rec(D, Li, Ui, bs);
+      }
       if (i < nb - 1) {
         // U_{i,i+1} = L_ii^-1 E_i (lower times lower: E_i has no entries above
-        // its diagonal), L_{i+1,i} = F_i U_ii^-1 (upper times upper)
-        lu.prod_LL(bs, T(1), L, blk(Uoff, nb - 1, i), Wm);
+        // its diagonal) and, on the second lane, L_{i+1,i} = F_i U_ii^-1
+        // (upper times upper); D is free again as the second lane's scratch
+        SAPB_PROF("wb_offdiag", st);
+        lu.fork();
+        lu.prod_LL(bs, T(1), Li, blk(Uoff, nb - 1, i), Wm);
         lu.copy(Wm, blk(Uoff, nb - 1, i), bs, bs);
-        lu.prod_UU(bs, T(1), blk(Loff, nb - 1, i), U, Wm);
-        lu.copy(Wm, blk(Loff, nb - 1, i), bs, bs);
+        lu.lane2([&] {
+          lu.prod_UU(bs, T(1), blk(Loff, nb - 1, i), Ui, D);
+          lu.copy(D, blk(Loff, nb - 1, i), bs, bs);
+        });
+        lu.join();
       }
     }
   }
+
 
   // tri: 0 full, 1 lower, 2 upper (see k_tgemv).  Grids with fewer than
   // about 2.5 CTAs per SM split the columns over gridDim.z CTAs.
@@ -528,16 +582,24 @@ class WideBand {
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t lane_stream(int lane) const { return lane ? st2 : st; }
-  template <int V>
-  void gemv_launch(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y,
-                   long long sy, int m, int nbatch, int mode, int tri, int lane) {
+  // CTAs one GEMV launch aims at through its column split (about 2.5 of the
+  // three resident CTAs per SM); SAPB_GEMV_CTAS overrides
+  static int gemv_ctas() {
+    const char* e = std::getenv("SAPB_GEMV_CTAS");
+    return (e && std::atoi(e) > 0) ? std::atoi(e) : 370;
+  }
+  template <int V, typename MT = T>
+  void gemv_launch(const MT* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y,
+                   long long sy, int m, int nbatch, int mode, int tri, int lane, const T* cs = nullptr,
+                   long long scs = 0) {
     cudaStream_t ls = lane_stream(lane);
     DBuf<T>& ws_ = gws[lane];
     DBuf<unsigned>& ct = gctr[lane];
     constexpr int R = tgemv_rows<T, V>();
     const int ntile = (m + R - 1) / R, pairs = (ntile + 1) / 2;
     const long long base = (long long)pairs * nbatch;
-    int S = (int)std::min<long long>(8, (370 + base - 1) / base);
+    const long long target = gemv_ctas();
+    int S = (int)std::min<long long>(8, (target + base - 1) / base);
     S = std::max(1, std::min(S, m / 256));
     if (S > 1) {
       const size_t need = (size_t)nbatch * ntile * S * R, nctr = (size_t)nbatch * ntile;
@@ -548,8 +610,20 @@ class WideBand {
         ct.zero(ls);
       }
     }
-    k_tgemv<T, V><<<dim3(pairs, nbatch, S), kGemvWarps * 32, 0, ls>>>(A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri,
-                                                                     ws_.get(), ct.get());
+    // programmatic dependent launch (the kernel waits for its predecessor
+    // on the device, see k_tgemv)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pairs, nbatch, S);
+    cfg.blockDim = dim3(kGemvWarps * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ls;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SAPB_CUDA(cudaLaunchKernelEx(&cfg, k_tgemv<T, V, MT>, A, ld, sA, x, sx, c, sc, y, sy, m, mode, tri, ws_.get(),
+                                 ct.get(), cs, scs));
     SAPB_LAUNCHED();
   }
   void gemv(const T* A, int ld, long long sA, const T* x, long long sx, const T* c, long long sc, T* y, long long sy,
@@ -558,6 +632,17 @@ class WideBand {
     const bool vec = ld % V == 0 && sA % V == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
     if (vec) gemv_launch<V>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane);
     else gemv_launch<1>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane);
+  }
+  // the same with an FP16 block-scaled matrix (column scales cs, batch stride scs)
+  void gemv(const __half* A, const T* cs, long long scs, int ld, long long sA, const T* x, long long sx, const T* c,
+            long long sc, T* y, long long sy, int m, int nbatch, int mode, int tri, int lane = 0) {
+    if constexpr (sizeof(T) == 4) {
+      const bool vec = ld % 8 == 0 && sA % 8 == 0 && (reinterpret_cast<uintptr_t>(A) % 16) == 0;
+      if (vec) gemv_launch<8, __half>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane, cs, scs);
+      else gemv_launch<1, __half>(A, ld, sA, x, sx, c, sc, y, sy, m, nbatch, mode, tri, lane, cs, scs);
+    } else {
+      throw Error(SAP_ERR_INVALID_ARGUMENT, "FP16 block storage needs an FP32 preconditioner");
+    }
   }
 
   // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
@@ -584,6 +669,7 @@ class WideBand {
 
   // the block sweeps of partitions [p0, p0+np) on one lane
   void solve_blocks_part(T* x, T* y, T* t, int p0, int np, int lane) {
+    if (h16) return solve_blocks_part_h16(x, y, t, p0, np, lane);
     const long long sv = plen;
     const long long od = (long long)p0 * nb * BB, oo = (long long)p0 * (nb - 1) * BB;
     for (int i = 0; i < nb; i++) {  // y_i = L_ii^-1 (x_i - L_{i,i-1} y_{i-1})
@@ -607,6 +693,35 @@ class WideBand {
            bs, np, 0, 2, lane);
     }
   }
+  // the same sweeps over the FP16 copies
+  void solve_blocks_part_h16(T* x, T* y, T* t, int p0, int np, int lane) {
+    const long long sv = plen;
+    const long long od = (long long)p0 * nb * BB, oo = (long long)p0 * (nb - 1) * BB;
+    const long long cd = (long long)p0 * nb * bs, co = (long long)p0 * (nb - 1) * bs;
+    const long long sd = (long long)nb * BB, so = (long long)(nb - 1) * BB;
+    const long long csd = (long long)nb * bs, cso = (long long)(nb - 1) * bs;
+    for (int i = 0; i < nb; i++) {
+      const T* rhs = x + (long long)i * bs;
+      if (i > 0) {
+        gemv(Loh.get() + oo + (long long)(i - 1) * BB, csLo.get() + co + (long long)(i - 1) * bs, cso, bs, so,
+             y + (long long)(i - 1) * bs, sv, x + (long long)i * bs, sv, t, sv, bs, np, 1, 2, lane);
+        rhs = t;
+      }
+      gemv(Lh.get() + od + (long long)i * BB, csL.get() + cd + (long long)i * bs, csd, bs, sd, rhs, sv, nullptr, 0,
+           y + (long long)i * bs, sv, bs, np, 0, 1, lane);
+    }
+    for (int i = nb - 1; i >= 0; i--) {
+      const T* rhs = y + (long long)i * bs;
+      if (i < nb - 1) {
+        gemv(Uoh.get() + oo + (long long)i * BB, csUo.get() + co + (long long)i * bs, cso, bs, so,
+             x + (long long)(i + 1) * bs, sv, y + (long long)i * bs, sv, t, sv, bs, np, 1, 1, lane);
+        rhs = t;
+      }
+      gemv(Uh.get() + od + (long long)i * BB, csU.get() + cd + (long long)i * bs, csd, bs, sd, rhs, sv, nullptr, 0,
+           x + (long long)i * bs, sv, bs, np, 0, 2, lane);
+    }
+  }
+
 
   // Interface positions inside the partitions' block vectors: pos[t][k] for
   // the bottom (which 0, partition t) or top (which 1, partition t+1) unknowns.

@@ -115,7 +115,7 @@ def test_tf32_banded_refinement():
     assert np.linalg.norm(x - 1.0) / np.sqrt(n) <= 1e-8
 
 
-@pytest.mark.parametrize("prec", ["double", "tf32"])
+@pytest.mark.parametrize("prec", ["double", "tf32", "tf32_f16"])
 def test_fgmres_reaches_fp64_tolerance(prec):
     # flexible GMRES keeps the preconditioned directions, so a low-precision
     # preconditioner needs no refinement restarts
@@ -197,3 +197,45 @@ def test_narrow_var_band_forced(monkeypatch):
     s.precond(vd, zd)
     zo = o.apply(x)
     assert np.linalg.norm(zd.cpu().numpy() - zo) / np.linalg.norm(zo) <= 1e-10
+
+
+@pytest.mark.parametrize("n,K,P,fact", [(20000, 300, 4, sap.LU_UL), (24011, 257, 5, sap.LU_only),
+                                        (6600, 1100, 2, sap.LU_UL)])
+def test_f16_block_storage_apply(n, K, P, fact):
+    # the FP16 block-scaled copies change only the storage of the factor
+    # blocks read by the sweeps: the apply stays within the FP16 rounding of
+    # the same TF32 factors, and both stay near the FP32 oracle's apply
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=n + K)
+    A = sap.BandedMatrix.from_array(band, n, K)
+    s32 = sap.Solver(P, sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False, factMethod=fact),
+                     prec="tf32")
+    s16 = sap.Solver(P, sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False, factMethod=fact),
+                     prec="tf32_f16")
+    s32.setup(A)
+    s16.setup(A)
+    assert s16.blockLayout()[:2] == s32.blockLayout()[:2] and s32.blockLayout()[0] > 0
+    assert s16.blockLayout()[2] == 2
+    o = oracle.Precond(P, fact=fact, ptype=sap.Spike, dtype="float")
+    assert o.setup_banded(band, n, K) == 0
+    rng = np.random.default_rng(K)
+    for _ in range(2):
+        v = rng.standard_normal(n)
+        z32, z16, zo = apply_gpu(s32, v), apply_gpu(s16, v), o.apply(v)
+        assert np.all(np.isfinite(z16))
+        assert np.linalg.norm(z16 - z32) / np.linalg.norm(z32) <= 5e-3
+        assert np.linalg.norm(z16 - zo) / np.linalg.norm(zo) <= 3e-2
+
+
+def test_f16_block_storage_fgmres_banded():
+    n, K, P = 40000, 300, 8
+    band = sap.generate_band_host(n, K, 1.0, 1, seed=12)
+    b = oracle.spmv_banded(band, n, K, np.ones(n))
+    A = sap.BandedMatrix.from_array(band, n, K)
+    opts = sap.Options(solverType=sap.FGMRES, performReorder=False, variableBandwidth=False, applyScaling=False,
+                       factMethod=sap.LU_UL, relTol=1e-10, maxNumIterations=200)
+    s = sap.Solver(P, opts, prec="tf32_f16")
+    s.setup(A)
+    x = np.zeros(n)
+    assert s.solve(sap.MVBanded(A), b, x)
+    assert s.getStats().relResidualNorm <= 1e-10
+    assert np.linalg.norm(x - 1.0) / np.sqrt(n) <= 1e-8
