@@ -40,13 +40,15 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(name="cd2d_m1000_conv0.3_fill2x5000_rowperm_p16_drop1e-4", m=1000, conv=0.3, fill_per_row=2,
                 fill_reach=5000, fill_mag=0.1, P=16, drop=1e-4, relTol=1e-10, maxit=100)
 FORMS = {
-    "tf32_refine": dict(prec="tf32", solver="BiCGStab2", refinementSweeps=6),
-    "tf32_fgmres": dict(prec="tf32", solver="FGMRES", refinementSweeps=0),
-    "tf32f16_fgmres": dict(prec="tf32_f16", solver="FGMRES", refinementSweeps=0),
-    "fp64": dict(prec="double", solver="BiCGStab2", refinementSweeps=0),
+    "tf32_refine": dict(prec="tf32", solver="BiCGStab2", refinementSweeps=6,
+                        dtype="f64 Krylov / tf32 factor, f32 sweeps"),
+    "tf32_fgmres": dict(prec="tf32", solver="FGMRES", refinementSweeps=0, dtype="f64 Krylov / tf32 factor, f32 sweeps"),
+    "tf32f16_fgmres": dict(prec="tf32_f16", solver="FGMRES", refinementSweeps=0,
+                           dtype="f64 Krylov / tf32 factor, f16 block-scaled sweeps"),
+    "fp64": dict(prec="double", solver="BiCGStab2", refinementSweeps=0, dtype="f64"),
 }
-HEADLINE = "tf32_fgmres"
-DEFAULT_FORMS = "tf32_fgmres,fp64"
+HEADLINE = "tf32f16_fgmres"
+DEFAULT_FORMS = "tf32f16_fgmres,tf32_fgmres,fp64"
 # rows of the CPU band-LU timing sample (about 5 s at K ~ 3000)
 LU_SAMPLE_ROWS = 400
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) over the
@@ -383,7 +385,7 @@ def main():
     line = {
         "metric": "time_to_solution", "value": head["tts_s"], "unit": "s", "n_gpus": ws, "steps": args.steps,
         "warmup": warm, "ms_per_step": head["tts_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 Krylov / tf32-f32 preconditioner", "data": "synthetic",
+        "vs_baseline": None, "dtype": FORMS[HEADLINE]["dtype"], "data": "synthetic",
         "config": {"workload": w["name"], "form": HEADLINE, "krylov": "flexible GMRES(50), FP64 Arnoldi",
                    "rel_tol": w["relTol"], "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (CSR 84 MB, factors tens of GB)"},

@@ -70,6 +70,16 @@ class DBuf {
     n_ = n;
     if (n) SAPB_CUDA(cudaMalloc(&p_, n * sizeof(T)));
   }
+  // grow-only: at least n elements (a smaller request keeps the buffer)
+  void ensure(size_t n) {
+    if (n > n_ || !p_) alloc(n);
+  }
+  // ensure(n) and copy n host elements to the front
+  void put(const T* h, size_t n, cudaStream_t s) {
+    ensure(n);
+    if (n) SAPB_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void put(const std::vector<T>& h, cudaStream_t s) { put(h.data(), h.size(), s); }
   void zero(cudaStream_t s) {
     if (n_) SAPB_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
   }
@@ -94,6 +104,33 @@ class DBuf {
   void swap(DBuf& o) { std::swap(p_, o.p_); std::swap(n_, o.n_); }
   T* p_ = nullptr;
   size_t n_ = 0;
+};
+
+// Page-locked host buffer (grow-only) for device->host copies at full speed.
+template <typename T>
+class PinnedBuf {
+ public:
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() {
+    if (p_) cudaFreeHost(p_);
+  }
+  T* reserve(size_t n) {
+    if (n > cap_ || !p_) {
+      if (p_) cudaFreeHost(p_);
+      p_ = nullptr;
+      cap_ = 0;
+      SAPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p_), (n ? n : 1) * sizeof(T)));
+      cap_ = n;
+    }
+    return p_;
+  }
+  T* get() const { return p_; }
+
+ private:
+  T* p_ = nullptr;
+  size_t cap_ = 0;
 };
 
 // --- asynchronous global->shared copies (sm_80+ cp.async) ---------------------

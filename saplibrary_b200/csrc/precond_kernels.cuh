@@ -656,15 +656,18 @@ k_reduced_apply(const PartDev* __restrict__ parts, const T* __restrict__ V, cons
 // DB edge weights on the device, as the reference computes them
 // (get_csc_matrix + getResidualValues, graph.h:1827-1857, db.cuh:14-37):
 // w[e] = log(max_row |a| / |a_e|) in double, one warp per row.
+// (as_float: the values are first rounded to FP32, the preconditioner's
+// value type, as the host copy the reordering runs on)
 __global__ void k_db_weights(const int* __restrict__ rp, const double* __restrict__ a, double* __restrict__ w,
-                             double* __restrict__ rowmax, int n) {
+                             double* __restrict__ rowmax, int n, int as_float) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  auto val = [&](int e) { return as_float ? (double)(float)a[e] : a[e]; };
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     double m = 0.0;
-    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) m = fmax(m, fabs(a[e]));
+    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) m = fmax(m, fabs(val(e)));
     for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
-    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) w[e] = log(m / fabs(a[e]));
+    for (int e = rp[i] + lane; e < rp[i + 1]; e += 32) w[e] = log(m / fabs(val(e)));
     if (lane == 0) rowmax[i] = m;
   }
 }

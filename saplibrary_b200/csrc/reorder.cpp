@@ -93,7 +93,7 @@ int partition_of(int r, int q, int rem) {
 // DB (graph.h:1214-1361): maximum-product matching of rows to columns by
 // shortest augmenting paths, with row/column scaling from its dual values.
 template <typename T>
-void Pipeline<T>::db(const std::vector<double>& weight, const std::vector<double>& rowmax) {
+void Pipeline<T>::db(const double* weight, const double* rowmax) {
   // weight[e] = log(rowmax[row] / |a_e|), computed on the device
   const std::vector<int>& Rp = in_rp;
   const std::vector<int>& Ci = in_ci;
@@ -884,7 +884,7 @@ void Pipeline<T>::assemble_var_band(int P) {
 // The whole sparse setup of transformToBandedMatrix (precond.h:1656-2101)
 // up to the band layout.
 template <typename T>
-void Pipeline<T>::run(const std::vector<double>& weight, const std::vector<double>& rowmax) {
+void Pipeline<T>::run(const double* weight, const double* rowmax) {
   stage_ms.clear();
   auto t0 = std::chrono::steady_clock::now();
   auto lap = [&](const char* name) {

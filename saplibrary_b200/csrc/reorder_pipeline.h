@@ -72,10 +72,10 @@ class Pipeline {
   }
 
   // weight[e] = log(rowmax[row(e)] / |a_e|) and rowmax, both from the device
-  void run(const std::vector<double>& weight, const std::vector<double>& rowmax);
+  void run(const double* weight, const double* rowmax);
 
  private:
-  void db(const std::vector<double>& weight, const std::vector<double>& rowmax);
+  void db(const double* weight, const double* rowmax);
   int rcm();
   int drop_off(T frac, int max_bw);
   void assemble_coupling(int K, int P);

@@ -432,26 +432,39 @@ class PrecondT : public PrecBase {
       }
     }
     pl.nnz = (int)pl.in_ci.size();
-    std::vector<double>& w = db_w;
-    std::vector<double>& rmax = db_rmax;
-    w.clear();
-    rmax.clear();
+    const double* w = nullptr;
+    const double* rmax = nullptr;
     if (pl.do_db) {
+      // weights from the matrix's device copy when no explicit zero was
+      // removed (same entries in the same order), else from an upload of the
+      // filtered host matrix; read back into page-locked buffers
+      const bool same = pl.nnz == A.nnz;
       DBuf<int> drp;
-      DBuf<double> da, dw, dmax;
-      std::vector<double>& av = db_av;
-      av.resize(pl.in_val.size());
+      DBuf<double> da;
+      const int* rpd = A.rp.get();
+      const double* ad = A.v.get();
+      if (!same) {
+        std::vector<double>& av = db_av;
+        av.resize(pl.in_val.size());
 #pragma omp parallel for schedule(static, 65536)
-      for (long long e = 0; e < (long long)av.size(); e++) av[e] = (double)pl.in_val[e];
-      drp.upload(pl.in_rp, st);
-      da.upload(av, st);
-      dw.alloc(av.size());
-      dmax.alloc(n);
-      k_db_weights<<<grid_for((long long)n * 32, 256, 148 * 32), 256, 0, st>>>(drp.get(), da.get(), dw.get(), dmax.get(), n);
+        for (long long e = 0; e < (long long)av.size(); e++) av[e] = (double)pl.in_val[e];
+        drp.upload(pl.in_rp, st);
+        da.upload(av, st);
+        rpd = drp.get();
+        ad = da.get();
+      }
+      db_wd.alloc(pl.in_val.size());
+      db_md.alloc(n);
+      k_db_weights<<<grid_for((long long)n * 32, 256, 148 * 32), 256, 0, st>>>(
+          rpd, ad, db_wd.get(), db_md.get(), n, (same && sizeof(T) == 4) ? 1 : 0);
       SAPB_LAUNCHED();
-      dw.download(w, st);
-      dmax.download(rmax, st);
+      double* wh = db_wh.reserve(pl.in_val.size());
+      double* mh = db_mh.reserve(n);
+      SAPB_CUDA(cudaMemcpyAsync(wh, db_wd.get(), pl.in_val.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      SAPB_CUDA(cudaMemcpyAsync(mh, db_md.get(), (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
       SAPB_CUDA(cudaStreamSynchronize(st));
+      w = wh;
+      rmax = mh;
     }
     t_transfer = ms_since(t0);
     auto t1 = Clock::now();
@@ -477,13 +490,12 @@ class PrecondT : public PrecBase {
     {
       std::vector<int> gin(n), sout(n);
       std::vector<T> sn(n), cn(n);
+#pragma omp parallel for schedule(static, 4096)
       for (int q = 0; q < n; q++) {
         gin[pl.final_pos[q]] = q;
         sn[pl.final_pos[q]] = pl.scale ? (T)pl.row_scale[q] : T(1);
-      }
-      for (int k = 0; k < n; k++) {
-        sout[k] = pl.final_order[k];
-        cn[k] = pl.scale ? (T)pl.col_scale[pl.final_order[k]] : T(1);
+        sout[q] = pl.final_order[q];
+        cn[q] = pl.scale ? (T)pl.col_scale[pl.final_order[q]] : T(1);
       }
       gin_d.upload(gin, st);
       sout_d.upload(sout, st);
@@ -540,18 +552,38 @@ class PrecondT : public PrecBase {
   long long boff_total = 0;
   // host state kept across setups (its memory is reused, not re-faulted)
   std::unique_ptr<rp::Pipeline<T>> pipe;
-  std::vector<double> db_w, db_rmax, db_av;
-  std::vector<int> coo_rows;
+  std::vector<double> db_av;
+  DBuf<double> db_wd, db_md;          // DB weights and row maxima on the device
+  PinnedBuf<double> db_wh, db_mh;     // and their page-locked host copies
+  PinnedBuf<int> coo_pin;  // staging of the COO uploads
 
   // device COO (band rows, columns, values) of a CSR in band order
+  // (through a page-locked staging buffer: rows, columns and values are
+  // packed into it in parallel, then copied in one transfer each)
   void upload_coo(const std::vector<int>& rp_, const std::vector<int>& ci_, const std::vector<T>& v_) {
-    std::vector<int>& rows = coo_rows;
-    rows.resize(ci_.size());
+    const size_t m = ci_.size();
+    const size_t words = 2 * m + (m * sizeof(T) + sizeof(int) - 1) / sizeof(int);
+    int* pin = coo_pin.reserve(words);
+    int* prow = pin;
+    int* pcol = pin + m;
+    T* pval = reinterpret_cast<T*>(pin + 2 * m);
+#pragma omp parallel for schedule(static, 4096)
     for (int i = 0; i < n; i++)
-      for (int e = rp_[i]; e < rp_[i + 1]; e++) rows[e] = i;
-    co_row.upload(rows, st);
-    co_col.upload(ci_, st);
-    co_val.upload(v_, st);
+      for (int e = rp_[i]; e < rp_[i + 1]; e++) {
+        prow[e] = i;
+        pcol[e] = ci_[e];
+        pval[e] = v_[e];
+      }
+    co_row.alloc(m);
+    co_col.alloc(m);
+    co_val.alloc(m);
+    if (m) {
+      SAPB_CUDA(cudaMemcpyAsync(co_row.get(), prow, m * sizeof(int), cudaMemcpyHostToDevice, st));
+      SAPB_CUDA(cudaMemcpyAsync(co_col.get(), pcol, m * sizeof(int), cudaMemcpyHostToDevice, st));
+      SAPB_CUDA(cudaMemcpyAsync(co_val.get(), pval, m * sizeof(T), cudaMemcpyHostToDevice, st));
+    }
+    // the staging buffer is reused by the next upload: finish these first
+    SAPB_CUDA(cudaStreamSynchronize(st));
   }
 
   // update() maps: every input entry located in the setup's numeric inputs

@@ -16,6 +16,7 @@
 
 #include <cuda_fp16.h>
 
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -230,14 +231,23 @@ __global__ void __launch_bounds__(RY * 32) k_leaf_lu(const T* __restrict__ M, in
   }
 }
 
-// Leaf size and CTA rows of k_leaf_lu per value type (register budget:
-// 2 * TM * TN values per thread).
-template <typename T>
+// CTA rows (warps) and shared memory of k_leaf_lu for a leaf of NL
+// (register budget: 2 * TM * TN values per thread).
+template <typename T, int NL>
 struct LeafShape {
-  static constexpr int NL = sizeof(T) == 4 ? 128 : 64;
-  static constexpr int RY = 16;
+  static constexpr int RY = NL >= 64 ? 16 : 8;
   static constexpr size_t smem = (size_t)(NL * (NL + 1) + 7 * NL) * sizeof(T);
 };
+// Largest leaf: 32 (measured on the 1M-row workload's 3168 / 3040 blocks:
+// TF32 block LU 190 ms with 32, 192 with 64, 215 with 128; FP64 1029 / 1040
+// with 32 / 64); SAPB_LEAF = 64 / 128 (128 for FP32 only) overrides.
+template <typename T>
+inline int leaf_size() {
+  const char* e = std::getenv("SAPB_LEAF");
+  const int v = e ? std::atoi(e) : 0;
+  if (v == 32 || v == 64 || (v == 128 && sizeof(T) == 4)) return v;
+  return 32;
+}
 
 // Batched dense matrix-vector product with an n x n column-major block:
 //   y = A x            (mode 0)

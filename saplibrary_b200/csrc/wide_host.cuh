@@ -192,30 +192,36 @@ class BlockLU {
     if (n1 >= n) n1 = n - kLeaf;
     return n1;
   }
-  static constexpr int kNL = LeafShape<T>::NL;  // largest leaf of the recursion
-  static long long rec_ws(int n) {
-    if (n <= kNL) return 0;
+  int leaf = leaf_size<T>();  // largest leaf of the recursion
+  static long long rec_ws(int n, int leaf) {
+    if (n <= leaf) return 0;
     const int n1 = split(n), n2 = n - n1;
-    return std::max(rec_ws(n1), 2LL * n1 * n2 + rec_ws(n2));
+    return std::max(rec_ws(n1, leaf), 2LL * n1 * n2 + rec_ws(n2, leaf));
+  }
+  template <int NL>
+  void leaf_launch(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n) {
+    using LS = LeafShape<T, NL>;
+    static bool smem_set = false;  // first call runs outside any graph capture
+    if (!smem_set) {
+      SAPB_CUDA(cudaFuncSetAttribute(k_leaf_lu<T, NL, LS::RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)LS::smem));
+      smem_set = true;
+    }
+    SAPB_PROF("wb_leaf", st);
+    k_leaf_lu<T, NL, LS::RY><<<batch, LS::RY * 32, LS::smem, st>>>(M.p, M.ld, M.s, Li.p, Ui.p, Li.ld, Li.s, n,
+                                                                    boost ? 1 : 0, flag);
+    SAPB_LAUNCHED();
   }
 
   // Li = L^-1, Ui = U^-1 of M = L U (n x n at M; Li, Ui pre-zeroed).  M's
   // trailing blocks are overwritten by the Schur complements.  wo: this
   // level's offset into rw.
   void rec(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n, long long wo = 0) {
-    if (n <= kNL) {
+    if (n <= leaf) {
       if (Li.s != Ui.s || Li.ld != Ui.ld) throw Error(SAP_ERR_INVALID_ARGUMENT, "leaf inverse layouts differ");
-      using LS = LeafShape<T>;
-      static bool smem_set = false;  // first call runs outside any graph capture
-      if (!smem_set) {
-        SAPB_CUDA(cudaFuncSetAttribute(k_leaf_lu<T, LS::NL, LS::RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)LS::smem));
-        smem_set = true;
-      }
-      SAPB_PROF("wb_leaf", st);
-      k_leaf_lu<T, LS::NL, LS::RY><<<batch, LS::RY * 32, LS::smem, st>>>(M.p, M.ld, M.s, Li.p, Ui.p, Li.ld, Li.s, n,
-                                                                          boost ? 1 : 0, flag);
-      SAPB_LAUNCHED();
+      if (leaf <= 32) leaf_launch<32>(M, Li, Ui, n);
+      else if (leaf <= 64 || sizeof(T) != 4) leaf_launch<64>(M, Li, Ui, n);
+      else leaf_launch<(sizeof(T) == 4 ? 128 : 64)>(M, Li, Ui, n);
       return;
     }
     const int n1 = split(n), n2 = n - n1;
@@ -270,12 +276,13 @@ class WideBand {
   // same layout so that a repeated setup does not free and re-allocate
   DBuf<T> Dw, Ww, X, Wt, S, Ws;
   DBuf<T> Rw, Rs;  // recursion workspaces of the partition factors / the reduced system
+  DBuf<int> nz_d, spk_cols[2], spk_pos[2], sflag;  // spike-tip setup scratch
 
   // device bytes this object holds
   size_t bytes_held() const {
     size_t b = 0;
     for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
-                             &t1, &t2, &Dw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1], &csL, &csU,
+                             &t1, &t2, &Dw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1], &gws[2], &gws[3], &csL, &csU,
                              &csLo, &csUo})
       b += d->size() * sizeof(T);
     for (const DBuf<__half>* d : {&Lh, &Uh, &Loh, &Uoh}) b += d->size() * sizeof(__half);
@@ -288,11 +295,17 @@ class WideBand {
   ~WideBand() {
     if (fgraph) cudaGraphExecDestroy(fgraph);
     if (st2) cudaStreamSynchronize(st2);
+    for (cudaStream_t x : st_more)
+      if (x) cudaStreamSynchronize(x);
     if (h) cublasDestroy(h);
     if (h2) cublasDestroy(h2);
     if (st2) cudaStreamDestroy(st2);
+    for (cudaStream_t x : st_more)
+      if (x) cudaStreamDestroy(x);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    for (cudaEvent_t e : ev_lane)
+      if (e) cudaEventDestroy(e);
   }
 
   // The factorization's launch sequence (about a thousand small GEMMs,
@@ -301,7 +314,7 @@ class WideBand {
   // (every buffer it touches is kept across setups of the layout).
   cudaGraphExec_t fgraph = nullptr;
   long long fgraph_key = -1;
-  int fgraph_cut = 0;
+  int fgraph_cut = 0, fgraph_leaf = 0;
   // SAPB_FACTOR_GRAPH=0 runs the factorization's launches directly every time
   static bool graph_enabled() {
     const char* e = std::getenv("SAPB_FACTOR_GRAPH");
@@ -402,6 +415,8 @@ class WideBand {
       SAPB_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
       SAPB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
       SAPB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+      for (cudaStream_t& x : st_more) SAPB_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      for (cudaEvent_t& e : ev_lane) SAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
     if (cublas_ws.size() == 0) cublas_ws.alloc((size_t)64 << 20);
@@ -475,11 +490,12 @@ class WideBand {
   void factor(bool boost) {
     Dw.alloc((size_t)P * BB);
     Ww.alloc((size_t)P * BB);
-    Rw.alloc((size_t)P * std::max(1LL, BlockLU<T>::rec_ws(bs)));
+    Rw.alloc((size_t)P * std::max(1LL, BlockLU<T>::rec_ws(bs, leaf_size<T>())));
     flag.alloc(1);
     const long long key = (((long long)P * 65537 + bs) * 65537 + nb) * 4 + (boost ? 2 : 0) + (tf32 ? 1 : 0);
-    if (key != fgraph_key || factor_cut() != fgraph_cut) {
+    if (key != fgraph_key || factor_cut() != fgraph_cut || leaf_size<T>() != fgraph_leaf) {
       fgraph_cut = factor_cut();
+      fgraph_leaf = leaf_size<T>();
       if (fgraph) cudaGraphExecDestroy(fgraph);
       fgraph = nullptr;
       fgraph_key = key;
@@ -534,7 +550,7 @@ class WideBand {
     lu.flag = flag.get();
     lu.cut = factor_cut();
     lanes(lu);
-    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(bs));
+    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(bs, lu.leaf));
     lu.rw = Rw.get();
     const Mat<T> D{Dw.get(), bs, BB}, Wm{Ww.get(), bs, BB};
     lu.W = Wm;
@@ -574,14 +590,15 @@ class WideBand {
 
   // tri: 0 full, 1 lower, 2 upper (see k_tgemv).  Grids with fewer than
   // about 2.5 CTAs per SM split the columns over gridDim.z CTAs.
-  // Two lanes (streams) for the block sweeps: each takes half of the
-  // partitions, so one lane's launch tails overlap the other's streaming.
-  // Each lane has its own column-split scratch.
-  DBuf<T> gws[2];          // column-split partial sums
-  DBuf<unsigned> gctr[2];  // column-split arrival counters (zero between launches)
-  cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaStream_t lane_stream(int lane) const { return lane ? st2 : st; }
+  // Lanes (streams) for the block sweeps: each takes a contiguous share of
+  // the partitions, so one lane's launch tails overlap the others'
+  // streaming.  Each lane has its own column-split scratch.
+  static constexpr int kMaxLanes = 4;
+  DBuf<T> gws[kMaxLanes];          // column-split partial sums
+  DBuf<unsigned> gctr[kMaxLanes];  // column-split arrival counters (zero between launches)
+  cudaStream_t st2 = nullptr, st_more[kMaxLanes - 2] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_lane[kMaxLanes] = {};
+  cudaStream_t lane_stream(int lane) const { return lane == 0 ? st : (lane == 1 ? st2 : st_more[lane - 2]); }
   // CTAs one GEMV launch aims at through its column split (about 2.5 of the
   // three resident CTAs per SM); SAPB_GEMV_CTAS overrides
   static int gemv_ctas() {
@@ -648,22 +665,33 @@ class WideBand {
   // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
   // and U_{i,i+1} = L_ii^-1 E_i are lower triangular, U_ii^-1 and
   // L_{i+1,i} = F_i U_ii^-1 upper triangular (the band fits in one block).
+  // lanes of the sweeps: up to SAPB_SWEEP_LANES (1, 2 or 4), with at least
+  // two partitions per lane; by default 4 for the FP16 copies (shorter
+  // launches: 2.96 against 3.09 ms per sweep on the 1M-row workload), 2 for
+  // FP32 / FP64 (3.95 against 4.18 ms with 4)
+  int sweep_lanes() const {
+    const char* e = std::getenv("SAPB_SWEEP_LANES");
+    const int dflt = h16 ? 4 : 2;
+    int want = e ? std::atoi(e) : dflt;
+    if (want != 1 && want != 2 && want != 4) want = dflt;
+    if (!st2) return 1;
+    while (want > 1 && P < 2 * want) want /= 2;
+    return want;
+  }
   void solve_blocks(T* x) {
-    const int lanes = (P >= 4 && st2) ? 2 : 1;
-    if (lanes == 2) {
+    const int lanes = sweep_lanes();
+    if (lanes > 1) {
       SAPB_CUDA(cudaEventRecord(ev_fork, st));
-      SAPB_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
+      for (int l = 1; l < lanes; l++) SAPB_CUDA(cudaStreamWaitEvent(lane_stream(l), ev_fork, 0));
     }
-    const int half = P / 2;
     for (int lane = 0; lane < lanes; lane++) {
-      const int p0 = lanes == 2 ? lane * half : 0;
-      const int np = lanes == 2 ? (lane ? P - half : half) : P;
+      const int p0 = (int)((long long)P * lane / lanes), p1 = (int)((long long)P * (lane + 1) / lanes);
       const long long vo = (long long)p0 * plen;
-      solve_blocks_part(x + vo, yv.get() + vo, tv.get() + vo, p0, np, lane);
+      solve_blocks_part(x + vo, yv.get() + vo, tv.get() + vo, p0, p1 - p0, lane);
     }
-    if (lanes == 2) {
-      SAPB_CUDA(cudaEventRecord(ev_join, st2));
-      SAPB_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+    for (int l = 1; l < lanes; l++) {
+      SAPB_CUDA(cudaEventRecord(ev_lane[l], lane_stream(l)));
+      SAPB_CUDA(cudaStreamWaitEvent(st, ev_lane[l], 0));
     }
   }
 
@@ -756,13 +784,12 @@ class WideBand {
     Wc.alloc((size_t)nI * sK);
     Vc.zero(st);
     Wc.zero(st);
-    std::vector<int> nzh;
+    std::vector<int> nzh((size_t)2 * nI * K);
     {
-      DBuf<int> nzd;
-      nzd.alloc((size_t)2 * nI * K);
-      k_nz_cols<T><<<dim3(grid1d(K, 256, 64), 2 * nI), 256, 0, st>>>(offd, K, nzd.get());
+      nz_d.ensure(nzh.size());
+      k_nz_cols<T><<<dim3(grid1d(K, 256, 64), 2 * nI), 256, 0, st>>>(offd, K, nz_d.get());
       SAPB_LAUNCHED();
-      nzd.download(nzh, st);
+      SAPB_CUDA(cudaMemcpyAsync(nzh.data(), nz_d.get(), nzh.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
       SAPB_CUDA(cudaStreamSynchronize(st));
     }
     // the X slab holds nI * plen * cs values
@@ -784,13 +811,15 @@ class WideBand {
         for (int c = 0; c < K; c++)
           if (nzh[(size_t)(2 * t + which) * K + c]) cols[(size_t)t * ncol + j++] = c;
       }
-      DBuf<int> cols_d, pos_d;
-      cols_d.upload(cols, st);
-      pos_d.upload(pos, st);
+      // (buffers grow only: the two sides and repeated setups reuse them)
+      DBuf<int>& cols_d = spk_cols[which];
+      DBuf<int>& pos_d = spk_pos[which];
+      cols_d.put(cols, st);
+      pos_d.put(pos, st);
       const int cs = std::min(ncol, cs_max);
       const long long sX = plen * cs;
-      X.alloc((size_t)nI * sX);
-      Wt.alloc((size_t)nI * bs * cs);
+      X.ensure((size_t)nI * sX);
+      Wt.ensure((size_t)nI * bs * cs);
       BlockLU<T> ops;
       ops.h = h;
       ops.st = st;
@@ -806,7 +835,7 @@ class WideBand {
       const int kt = std::min(1024, ((K + 31) / 32) * 32);
       for (int j0 = 0; j0 < ncol; j0 += cs) {
         const int w = std::min(cs, ncol - j0);
-        X.zero(st);
+        SAPB_CUDA(cudaMemsetAsync(X.get(), 0, (size_t)nI * sX * sizeof(T), st));
         k_spike_rhs<T><<<dim3(w, nI), kt, 0, st>>>(offd, which, K, cols_d.get(), ncol, j0, pos_d.get(), X.get(), sX,
                                                     plen);
         SAPB_LAUNCHED();
@@ -844,7 +873,6 @@ class WideBand {
     SAPB_LAUNCHED();
     k_couple_colmajor<T><<<tg, dim3(32, 8), 0, st>>>(offd, 1, K, ldK, sK, Cc.get());
     SAPB_LAUNCHED();
-    DBuf<int> sflag;
     S.alloc((size_t)nI * sK);
     Ws.alloc((size_t)nI * sK);
     sflag.alloc(1);
@@ -863,7 +891,7 @@ class WideBand {
     lu.flag = sflag.get();
     lu.W = Mat<T>{Ws.get(), ldK, sK};
     lanes(lu);
-    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(K));
+    lu.rws = std::max(1LL, BlockLU<T>::rec_ws(K, lu.leaf));
     Rs.alloc((size_t)nI * lu.rws);
     lu.rw = Rs.get();
     const Mat<T> Sm{S.get(), ldK, sK};
