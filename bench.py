@@ -54,8 +54,9 @@ LU_SAMPLE_ROWS = 400
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) over the
 # algorithmic bytes of one block-sweep k_tgemv launch, measured with ncu on
 # this workload at grid side 310 (block size 3168, the FP32 block size at
-# the full size); a launch's traffic scales with its triangle's bytes
-TGEMV_TRAFFIC_RATIO = {4: 1.051}
+# the full size), per bytes of a factor value (4: FP32, 2: FP16 copies); a
+# launch's traffic scales with its triangle's bytes
+TGEMV_TRAFFIC_RATIO = {4: 1.051, 2: 1.115}
 
 
 def measured_peaks():
