@@ -148,6 +148,8 @@ class PrecBase {
   virtual void setup_sparse(const Csr& A) = 0;
   virtual void apply_band(const double* v, double* z) = 0;
   virtual void block_layout(int& bs, int& nb) const = 0;
+  // raise the errors device waits recorded (call after a stream synchronisation)
+  virtual void check_device() = 0;
   virtual void update_values(const double* entries, long long nnz, bool device) = 0;
   void apply(const double* v, double* z) { apply_band(v, z); }
 
@@ -949,6 +951,10 @@ class PrecondT : public PrecBase {
 
   // Precond::operator() + solve + getSRev (sap/precond.h:1370-1528) in the
   // band's row order.
+  void check_device() override {
+    if (wide) wide->check_device();
+  }
+
   void apply_band(const double* v, double* z) override {
     if (ptype == SAP_PRECOND_NONE) {
       SAPB_CUDA(cudaMemcpyAsync(z, v, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1907,6 +1913,7 @@ int sap_solver_solve(sap_solver* h, sap_spmv* spmv, const double* b, double* x, 
     cudaMemcpyKind kout = memspace == SAP_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     SAPB_CUDA(cudaMemcpyAsync(x, S.xvec.get(), bytes, kout, S.st));
     SAPB_CUDA(cudaStreamSynchronize(S.st));
+    S.pc().check_device();
     S.stats.timeSolve = ms_since(t0);
     S.stats.rhsNorm = S.mon.rhsNorm;
     S.stats.residualNorm = S.mon.rNorm;
@@ -1923,6 +1930,7 @@ int sap_precond_apply(sap_solver* h, const double* v, double* z) {
     if (!S.setup_done) throw Error(SAP_ILLEGAL_SOLVE, "preconditioner used before setup().");
     S.pc().apply(v, z);
     SAPB_CUDA(cudaStreamSynchronize(S.st));
+    S.pc().check_device();
   });
 }
 

@@ -343,32 +343,27 @@ __device__ __forceinline__ void vec_fma(const uint4& a, T xv, T* acc) {  // 8 x 
 // arrives last at the tile's counter (ctr, zero between launches) adds the S
 // slices in order s = 0..S-1, writes y and resets the counter.  No CTA waits
 // for another.
-// (three CTAs per SM for the vector forms: 16 warps each, <= 42 registers)
-template <typename T, int VEC, typename MT = T>
-__global__ void __launch_bounds__(kGemvWarps * 32, VEC > 1 ? 3 : 1) k_tgemv(const MT* A, int ld, long long sA, const T* x, long long sx,
-                                                           const T* c, long long sc, T* y, long long sy, int n,
-                                                           int mode, int tri, T* ws, unsigned* ctr,
-                                                           const T* cs = nullptr, long long scs = 0) {
+// One work item of the GEMV: tile pair `pair` (tiles pair and T-1-pair) of
+// batch element b, column slice sl of S.  A, x, c, y and cs point at batch
+// element b already; b only selects the column-split scratch slots.  CG:
+// x and c are read through L2 (written by other CTAs of the same launch).
+template <typename T, int VEC, typename MT, bool CG = false>
+__device__ __forceinline__ void tgemv_item(int pair, int b, int S, int sl, const MT* Ab, int ld, const T* xb,
+                                           const T* cb, T* yb, int n, int mode, int tri, T* ws, unsigned* ctr,
+                                           const T* csb, T (*part)[32 * (VEC > 1 ? VEC : 2)],
+                                           unsigned& last_cta) {
   constexpr int R = 32 * (VEC > 1 ? VEC : 2);
-  __shared__ T part[kGemvWarps][R];
-  __shared__ unsigned last_cta;
-  const int b = blockIdx.y;
-  const int S = gridDim.z, sl = blockIdx.z;
   const int ntile = (n + R - 1) / R;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  const MT* Ab = A + b * sA;
-  const T* xb = x + b * sx;
-  const T* csb = cs + b * scs;
   // x_c, times the column scale for a scaled FP16 matrix
   auto xs = [&](int col) -> T {
-    if constexpr (std::is_same<MT, T>::value) return xb[col];
-    else return xb[col] * csb[col];
+    const T xc = CG ? __ldcg(xb + col) : xb[col];
+    if constexpr (std::is_same<MT, T>::value) return xc;
+    else return xc * csb[col];
   };
   for (int half = 0; half < 2; half++) {
-    const int tile = half == 0 ? (int)blockIdx.x : ntile - 1 - (int)blockIdx.x;
-    if (half == 1 && tile <= (int)blockIdx.x) break;
+    const int tile = half == 0 ? pair : ntile - 1 - pair;
+    if (half == 1 && tile <= pair) break;
     const int r0 = tile * R;
     int c0 = 0, c1 = n;
     if (tri == 1) c1 = min(n, r0 + R);
@@ -450,7 +445,7 @@ __global__ void __launch_bounds__(kGemvWarps * 32, VEC > 1 ? 3 : 1) k_tgemv(cons
         T s = T(0);
 #pragma unroll
         for (int k = 0; k < kGemvWarps; k++) s += part[k][q];
-        if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+        if (r < n) yb[r] = (mode == 1) ? (CG ? __ldcg(cb + r) : cb[r]) - s : s;
       }
     } else {
       const long long slot = (long long)b * ntile + tile;
@@ -470,12 +465,133 @@ __global__ void __launch_bounds__(kGemvWarps * 32, VEC > 1 ? 3 : 1) k_tgemv(cons
           const int r = r0 + q;
           T s = T(0);
           for (int k = 0; k < S; k++) s += __ldcg(ws + (slot * S + k) * R + q);
-          if (r < n) y[b * sy + r] = (mode == 1) ? c[b * sc + r] - s : s;
+          if (r < n) yb[r] = (mode == 1) ? (CG ? __ldcg(cb + r) : cb[r]) - s : s;
         }
         if (threadIdx.x == 0) ctr[slot] = 0u;
       }
     }
     __syncthreads();
+  }
+}
+
+// (three CTAs per SM for the vector forms: 16 warps each, <= 42 registers)
+template <typename T, int VEC, typename MT = T>
+__global__ void __launch_bounds__(kGemvWarps * 32, VEC > 1 ? 3 : 1) k_tgemv(const MT* A, int ld, long long sA, const T* x, long long sx,
+                                                           const T* c, long long sc, T* y, long long sy, int n,
+                                                           int mode, int tri, T* ws, unsigned* ctr,
+                                                           const T* cs = nullptr, long long scs = 0) {
+  constexpr int R = 32 * (VEC > 1 ? VEC : 2);
+  __shared__ T part[kGemvWarps][R];
+  __shared__ unsigned last_cta;
+  const int b = blockIdx.y;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  tgemv_item<T, VEC, MT>((int)blockIdx.x, b, (int)gridDim.z, (int)blockIdx.z, A + b * sA, ld, x + b * sx,
+                         c ? c + b * sc : nullptr, y + b * sy, n, mode, tri, ws, ctr, cs ? cs + b * scs : nullptr,
+                         part, last_cta);
+}
+
+// Barrier of the `n` CTAs of one group (a counter and a generation word in
+// global memory, zero before the first use).  The wait is bounded: after
+// kBarrierSpins polls it raises *err and returns false.
+constexpr long long kBarrierSpins = 1LL << 22;
+__device__ __forceinline__ bool group_barrier(unsigned* cnt, unsigned* gen, unsigned n, int* err) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    const unsigned g = *reinterpret_cast<volatile unsigned*>(gen);
+    __threadfence();
+    if (atomicAdd(cnt, 1u) == n - 1) {
+      *cnt = 0u;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      long long it = 0;
+      while (*reinterpret_cast<volatile unsigned*>(gen) == g) {
+        if (++it > kBarrierSpins || *reinterpret_cast<volatile int*>(err)) {
+          atomicOr(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+// One whole block sweep (x <- A_p^-1 x for every partition) as a single
+// cooperative launch: partition p is served by the G CTAs of group p, which
+// run its 4 nb - 2 block-row GEMVs (the steps of solve_blocks_part) with a
+// group barrier between steps, S column slices per tile pair (items =
+// pairs * S per step, spread over the group).  Partitions do not wait for
+// each other.  Factor blocks: L_ii^-1 at Li + (p nb + i) BB, L_{i+1,i} at
+// Lo + (p (nb-1) + i) BB, likewise U; their column scales (FP16 copies) at
+// cs* + (block index) bs.  bar holds 2 words per partition; err is raised by
+// a barrier that timed out (the kernel then returns).
+template <typename T, int VEC, typename MT>
+__global__ void __launch_bounds__(kGemvWarps * 32, 3) k_sweep(const MT* __restrict__ Li, const MT* __restrict__ Ui,
+                                                              const MT* __restrict__ Lo, const MT* __restrict__ Uo,
+                                                              const T* csL, const T* csU, const T* csLo, const T* csUo,
+                                                              T* x, T* y, T* t, int nb, int bs, long long BB,
+                                                              long long plen, int G, int S, T* ws, unsigned* ctr,
+                                                              unsigned* bar, int* err) {
+  constexpr int R = 32 * (VEC > 1 ? VEC : 2);
+  __shared__ T part[kGemvWarps][R];
+  __shared__ unsigned last_cta;
+  const int p = blockIdx.x / G, g = blockIdx.x - p * G;
+  const int ntile = (bs + R - 1) / R, pairs = (ntile + 1) / 2, items = pairs * S;
+  T* xp = x + p * plen;
+  T* yp = y + p * plen;
+  T* tp = t + p * plen;
+  const long long bd = (long long)p * nb, bo = (long long)p * (nb - 1);
+  const bool scaled = !std::is_same<MT, T>::value;
+  const int steps = 4 * nb - 2;
+  for (int s = 0; s < steps; s++) {
+    const MT* A;
+    const T *xv, *cv = nullptr, *cs = nullptr;
+    T* yv;
+    int mode = 0, tri;
+    if (s < 2 * nb - 1) {  // forward: y_i = L_ii^-1 (x_i - L_{i,i-1} y_{i-1})
+      const int i = (s + 1) / 2;
+      if (s & 1) {
+        A = Lo + (bo + i - 1) * BB;
+        cs = scaled ? csLo + (bo + i - 1) * bs : nullptr;
+        xv = yp + (long long)(i - 1) * bs;
+        cv = xp + (long long)i * bs;
+        yv = tp;
+        mode = 1;
+        tri = 2;
+      } else {
+        A = Li + (bd + i) * BB;
+        cs = scaled ? csL + (bd + i) * bs : nullptr;
+        xv = i > 0 ? tp : xp;
+        yv = yp + (long long)i * bs;
+        tri = 1;
+      }
+    } else {  // backward: x_i = U_ii^-1 (y_i - U_{i,i+1} x_{i+1})
+      const int s2 = s - (2 * nb - 1), k = (s2 + 1) / 2, i = nb - 1 - k;
+      if (s2 & 1) {
+        A = Uo + (bo + i) * BB;
+        cs = scaled ? csUo + (bo + i) * bs : nullptr;
+        xv = xp + (long long)(i + 1) * bs;
+        cv = yp + (long long)i * bs;
+        yv = tp;
+        mode = 1;
+        tri = 1;
+      } else {
+        A = Ui + (bd + i) * BB;
+        cs = scaled ? csU + (bd + i) * bs : nullptr;
+        xv = k > 0 ? tp : yp + (long long)i * bs;
+        yv = xp + (long long)i * bs;
+        tri = 2;
+      }
+    }
+    for (int it = g; it < items; it += G)
+      tgemv_item<T, VEC, MT, true>(it / S, p, S, it % S, A, bs, xv, cv, yv, bs, mode, tri, ws, ctr, cs, part,
+                                   last_cta);
+    if (!group_barrier(bar + 2 * p, bar + 2 * p + 1, (unsigned)G, err)) return;
   }
 }
 

@@ -282,7 +282,7 @@ class WideBand {
   size_t bytes_held() const {
     size_t b = 0;
     for (const DBuf<T>* d : {&Linv, &Uinv, &Uoff, &Loff, &Vc, &Wc, &Bc, &Cc, &SLi, &SUi, &Fb, &xv, &yv, &tv, &xbt, &fbt,
-                             &t1, &t2, &Dw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1], &gws[2], &gws[3], &csL, &csU,
+                             &t1, &t2, &Dw, &Ww, &X, &Wt, &S, &Ws, &Rw, &Rs, &gws[0], &gws[1], &gws[2], &gws[3], &pws, &csL, &csU,
                              &csLo, &csUo})
       b += d->size() * sizeof(T);
     for (const DBuf<__half>* d : {&Lh, &Uh, &Loh, &Uoh}) b += d->size() * sizeof(__half);
@@ -338,8 +338,7 @@ class WideBand {
   }
 
   // tf32: FP32 block products on the tensor cores (TF32 inputs, FP32
-  // accumulation) for the partition factors and spikes; the reduced system
-  // keeps full FP32 products.
+  // accumulation) for the partition factors, spikes and reduced systems.
   bool tf32 = false;
   // h16: the block sweeps of the apply read FP16 copies of the factor
   // blocks with a power-of-two scale per column (half the bytes of FP32);
@@ -381,12 +380,21 @@ class WideBand {
     if (e && std::atoi(e) > 0) return std::atoi(e);
     return tf32 ? (1 << 30) : 384;
   }
-  // the same cut-off for the products of the partition factorization;
+  // The TF32 form builds and factors the reduced systems with TF32 products
+  // too (1M-row workload: 41 -> 21 ms, the same 23 FGMRES iterations);
+  // SAPB_REDUCED_TF32=0 keeps them in full FP32
+  static bool reduced_tf32() {
+    const char* e = std::getenv("SAPB_REDUCED_TF32");
+    return !(e && std::atoi(e) == 0);
+  }
+  // the same cut-off for the products of the partition factorization: one
+  // structure-aware level for TF32 (1M-row workload: block LU 187 -> 171 ms),
+  // down to 384 for the compute-bound FP64 / FP32 products;
   // SAPB_FACTOR_CUT overrides
   int factor_cut() const {
     const char* e = std::getenv("SAPB_FACTOR_CUT");
     if (e && std::atoi(e) > 0) return std::atoi(e);
-    return tf32 ? (1 << 30) : 384;
+    return tf32 ? 2048 : 384;
   }
   void math_mode(bool fast) {
     for (cublasHandle_t x : {h, h2})
@@ -678,7 +686,96 @@ class WideBand {
     while (want > 1 && P < 2 * want) want /= 2;
     return want;
   }
+  // Persistent sweeps (k_sweep, one cooperative launch per sweep), the
+  // default for the FP16 copies (1M-row workload: 2.77 ms per sweep against
+  // 3.10 with 4 lanes of per-step launches); the FP32 / FP64 sweeps stay on
+  // per-step launches (3.90 / 7.05 ms against 3.97 / 7.29 persistent).
+  // SAPB_SWEEP_PERSISTENT = 0 / 1 forces either.
+  DBuf<T> pws;
+  DBuf<unsigned> pctr, pbar;
+  DBuf<int> perr;
+  PinnedBuf<int> perr_h;
+  bool persistent_enabled() const {
+    const char* e = std::getenv("SAPB_SWEEP_PERSISTENT");
+    if (e) return std::atoi(e) != 0;
+    return h16;
+  }
+  template <int V, typename MT>
+  bool sweep_persistent(T* x, const MT* Li, const MT* Ui, const MT* Lo, const MT* Uo, const T* cL, const T* cU,
+                        const T* cLo, const T* cUo) {
+    auto kern = k_sweep<T, V, MT>;
+    int dev = 0, sms = 0, occ = 0, coop = 0;
+    SAPB_CUDA(cudaGetDevice(&dev));
+    SAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SAPB_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    SAPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kGemvWarps * 32, 0));
+    const int gmax = occ * sms / P;
+    if (!coop || gmax < 1) return false;
+    constexpr int R = tgemv_rows<T, V>();
+    const int ntile = (bs + R - 1) / R, pairs = (ntile + 1) / 2;
+    int S = 1, G = gmax;
+    if (pairs <= gmax) {
+      S = std::max(1, std::min({8, gmax / pairs, std::max(1, bs / 256)}));
+      G = pairs * S;
+    }
+    pws.ensure((size_t)P * ntile * S * R);
+    if (pctr.size() < (size_t)P * ntile) {
+      pctr.alloc((size_t)P * ntile);
+      pctr.zero(st);
+    }
+    if (pbar.size() < (size_t)2 * P) {
+      pbar.alloc((size_t)2 * P);
+      pbar.zero(st);
+    }
+    if (perr.size() == 0) {
+      perr.alloc(1);
+      perr.zero(st);
+      *perr_h.reserve(1) = 0;
+    }
+    T* y = yv.get();
+    T* t = tv.get();
+    T* ws = pws.get();
+    unsigned* ctr = pctr.get();
+    unsigned* bar = pbar.get();
+    int* err = perr.get();
+    int nbv = nb, bsv = bs;
+    long long BBv = BB, plenv = plen;
+    void* args[] = {(void*)&Li, (void*)&Ui, (void*)&Lo, (void*)&Uo, (void*)&cL, (void*)&cU, (void*)&cLo, (void*)&cUo,
+                    (void*)&x, (void*)&y, (void*)&t, (void*)&nbv, (void*)&bsv, (void*)&BBv, (void*)&plenv, (void*)&G,
+                    (void*)&S, (void*)&ws, (void*)&ctr, (void*)&bar, (void*)&err};
+    SAPB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)(P * G)), dim3(kGemvWarps * 32), args, 0,
+                                          st));
+    count_launch();
+    SAPB_CUDA(cudaMemcpyAsync(perr_h.get(), err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    return true;
+  }
+  // after the caller synchronised the stream: a barrier of a persistent
+  // sweep that timed out is reported (and the barrier state reset)
+  void check_device() {
+    if (!perr_h.get() || *perr_h.get() == 0) return;
+    *perr_h.get() = 0;
+    perr.zero(st);
+    pbar.zero(st);
+    pctr.zero(st);
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    throw Error(SAP_ERR_DEVICE_TIMEOUT, "a block-sweep barrier wait ran out of its iteration limit");
+  }
   void solve_blocks(T* x) {
+    if (persistent_enabled()) {
+      if (h16) {
+        if constexpr (sizeof(T) == 4) {
+          if (sweep_persistent<8, __half>(x, Lh.get(), Uh.get(), Loh.get(), Uoh.get(), csL.get(), csU.get(),
+                                          csLo.get(), csUo.get()))
+            return;
+        }
+      } else {
+        constexpr int V = 16 / sizeof(T);
+        const bool vec = bs % V == 0;
+        if (vec && sweep_persistent<V, T>(x, Linv.get(), Uinv.get(), Loff.get(), Uoff.get(), nullptr, nullptr,
+                                          nullptr, nullptr))
+          return;
+      }
+    }
     const int lanes = sweep_lanes();
     if (lanes > 1) {
       SAPB_CUDA(cudaEventRecord(ev_fork, st));
@@ -862,7 +959,7 @@ class WideBand {
   // S_t = I - W_t V_t, factored with its triangular inverses (boosted only
   // when `boost`); coupling blocks kept column-major for the apply.
   void reduced(const T* offd, const std::vector<int>& iface, bool boost) {
-    math_mode(false);
+    math_mode(tf32 && reduced_tf32());
     const int nI = P - 1;
     Bc.alloc((size_t)nI * sK);
     Cc.alloc((size_t)nI * sK);

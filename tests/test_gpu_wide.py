@@ -239,3 +239,23 @@ def test_f16_block_storage_fgmres_banded():
     assert s.solve(sap.MVBanded(A), b, x)
     assert s.getStats().relResidualNorm <= 1e-10
     assert np.linalg.norm(x - 1.0) / np.sqrt(n) <= 1e-8
+
+
+@pytest.mark.parametrize("prec,tol", [("double", 1e-12), ("float", 1e-5), ("tf32_f16", 1e-5)])
+def test_persistent_sweep_matches_launch_chain(monkeypatch, prec, tol):
+    # the block sweeps as one cooperative launch (group barriers between the
+    # block-row steps) against the chain of per-step launches: the same
+    # products, summed in slices that may differ
+    n, K, P = 24011, 257, 5
+    band = sap.generate_band_host(n, K, 0.8, 2, seed=n + K)
+    A = sap.BandedMatrix.from_array(band, n, K)
+    s = sap.Solver(P, sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False,
+                                  factMethod=sap.LU_only), prec=prec)
+    s.setup(A)
+    v = np.random.default_rng(5).standard_normal(n)
+    monkeypatch.setenv("SAPB_SWEEP_PERSISTENT", "1")
+    z1 = apply_gpu(s, v)
+    monkeypatch.setenv("SAPB_SWEEP_PERSISTENT", "0")
+    z0 = apply_gpu(s, v)
+    assert np.all(np.isfinite(z1))
+    assert np.linalg.norm(z1 - z0) / np.linalg.norm(z0) <= tol
