@@ -377,7 +377,9 @@ def main():
     if "block_sweep" in head:
         bsw = head["block_sweep"]
         ratio = TGEMV_TRAFFIC_RATIO.get(head["value_bytes"])
-        roofline = {"kernel": "k_tgemv (one block_sweep = 4*nb-2 launches)", "bound": "hbm", "achieved": bsw["gbs"],
+        kern = ("k_sweep<float, 8, __half> (one cooperative launch per block sweep)" if head["value_bytes"] == 2
+                else "k_tgemv (one block sweep = 4*nb-2 launches)")
+        roofline = {"kernel": kern, "bound": "hbm", "achieved": bsw["gbs"],
                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": bsw["gbs"] / peaks["hbm_gbs"],
                     "traffic": int(ratio * bsw["bytes"]) if ratio else None,
                     "traffic_source": "ncu ratio of one block-sweep launch at grid side 310, scaled" if ratio else None,
