@@ -1694,13 +1694,27 @@ int sap_csr_create(int n, int nnz, const int* rp, const int* ci, const double* v
     auto h = std::make_unique<sap_csr>();
     h->c.n = n; h->c.nnz = nnz;
     h->c.rp_h.resize(n + 1); h->c.ci_h.resize(nnz); h->c.v_h.resize(nnz);
-    cudaMemcpyKind kind = memspace == SAP_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
-    SAPB_CUDA(cudaMemcpy(h->c.rp_h.data(), rp, (n + 1) * sizeof(int), kind));
-    SAPB_CUDA(cudaMemcpy(h->c.ci_h.data(), ci, (size_t)nnz * sizeof(int), kind));
-    SAPB_CUDA(cudaMemcpy(h->c.v_h.data(), v, (size_t)nnz * sizeof(double), kind));
+    if (memspace == SAP_DEVICE) {
+      SAPB_CUDA(cudaMemcpy(h->c.rp_h.data(), rp, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      SAPB_CUDA(cudaMemcpy(h->c.ci_h.data(), ci, (size_t)nnz * sizeof(int), cudaMemcpyDeviceToHost));
+      SAPB_CUDA(cudaMemcpy(h->c.v_h.data(), v, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {  // host copies in parallel chunks
+      std::copy(rp, rp + n + 1, h->c.rp_h.begin());
+      _Pragma("omp parallel for schedule(static)")
+      for (int c = 0; c < 64; c++) {
+        const long long a = (long long)nnz * c / 64, e = (long long)nnz * (c + 1) / 64;
+        std::copy(ci + a, ci + e, h->c.ci_h.begin() + a);
+        std::copy(v + a, v + e, h->c.v_h.begin() + a);
+      }
+    }
     SAP_REQUIRE(h->c.rp_h[0] == 0 && h->c.rp_h[n] == nnz, "row offsets inconsistent with nnz");
-    for (int i = 0; i < n; i++) SAP_REQUIRE(h->c.rp_h[i] <= h->c.rp_h[i + 1], "row offsets not monotone");
-    for (int p = 0; p < nnz; p++) SAP_REQUIRE(h->c.ci_h[p] >= 0 && h->c.ci_h[p] < n, "column index out of range");
+    int bad_rp = 0, bad_ci = 0;
+    _Pragma("omp parallel for schedule(static) reduction(| : bad_rp)")
+    for (int i = 0; i < n; i++) bad_rp |= h->c.rp_h[i] > h->c.rp_h[i + 1];
+    SAP_REQUIRE(!bad_rp, "row offsets not monotone");
+    _Pragma("omp parallel for schedule(static) reduction(| : bad_ci)")
+    for (int p = 0; p < nnz; p++) bad_ci |= h->c.ci_h[p] < 0 || h->c.ci_h[p] >= n;
+    SAP_REQUIRE(!bad_ci, "column index out of range");
     h->c.rp.upload(h->c.rp_h, nullptr);
     h->c.ci.upload(h->c.ci_h, nullptr);
     h->c.v.upload(h->c.v_h, nullptr);
