@@ -243,6 +243,31 @@ int sap_solver_info(const sap_solver* s, int* n, int* k, int* num_partitions);
  * 4: per-partition half-bandwidths K_p (m_ks_host).
  * With out == NULL only *count is set. */
 int sap_solver_get_reorder(const sap_solver* s, int which, int* out, int64_t* count);
+
+/* The host reordering of a CSR setup on its own, without a device: the
+ * matrix converted to the preconditioner type (SAP_PREC_FLOAT or
+ * SAP_PREC_DOUBLE) with explicit zeros removed (precond.h:1667-1713), DB
+ * matching and scaling with edge weights log(rowmax / |a|) computed on the
+ * host (graph.h:1214-1361, 1875-2173), RCM (graph.h:1371-1584), drop-off
+ * (graph.h:598-747), coupling split and second-level reordering
+ * (graph.h:756-1008), variable half-bandwidths (graph.h:1093-1206) and the
+ * composed permutations (precond.h:2071-2097), as a setup with
+ * num_partitions and opts runs them (Graph::reorder and
+ * transformToBandedMatrix's host part).  Outputs (NULL to skip): db_row_perm
+ * and final_pos / final_order (n each, the arrays 0-2 of
+ * sap_solver_get_reorder), first_rows (P-1, variable band only) and part_k
+ * (P; K in every partition for a constant band), P <= num_partitions.  threads > 0 sets the host threads for this call (the
+ * outputs do not depend on it).  Errors: SAP_ERR_INVALID_ARGUMENT, the DB's
+ * SAP_MATRIX_SINGULAR / SAP_NEGATIVE_DB_WEIGHT.  Extension, no reference
+ * counterpart as a separate call. */
+typedef struct sap_reorder_info {
+  int K, P, k_db, k_reorder, var_band;
+  double drop_actual;
+} sap_reorder_info;
+int sap_reorder_host(int n, int nnz, const int* row_offsets, const int* column_indices, const double* values,
+                     int num_partitions, const sap_options* opts, int prec_dtype, int threads,
+                     sap_reorder_info* info, int* db_row_perm, int* final_pos, int* final_order, int* first_rows,
+                     int* part_k);
 /* The cudaStream_t all device work of this solver is enqueued on. */
 void* sap_solver_stream(const sap_solver* s);
 /* Layout of the wide-band block path after setup: the block size and the

@@ -132,6 +132,7 @@ _sig = {
     "sap_solver_info": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "sap_solver_stream": (_vp, [_vp]),
     "sap_solver_get_reorder": (_i, [_vp, _i, _vp, ctypes.POINTER(ctypes.c_int64)]),
+    "sap_reorder_host": (_i, [_i, _i, _vp, _vp, _vp, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_blas_dots_noalloc": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_profile_select": (_i, [ctypes.c_char_p]),
@@ -234,6 +235,41 @@ def solve_batch(bands, ks, bs, num_partitions: int, opts: "Options", prec: str =
                                        int(num_partitions), ctypes.cast(ctypes.pointer(copts), ctypes.c_void_p),
                                        _PREC[prec], ctypes.cast(res, ctypes.c_void_p), ctypes.byref(sec)))
     return xs, [(r.rel_residual, r.iterations, bool(r.converged)) for r in res], sec.value
+
+
+class _ReorderInfo(ctypes.Structure):
+    _fields_ = [("K", ctypes.c_int), ("P", ctypes.c_int), ("k_db", ctypes.c_int), ("k_reorder", ctypes.c_int),
+                ("var_band", ctypes.c_int), ("drop_actual", ctypes.c_double)]
+
+
+def reorder_host(row_offsets, column_indices, values, num_partitions: int, opts: "Options" = None,
+                 prec: str = "float", threads: int = 0) -> dict:
+    """The host reordering of a CSR setup on its own, without a device
+    (`sap_reorder_host`): DB, RCM, drop-off, second level and the composed
+    permutations.  Returns K, P, k_db, k_reorder, var_band, drop_actual and
+    the arrays dbRowPerm, finalPerm, finalReordering, first_rows, ks (the
+    names of Solver.getReorder)."""
+    rp = np.ascontiguousarray(row_offsets, np.int32)
+    ci = np.ascontiguousarray(column_indices, np.int32)
+    v = np.ascontiguousarray(values, np.float64)
+    n, nnz, P = rp.size - 1, ci.size, int(num_partitions)
+    if prec not in ("float", "double"):
+        raise ValueError("prec must be 'float' or 'double'")
+    copts = (opts or Options())._c()
+    info = _ReorderInfo()
+    out = {k: np.empty(m, np.int32) for k, m in (("dbRowPerm", n), ("finalPerm", n), ("finalReordering", n),
+                                                  ("first_rows", max(P - 1, 0)), ("ks", P))}
+    _check(_lib.sap_reorder_host(n, nnz, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, P,
+                                 ctypes.cast(ctypes.pointer(copts), ctypes.c_void_p), _PREC[prec], int(threads),
+                                 ctypes.cast(ctypes.pointer(info), ctypes.c_void_p),
+                                 *[out[k].ctypes.data for k in ("dbRowPerm", "finalPerm", "finalReordering",
+                                                                "first_rows", "ks")]))
+    res = {f: getattr(info, f) for f, _ in _ReorderInfo._fields_}
+    res["first_rows"] = out["first_rows"][:max(info.P - 1, 0)] if info.var_band else np.empty(0, np.int32)
+    res["ks"] = out["ks"][:info.P]
+    for k in ("dbRowPerm", "finalPerm", "finalReordering"):
+        res[k] = out[k]
+    return res
 
 
 def library_call_count() -> int:

@@ -953,4 +953,112 @@ template class Pipeline<float>;
 template class Pipeline<double>;
 
 }  // namespace rp
+
+void set_last_error(const std::string& msg);
+
+namespace {
+
+// The host part of a CSR setup on its own: explicit zeros removed in T,
+// DB weights log(rowmax / |a|) computed on the host (std::log), the
+// pipeline, and its outputs copied out.
+template <typename T>
+int reorder_host(int n, int nnz, const int* rp, const int* ci, const double* v, int P, const sap_options& o,
+                 sap_reorder_info* info, int* db_row_perm, int* final_pos, int* final_order, int* first_rows,
+                 int* part_k) {
+  rp::Pipeline<T> pl;
+  pl.n = n;
+  pl.P_req = P;
+  pl.do_db = o.performDB != 0;
+  pl.scale = o.applyScaling != 0;
+  pl.drop_frac = o.dropOffFraction;
+  pl.max_bandwidth = o.maxBandwidth;
+  pl.var_band = o.variableBandwidth != 0;
+  pl.in_rp.assign(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    int c = 0;
+    for (int e = rp[i]; e < rp[i + 1]; e++) c += (T)v[e] != T(0);
+    pl.in_rp[i + 1] = pl.in_rp[i] + c;
+  }
+  pl.in_ci.resize(pl.in_rp[n]);
+  pl.in_val.resize(pl.in_rp[n]);
+  for (int i = 0, d = 0; i < n; i++)
+    for (int e = rp[i]; e < rp[i + 1]; e++)
+      if ((T)v[e] != T(0)) {
+        pl.in_ci[d] = ci[e];
+        pl.in_val[d++] = (T)v[e];
+      }
+  pl.nnz = (int)pl.in_ci.size();
+  std::vector<double> w, rmax;
+  if (pl.do_db) {
+    w.resize(pl.nnz);
+    rmax.resize(n);
+    for (int i = 0; i < n; i++) {
+      double m = 0.0;
+      for (int e = pl.in_rp[i]; e < pl.in_rp[i + 1]; e++) m = std::max(m, std::fabs((double)pl.in_val[e]));
+      rmax[i] = m;
+      for (int e = pl.in_rp[i]; e < pl.in_rp[i + 1]; e++) w[e] = std::log(m / std::fabs((double)pl.in_val[e]));
+    }
+  }
+  pl.run(w.data(), rmax.data());
+  info->K = pl.K;
+  info->P = pl.P;
+  info->k_db = pl.k_db;
+  info->k_reorder = pl.k_reorder;
+  info->var_band = pl.var_band ? 1 : 0;
+  info->drop_actual = (double)pl.drop_actual;
+  if (db_row_perm) std::copy(pl.db_row_perm.begin(), pl.db_row_perm.end(), db_row_perm);
+  if (final_pos) std::copy(pl.final_pos.begin(), pl.final_pos.end(), final_pos);
+  if (final_order) std::copy(pl.final_order.begin(), pl.final_order.end(), final_order);
+  if (first_rows) std::copy(pl.first_rows.begin(), pl.first_rows.end(), first_rows);
+  if (part_k) {  // a constant band has K in every partition
+    if (pl.var_band) std::copy(pl.part_k.begin(), pl.part_k.end(), part_k);
+    else std::fill(part_k, part_k + pl.P, pl.K);
+  }
+  return SAP_OK;
+}
+
+}  // namespace
 }  // namespace sapb
+
+extern "C" int sap_reorder_host(int n, int nnz, const int* rp, const int* ci, const double* v, int num_partitions,
+                                const sap_options* opts, int prec_dtype, int threads, sap_reorder_info* info,
+                                int* db_row_perm, int* final_pos, int* final_order, int* first_rows, int* part_k) {
+  using namespace sapb;
+  if (n <= 0 || nnz < 0 || !rp || !ci || !v || !opts || !info || num_partitions < 1 ||
+      (prec_dtype != SAP_PREC_FLOAT && prec_dtype != SAP_PREC_DOUBLE)) {
+    set_last_error("invalid arguments to sap_reorder_host");
+    return SAP_ERR_INVALID_ARGUMENT;
+  }
+  if (rp[0] != 0 || rp[n] != nnz) {
+    set_last_error("row offsets inconsistent with nnz");
+    return SAP_ERR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < n; i++)
+    if (rp[i] > rp[i + 1]) {
+      set_last_error("row offsets not monotone");
+      return SAP_ERR_INVALID_ARGUMENT;
+    }
+  for (int e = 0; e < nnz; e++)
+    if (ci[e] < 0 || ci[e] >= n) {
+      set_last_error("column index out of range");
+      return SAP_ERR_INVALID_ARGUMENT;
+    }
+  const int saved = omp_get_max_threads();
+  if (threads > 0) omp_set_num_threads(threads);
+  int rc = SAP_OK;
+  try {
+    rc = prec_dtype == SAP_PREC_DOUBLE
+             ? reorder_host<double>(n, nnz, rp, ci, v, num_partitions, *opts, info, db_row_perm, final_pos,
+                                    final_order, first_rows, part_k)
+             : reorder_host<float>(n, nnz, rp, ci, v, num_partitions, *opts, info, db_row_perm, final_pos,
+                                   final_order, first_rows, part_k);
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    rc = e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    rc = SAP_ERR_INVALID_ARGUMENT;
+  }
+  if (threads > 0) omp_set_num_threads(saved);
+  return rc;
+}
