@@ -6,6 +6,8 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <cmath>
 #include <cstdlib>
 #include <string>
@@ -673,33 +675,12 @@ class WideBand {
   // x <- A_p^-1 x for the padded block vectors of all partitions.  L_ii^-1
   // and U_{i,i+1} = L_ii^-1 E_i are lower triangular, U_ii^-1 and
   // L_{i+1,i} = F_i U_ii^-1 upper triangular (the band fits in one block).
-  // lanes of the sweeps: up to SAPB_SWEEP_LANES (1, 2 or 4), with at least
-  // two partitions per lane; by default 4 for the FP16 copies (shorter
-  // launches: 2.96 against 3.09 ms per sweep on the 1M-row workload), 2 for
-  // FP32 / FP64 (3.95 against 4.18 ms with 4)
-  int sweep_lanes() const {
-    const char* e = std::getenv("SAPB_SWEEP_LANES");
-    const int dflt = h16 ? 4 : 2;
-    int want = e ? std::atoi(e) : dflt;
-    if (want != 1 && want != 2 && want != 4) want = dflt;
-    if (!st2) return 1;
-    while (want > 1 && P < 2 * want) want /= 2;
-    return want;
-  }
-  // Persistent sweeps (k_sweep, one cooperative launch per sweep), the
-  // default for the FP16 copies (1M-row workload: 2.77 ms per sweep against
-  // 3.10 with 4 lanes of per-step launches); the FP32 / FP64 sweeps stay on
-  // per-step launches (3.90 / 7.05 ms against 3.97 / 7.29 persistent).
-  // SAPB_SWEEP_PERSISTENT = 0 / 1 forces either.
+  // Persistent sweeps (k_sweep, one cooperative launch per sweep): group
+  // size G and column slices S per partition, scratch and barrier words.
   DBuf<T> pws;
   DBuf<unsigned> pctr, pbar;
   DBuf<int> perr;
   PinnedBuf<int> perr_h;
-  bool persistent_enabled() const {
-    const char* e = std::getenv("SAPB_SWEEP_PERSISTENT");
-    if (e) return std::atoi(e) != 0;
-    return h16;
-  }
   template <int V, typename MT>
   bool sweep_persistent(T* x, const MT* Li, const MT* Ui, const MT* Lo, const MT* Uo, const T* cL, const T* cU,
                         const T* cLo, const T* cUo) {
@@ -760,23 +741,23 @@ class WideBand {
     SAPB_CUDA(cudaStreamSynchronize(st));
     throw Error(SAP_ERR_DEVICE_TIMEOUT, "a block-sweep barrier wait ran out of its iteration limit");
   }
-  void solve_blocks(T* x) {
-    if (persistent_enabled()) {
+  // One block sweep in schedule `mode`: 0 persistent (k_sweep), 1 / 2 / 4
+  // lanes of per-step launches (fewer when a lane would get fewer than two
+  // partitions).  False when the persistent launch is not possible.
+  bool run_sweep(T* x, int mode) {
+    if (mode == 0) {
       if (h16) {
-        if constexpr (sizeof(T) == 4) {
-          if (sweep_persistent<8, __half>(x, Lh.get(), Uh.get(), Loh.get(), Uoh.get(), csL.get(), csU.get(),
-                                          csLo.get(), csUo.get()))
-            return;
-        }
-      } else {
-        constexpr int V = 16 / sizeof(T);
-        const bool vec = bs % V == 0;
-        if (vec && sweep_persistent<V, T>(x, Linv.get(), Uinv.get(), Loff.get(), Uoff.get(), nullptr, nullptr,
-                                          nullptr, nullptr))
-          return;
+        if constexpr (sizeof(T) == 4)
+          return sweep_persistent<8, __half>(x, Lh.get(), Uh.get(), Loh.get(), Uoh.get(), csL.get(), csU.get(),
+                                             csLo.get(), csUo.get());
+        return false;
       }
+      constexpr int V = 16 / sizeof(T);
+      return bs % V == 0 && sweep_persistent<V, T>(x, Linv.get(), Uinv.get(), Loff.get(), Uoff.get(), nullptr,
+                                                   nullptr, nullptr, nullptr);
     }
-    const int lanes = sweep_lanes();
+    int lanes = st2 ? mode : 1;
+    while (lanes > 1 && P < 2 * lanes) lanes /= 2;
     if (lanes > 1) {
       SAPB_CUDA(cudaEventRecord(ev_fork, st));
       for (int l = 1; l < lanes; l++) SAPB_CUDA(cudaStreamWaitEvent(lane_stream(l), ev_fork, 0));
@@ -790,6 +771,73 @@ class WideBand {
       SAPB_CUDA(cudaEventRecord(ev_lane[l], lane_stream(l)));
       SAPB_CUDA(cudaStreamWaitEvent(st, ev_lane[l], 0));
     }
+    return true;
+  }
+
+  // Sweep schedule autotuner, keyed on the layout (P, block size, blocks per
+  // partition, bytes per factor value): the first sweep of an unseen key
+  // times the candidate schedules (persistent, 2 lanes, 4 lanes; best of
+  // two runs each, CUDA events) on a copy of its right-hand side and keeps
+  // the fastest for the process.  Measured on the 1M-row workload: the
+  // persistent sweep for the FP16 copies (2.77 ms against 3.10 / 3.21 with 4
+  // / 2 lanes), 2 lanes for FP32 / FP64 (3.90 / 7.05 ms against 3.97 / 7.29
+  // persistent).  SAPB_SWEEP_PERSISTENT = 1 (or 0) and SAPB_SWEEP_LANES =
+  // 1 / 2 / 4 fix the schedule instead.
+  DBuf<T> tune_x;
+  static std::map<std::tuple<int, int, int, int>, int>& tuned() {
+    static std::map<std::tuple<int, int, int, int>, int> m;
+    return m;
+  }
+  static int fixed_mode() {
+    const char* pe = std::getenv("SAPB_SWEEP_PERSISTENT");
+    const char* le = std::getenv("SAPB_SWEEP_LANES");
+    int lanes = le ? std::atoi(le) : 0;
+    if (lanes != 1 && lanes != 2 && lanes != 4) lanes = 0;
+    if (pe && std::atoi(pe) != 0) return 0;
+    if (pe || lanes) return lanes ? lanes : 2;
+    return -1;
+  }
+  int tune_sweep(const T* x) {
+    const size_t len = (size_t)P * plen;
+    tune_x.ensure(len);
+    cudaEvent_t a = nullptr, b = nullptr;
+    SAPB_CUDA(cudaEventCreate(&a));
+    SAPB_CUDA(cudaEventCreate(&b));
+    int best = 2;
+    float best_ms = 1e30f;
+    for (int mode : {0, 2, 4}) {
+      if (mode == 4 && P < 8) continue;
+      float t = 1e30f;
+      bool ok = true;
+      for (int r = 0; r < 2 && ok; r++) {
+        SAPB_CUDA(cudaMemcpyAsync(tune_x.get(), x, len * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        SAPB_CUDA(cudaEventRecord(a, st));
+        ok = run_sweep(tune_x.get(), mode);
+        SAPB_CUDA(cudaEventRecord(b, st));
+        SAPB_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        SAPB_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (ok) t = std::min(t, ms);
+      }
+      if (ok && t < best_ms) {
+        best_ms = t;
+        best = mode;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    check_device();
+    return best;
+  }
+  void solve_blocks(T* x) {
+    int mode = fixed_mode();
+    if (mode < 0) {
+      const auto key = std::make_tuple(P, bs, nb, h16 ? 2 : (int)sizeof(T));
+      auto it = tuned().find(key);
+      if (it == tuned().end()) it = tuned().emplace(key, tune_sweep(x)).first;
+      mode = it->second;
+    }
+    if (!run_sweep(x, mode)) run_sweep(x, 2);
   }
 
   // the block sweeps of partitions [p0, p0+np) on one lane
