@@ -89,6 +89,16 @@ int partition_of(int r, int q, int rem) {
 
 }  // namespace
 
+// v resized to n (its memory kept across runs) with every element set to x,
+// in parallel
+template <typename V, typename X>
+V& pfill(V& v, size_t n, X x) {
+  if (v.size() != n) v.resize(n);
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < (long long)n; i++) v[i] = x;
+  return v;
+}
+
 // ---------------------------------------------------------------------------
 // DB (graph.h:1214-1361): maximum-product matching of rows to columns by
 // shortest augmenting paths, with row/column scaling from its dual values.
@@ -97,11 +107,12 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   // weight[e] = log(rowmax[row] / |a_e|), computed on the device
   const std::vector<int>& Rp = in_rp;
   const std::vector<int>& Ci = in_ci;
-  std::vector<double> u(n, 0.0), v(n, kInf);
-  std::vector<int> match(n, 0);
-  std::vector<int>& rev_match = ws_i0;
-  rev_match.assign(nnz, 0);
-  std::vector<char> row_done(n, 0), col_done(n, 0);
+  std::vector<double>& u = pfill(db_u, n, 0.0);
+  std::vector<double>& v = pfill(db_v, n, kInf);
+  std::vector<int>& match = pfill(db_match, n, 0);
+  std::vector<int>& rev_match = pfill(ws_i0, nnz, 0);
+  std::vector<char>& row_done = pfill(db_rowdone, n, (char)0);
+  std::vector<char>& col_done = pfill(db_coldone, n, (char)0);
   // initial duals: u = per-row minimum weight (reduce_by_key over CSR rows)
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
@@ -140,9 +151,12 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     if (!col_done[i]) v[i] = 0.0;
   }
   // augmenting paths (find_shortest_aug_path, graph.h:2043-2173)
-  std::vector<char> inB(n, 0), visited(n, 0);
-  std::vector<double> dist(n, kInf);
-  std::vector<int> Bset(n, 0), irn(n, 0), prev(n, 0);
+  std::vector<char>& inB = pfill(db_inb, n, (char)0);
+  std::vector<char>& visited = pfill(db_visited, n, (char)0);
+  std::vector<double>& dist = pfill(db_dist, n, kInf);
+  std::vector<int>& Bset = pfill(db_bset, n, 0);
+  std::vector<int>& irn = pfill(db_irn, n, 0);
+  std::vector<int>& prev = pfill(db_prev, n, 0);
   for (int start = 0; start < n; start++) {
     if (col_done[start]) continue;
     std::priority_queue<std::pair<int, double>, std::vector<std::pair<int, double>>, ByDist> heap;
@@ -245,20 +259,23 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
 // Symmetrised adjacency of edges [e0, e1) without self loops (duplicates
 // kept), rows [nb, ne] prefix-summed, entries stable (buildTopology,
 // graph.h:1764-1809).
+// obase: node x's range is off[x - obase]; 0 gives an array of n + 1 over
+// all nodes, nb one of ne - nb + 1 over the partition's nodes only.
 static void symmetric_adjacency(const std::vector<int>& er, const std::vector<int>& ec, int e0, int e1, int nb,
-                                int ne, int n, std::vector<int>& off, std::vector<int>& adj) {
+                                int ne, int n, std::vector<int>& off, std::vector<int>& adj, int obase = 0) {
   // each edge (r, c), r != c, contributes (r -> c) then (c -> r); a node's
   // neighbours keep the order of these contributions
-  off.assign(n + 1, 0);
+  off.assign(obase ? ne - nb + 1 : n + 1, 0);
+  auto o = [&](int x) -> int& { return off[x - obase]; };  // x in [nb, ne]
   for (int e = e0; e < e1; e++) {
     if (er[e] == ec[e]) continue;
-    off[er[e]]++;
-    off[ec[e]]++;
+    o(er[e])++;
+    o(ec[e])++;
   }
-  for (int i = nb + 1; i <= ne; i++) off[i] += off[i - 1];
-  for (int i = ne - 1; i >= nb; i--) off[i] = i > nb ? off[i - 1] : 0;  // exclusive starts
-  adj.resize(off[ne]);
-  std::vector<int> pos(off.begin() + nb, off.begin() + ne);
+  for (int i = nb + 1; i <= ne; i++) o(i) += o(i - 1);
+  for (int i = ne - 1; i >= nb; i--) o(i) = i > nb ? o(i - 1) : 0;  // exclusive starts
+  adj.resize(o(ne));
+  std::vector<int> pos(off.begin() + (nb - obase), off.begin() + (ne - obase));
   for (int e = e0; e < e1; e++) {
     const int r = er[e], c = ec[e];
     if (r == c) continue;
@@ -339,9 +356,10 @@ static void symmetric_adjacency_csr(int n, const std::vector<int>& rp, const std
 // children are queued in increasing `degree` order through a binary heap
 // (ties broken by the heap, as in the reference), restarts take the lowest
 // unvisited node.  Returns false when the queue cannot be refilled.
-static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& off, const std::vector<int>& adj,
+static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& offv, const std::vector<int>& adj,
                    const std::vector<int>* fixed_degree, std::vector<int>& pushed, std::vector<int>& level,
-                   std::vector<int>& order, int& last_level) {
+                   std::vector<int>& order, int& last_level, int obase = 0) {
+  auto off = [&](int x) { return offv[x - obase]; };  // node x's range starts at off(x) (see symmetric_adjacency)
   // FIFO as an array: every node enters at most once per trial
   std::vector<int> fifo((size_t)(ne - nb) + 2);
   size_t head = 0, tail = 0;
@@ -364,11 +382,11 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
     int node = fifo[head++];
     order[out++] = node;
     int lv = level[node];
-    for (int e = off[node]; e < off[node + 1]; e++) {
+    for (int e = off(node); e < off(node + 1); e++) {
       int t = adj[e];
       if (pushed[t] == trial) continue;
       pushed[t] = trial;
-      int deg = fixed_degree ? (*fixed_degree)[t] : off[t + 1] - off[t];
+      int deg = fixed_degree ? (*fixed_degree)[t] : off(t + 1) - off(t);
       kids.push(std::make_pair(t, deg));
       level[t] = lv + 1;
       last_level = lv + 1;
@@ -531,10 +549,14 @@ int Pipeline<T>::rcm() {
   std::vector<int>& adj = ws_adj;
   symmetric_adjacency_csr(n, m_rp, m_ci, off, adj, ws_cnt, ws_i1, ws_i2);
   rcm_order.resize(n);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) rcm_order[i] = i;
-  rcm_pos.assign(n, 0);
-  std::vector<char> tried(n, 0);
-  std::vector<int> pushed(n, -1), level(n, 0), order(n), claim(n, INT_MAX);
+  pfill(rcm_pos, n, 0);
+  std::vector<char>& tried = pfill(bfs_tried, n, (char)0);
+  std::vector<int>& pushed = pfill(bfs_pushed, n, -1);
+  std::vector<int>& level = pfill(bfs_level, n, 0);
+  std::vector<int>& order = pfill(bfs_order, n, 0);
+  std::vector<int>& claim = pfill(bfs_claim, n, INT_MAX);
   const int tracked_level = 0;  // never advanced (graph.h:1413-1414)
   for (int trial = 0; trial < 5; trial++) {
     int root;
@@ -780,9 +802,15 @@ void Pipeline<T>::second_level(int K, int P) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++)
     for (int e = d_rp[i]; e < d_rp[i + 1]; e++) row[e] = i;
-  second_order.assign(n, 0);
-  second_pos.assign(n, 0);
-  std::vector<int> order(n, 0);
+  pfill(second_order, n, 0);
+  pfill(second_pos, n, 0);
+  std::vector<int>& order = pfill(bfs_order, n, 0);
+  // the parallel pass keeps each partition's BFS state in the ranges of
+  // shared arrays (its trials never leave its nodes); the serial replay
+  // uses fresh whole-size arrays per partition
+  std::vector<char>& tried_sh = pfill(bfs_tried, n, (char)0);
+  std::vector<int>& pushed_sh = pfill(bfs_pushed, n, -1);
+  std::vector<int>& level_sh = pfill(bfs_level, n, 0);
   std::vector<int> pnb(P + 1, 0);
   for (int p = 0; p < P; p++) pnb[p + 1] = pnb[p] + q + (p < rem ? 1 : 0);
   // One partition.  Returns false, in the parallel pass, when a trial root
@@ -796,11 +824,20 @@ void Pipeline<T>::second_level(int K, int P) {
     int best_bw = 0;
     for (int e = e0; e < e1; e++) best_bw = std::max(best_bw, std::abs(row[e] - d_ci[e]));
     std::vector<int> off, adj;
-    symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj);
+    const int obase = serial ? 0 : nb;
+    symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj, obase);
     std::vector<int> rowlen(ne - nb);
     for (int i = nb; i < ne; i++) rowlen[i - nb] = d_rp[i + 1] - d_rp[i];
-    std::vector<char> tried(n, 0);
-    std::vector<int> pushed(n, -1), level(n, 0);
+    std::vector<char> tried_own;
+    std::vector<int> pushed_own, level_own;
+    if (serial) {
+      tried_own.assign(n, 0);
+      pushed_own.assign(n, -1);
+      level_own.assign(n, 0);
+    }
+    std::vector<char>& tried = serial ? tried_own : tried_sh;
+    std::vector<int>& pushed = serial ? pushed_own : pushed_sh;
+    std::vector<int>& level = serial ? level_own : level_sh;
     int last_level = 0, prev_last = 0;
     for (int trial = 0; trial < 5; trial++) {
       int root;
@@ -817,11 +854,15 @@ void Pipeline<T>::second_level(int K, int P) {
         } else {
           root = (int)(std::max_element(level.begin() + nb, level.begin() + ne) - level.begin());
         }
-        while (tried[root]) root = (root + 1) % n;
+        if (serial) {
+          while (tried[root]) root = (root + 1) % n;
+        } else {  // the same walk, ending at the partition's end
+          while (root < ne && tried[root]) root++;
+        }
       }
       if (!serial && (root < nb || root >= ne)) return false;
       tried[root] = 1;
-      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level)) break;
+      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level, obase)) break;
       for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
       int bw = 0;
       for (int e = e0; e < e1; e++) bw = std::max(bw, std::abs(second_pos[row[e]] - second_pos[d_ci[e]]));

@@ -61,6 +61,13 @@ class Pipeline {
   // its memory instead of allocating and page-faulting it again)
   std::vector<int> ws_i0, ws_i1, ws_i2, ws_off, ws_adj, ws_cnt, tmp_rp, tmp_ci;
   std::vector<T> ws_t0, tmp_val;
+  // per-node state of the DB search and of the BFS trials (refilled in
+  // parallel by every run)
+  std::vector<double> db_u, db_v, db_dist;
+  std::vector<int> db_match, db_bset, db_irn, db_prev;
+  std::vector<char> db_rowdone, db_coldone, db_inb, db_visited;
+  std::vector<char> bfs_tried;
+  std::vector<int> bfs_pushed, bfs_level, bfs_order, bfs_claim;
 
   // wall time of the stages of run(), in order (ms)
   std::vector<std::pair<const char*, double>> stage_ms;
