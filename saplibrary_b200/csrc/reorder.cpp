@@ -123,8 +123,12 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   // greedy initial matching (init_reduced_cval, graph.h:1890-1918): every
   // column's smallest reduced weight and its entry are independent of the
   // others (parallel); the claims are then made in column order
+  // (each column's best entry and that entry's row, so that the ordered
+  // claims below read sequential arrays)
   std::vector<int>& best_e = ws_i1;
-  best_e.assign(n, -1);
+  std::vector<int>& best_r = ws_i2;
+  best_e.resize(n);
+  best_r.resize(n);
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     int best = -1;
@@ -136,16 +140,18 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     }
     v[i] = vi;
     best_e[i] = best;
+    best_r[i] = best >= 0 ? Ci[best] : -1;
   }
   for (int i = 0; i < n; i++) {
-    const int best = best_e[i];
-    if (best >= 0 && !row_done[Ci[best]]) {
+    const int r = best_r[i];
+    if (r >= 0 && !row_done[r]) {
       col_done[i] = 1;
-      row_done[Ci[best]] = 1;
-      match[Ci[best]] = i;
-      rev_match[i] = best;
+      row_done[r] = 1;
+      match[r] = i;
+      rev_match[i] = best_e[i];
     }
   }
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     if (!row_done[i]) u[i] = 0.0;
     if (!col_done[i]) v[i] = 0.0;
@@ -245,6 +251,7 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     row_scale[i] = std::exp(v[i]) / rowmax[i];
   }
   db_row_perm.resize(n);
+#pragma omp parallel for schedule(static)
   for (int c = 0; c < n; c++) db_row_perm[match[c]] = c;
   // permuted (and scaled) matrix, rows in the new order, entries stable
   std::vector<T>& val = ws_t0;
@@ -577,6 +584,7 @@ int Pipeline<T>::rcm() {
     }
     tried[root] = 1;
     if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, ws_i2)) break;
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
     int bw = 0;
 #pragma omp parallel for reduction(max : bw) schedule(static)
@@ -588,6 +596,7 @@ int Pipeline<T>::rcm() {
     if (trial > 0) break;            // tracked level never grows: the second trial is the last
     if (best_bw <= 256) break;       // BANDWIDTH_THRESHOLD
   }
+#pragma omp parallel for schedule(static)
   for (int k = 0; k < n; k++) rcm_pos[rcm_order[k]] = k;
   tmp_rp.swap(m_rp);
   tmp_ci.swap(m_ci);
