@@ -66,7 +66,9 @@ template <typename V>
 void permute_rows(int n, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<V>& val,
                   const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
                   std::vector<int>& out_ci, std::vector<V>& out_val) {
-  out_rp.assign(n + 1, 0);
+  out_rp.resize(n + 1);
+  out_rp[0] = 0;
+#pragma omp parallel for schedule(static)
   for (int r = 0; r < n; r++) out_rp[newpos[r] + 1] = rp[r + 1] - rp[r];
   for (int i = 0; i < n; i++) out_rp[i + 1] += out_rp[i];
   out_ci.resize(ci.size());
