@@ -83,3 +83,33 @@ def test_structurally_singular_matrix_is_reported():
     r = 7  # zero out one whole row: no matching can cover it
     v[rp[r]:rp[r + 1]] = 0.0
     check_against_oracle(rp, ci, v, 4, "double", 0.0, 3)
+
+
+def random_sparse(n, seed, band=40, extra=3, far=0.02):
+    """A nonsymmetric sparse pattern: a random band around the diagonal,
+    `extra` random entries per row at any distance, some far outliers; a
+    dominant diagonal keeps the DB matching well defined."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        k = rng.integers(1, 6)
+        cs = set(np.clip(i + rng.integers(-band, band + 1, size=k), 0, n - 1).tolist())
+        cs |= set(rng.integers(0, n, size=extra).tolist()) if rng.random() < 0.5 else set()
+        if rng.random() < far:
+            cs.add(int(rng.integers(0, n)))
+        cs.add(i)
+        for c in sorted(cs):
+            rows.append(i)
+            cols.append(c)
+            vals.append(10.0 if c == i else float(rng.uniform(-1, 1)))
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, np.asarray(rows) + 1, 1)
+    return np.cumsum(rp).astype(np.int32), np.asarray(cols, np.int32), np.asarray(vals)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+@pytest.mark.parametrize("dtype", ["float", "double"])
+def test_random_patterns_match_oracle(seed, dtype):
+    rp, ci, v = random_sparse(3000 + 517 * seed, seed)
+    for P, drop, threads in ((4, 0.0, 1), (7, 1e-3, 6), (12, 1e-2, 3)):
+        check_against_oracle(rp, ci, v, P, dtype, drop, threads)
