@@ -529,14 +529,16 @@ __device__ __forceinline__ bool group_barrier(unsigned* cnt, unsigned* gen, unsi
 // each other.  Factor blocks: L_ii^-1 at Li + (p nb + i) BB, L_{i+1,i} at
 // Lo + (p (nb-1) + i) BB, likewise U; their column scales (FP16 copies) at
 // cs* + (block index) bs.  bar holds 2 words per partition; err is raised by
-// a barrier that timed out (the kernel then returns).
+// a barrier that timed out (the kernel then returns).  stall > 0 makes every
+// group barrier wait for that many CTAs more than the group has, so that the
+// bounded wait runs out (tests of the timeout path only).
 template <typename T, int VEC, typename MT>
 __global__ void __launch_bounds__(kGemvWarps * 32, 3) k_sweep(const MT* __restrict__ Li, const MT* __restrict__ Ui,
                                                               const MT* __restrict__ Lo, const MT* __restrict__ Uo,
                                                               const T* csL, const T* csU, const T* csLo, const T* csUo,
                                                               T* x, T* y, T* t, int nb, int bs, long long BB,
                                                               long long plen, int G, int S, T* ws, unsigned* ctr,
-                                                              unsigned* bar, int* err) {
+                                                              unsigned* bar, int* err, int stall) {
   constexpr int R = 32 * (VEC > 1 ? VEC : 2);
   __shared__ T part[kGemvWarps][R];
   __shared__ unsigned last_cta;
@@ -591,7 +593,7 @@ __global__ void __launch_bounds__(kGemvWarps * 32, 3) k_sweep(const MT* __restri
     for (int it = g; it < items; it += G)
       tgemv_item<T, VEC, MT, true>(it / S, p, S, it % S, A, bs, xv, cv, yv, bs, mode, tri, ws, ctr, cs, part,
                                    last_cta);
-    if (!group_barrier(bar + 2 * p, bar + 2 * p + 1, (unsigned)G, err)) return;
+    if (!group_barrier(bar + 2 * p, bar + 2 * p + 1, (unsigned)(G + stall), err)) return;
   }
 }
 

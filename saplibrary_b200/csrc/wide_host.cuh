@@ -721,9 +721,14 @@ class WideBand {
     int* err = perr.get();
     int nbv = nb, bsv = bs;
     long long BBv = BB, plenv = plen;
+    // SAPB_TEST_BARRIER_STALL = 1: every group barrier waits for one CTA
+    // more than exists, so that its bounded wait runs out and the error path
+    // is taken (tests only)
+    const char* se = std::getenv("SAPB_TEST_BARRIER_STALL");
+    int stall = (se && std::atoi(se) == 1) ? 1 : 0;
     void* args[] = {(void*)&Li, (void*)&Ui, (void*)&Lo, (void*)&Uo, (void*)&cL, (void*)&cU, (void*)&cLo, (void*)&cUo,
                     (void*)&x, (void*)&y, (void*)&t, (void*)&nbv, (void*)&bsv, (void*)&BBv, (void*)&plenv, (void*)&G,
-                    (void*)&S, (void*)&ws, (void*)&ctr, (void*)&bar, (void*)&err};
+                    (void*)&S, (void*)&ws, (void*)&ctr, (void*)&bar, (void*)&err, (void*)&stall};
     SAPB_CUDA(cudaLaunchCooperativeKernel((const void*)kern, dim3((unsigned)(P * G)), dim3(kGemvWarps * 32), args, 0,
                                           st));
     count_launch();

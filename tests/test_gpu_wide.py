@@ -259,3 +259,26 @@ def test_persistent_sweep_matches_launch_chain(monkeypatch, prec, tol):
     z0 = apply_gpu(s, v)
     assert np.all(np.isfinite(z1))
     assert np.linalg.norm(z1 - z0) / np.linalg.norm(z0) <= tol
+
+
+def test_persistent_sweep_barrier_timeout_is_reported(monkeypatch):
+    # a group barrier made to wait for one CTA more than its group has (a
+    # count nothing completes): its bounded wait runs out, the kernel
+    # returns, the host reports SAP_ERR_DEVICE_TIMEOUT, and the next apply
+    # works again
+    n, K, P = 24011, 257, 5
+    band = sap.generate_band_host(n, K, 0.8, 2, seed=n + K)
+    A = sap.BandedMatrix.from_array(band, n, K)
+    s = sap.Solver(P, sap.Options(performReorder=False, variableBandwidth=False, applyScaling=False,
+                                  factMethod=sap.LU_only), prec="tf32_f16")
+    s.setup(A)
+    v = np.random.default_rng(6).standard_normal(n)
+    monkeypatch.setenv("SAPB_SWEEP_PERSISTENT", "1")
+    z_ok = apply_gpu(s, v)
+    monkeypatch.setenv("SAPB_TEST_BARRIER_STALL", "1")
+    with pytest.raises(sap.LibraryError) as ei:
+        apply_gpu(s, v)
+    assert ei.value.code == -104  # SAP_ERR_DEVICE_TIMEOUT
+    monkeypatch.delenv("SAPB_TEST_BARRIER_STALL")
+    z_again = apply_gpu(s, v)
+    assert np.linalg.norm(z_again - z_ok) / np.linalg.norm(z_ok) <= 1e-6
