@@ -23,6 +23,7 @@
 
 namespace sapb {
 
+// Granularity (rows) of the block sizes and of the recursion's splits.
 constexpr int kLeaf = 32;
 
 // COO entries of the diagonal blocks (row j, col l in band order) into the
