@@ -306,6 +306,7 @@ class WideBand {
       if (x) cudaStreamDestroy(x);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_half) cudaEventDestroy(ev_half);
     for (cudaEvent_t e : ev_lane)
       if (e) cudaEventDestroy(e);
   }
@@ -361,10 +362,14 @@ class WideBand {
       csLo.alloc((size_t)(no * bs));
       csUo.alloc((size_t)(no * bs));
     }
+    // on the second stream, beside the spike products that follow on st
+    // (both only read the factors); the apply and the next setup wait for it
+    SAPB_CUDA(cudaEventRecord(ev_fork, st));
+    SAPB_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
     constexpr int R = tgemv_rows<T, 8>();  // rows per tile of the FP16 sweep kernel
     auto conv = [&](const T* A, __half* H, T* cs, long long nblk, int tri) {
       if (nblk <= 0) return;
-      k_blocks_to_half<T, R><<<dim3((bs + 7) / 8, (unsigned)nblk), 256, 0, st>>>(A, H, cs, bs, BB, tri);
+      k_blocks_to_half<T, R><<<dim3((bs + 7) / 8, (unsigned)nblk), 256, 0, st2>>>(A, H, cs, bs, BB, tri);
       SAPB_LAUNCHED();
     };
     conv(Linv.get(), Lh.get(), csL.get(), nd, 1);
@@ -373,6 +378,17 @@ class WideBand {
       conv(Loff.get(), Loh.get(), csLo.get(), no, 2);
       conv(Uoff.get(), Uoh.get(), csUo.get(), no, 1);
     }
+    SAPB_CUDA(cudaEventRecord(ev_half, st2));
+    half_pending = true;
+  }
+  cudaEvent_t ev_half = nullptr;
+  bool half_pending = false;
+  // st waits for the FP16 conversion (before an apply reads the copies or a
+  // setup overwrites the factors)
+  void wait_half() {
+    if (!half_pending) return;
+    SAPB_CUDA(cudaStreamWaitEvent(st, ev_half, 0));
+    half_pending = false;
   }
   // recursion cut-off of the spike slab products: structure-aware for the
   // compute-bound FP64 / FP32 products (FP64 spikes 0.99 -> 0.62 s on the
@@ -427,7 +443,9 @@ class WideBand {
       SAPB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
       for (cudaStream_t& x : st_more) SAPB_CUDA(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
       for (cudaEvent_t& e : ev_lane) SAPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      SAPB_CUDA(cudaEventCreateWithFlags(&ev_half, cudaEventDisableTiming));
     }
+    wait_half();
     cublas_check(cublasSetStream(h, st), "cublasSetStream");
     if (cublas_ws.size() == 0) cublas_ws.alloc((size_t)64 << 20);
     cublas_check(cublasSetWorkspace(h, cublas_ws.get(), cublas_ws.size()), "cublasSetWorkspace");
@@ -1093,6 +1111,7 @@ class WideBand {
   // correction, partition solves, rightTrans scatter (sout/cout).  The
   // permutation arguments are null for a matrix used in its own order.
   void apply(const double* v, double* z, const int* gin, const T* sin, const int* sout, const T* cout) {
+    wait_half();
     const dim3 gb(grid1d(plen, 256, 1024), P);
     k_wb_in<T><<<grid1d(n), 256, 0, st>>>(v, gin, sin, Fb.get(), n);
     SAPB_LAUNCHED();
