@@ -28,3 +28,19 @@ def test_ensemble_generator_shapes_and_seeds():
         assert K in (8, 16) and 2000 <= len(b) <= 8000 and band.size == len(b) * (2 * K + 1)
     again = ensemble.make_ensemble(12, seed=4, n_min=2000, n_max=8000, ks=(8, 16))
     assert all(np.array_equal(a, c) for a, c in zip(bands, again[0]))
+
+
+def test_sweep_bytes_counts_triangles_vectors_and_scales():
+    # algorithmic bytes of one block sweep (the roofline numerator)
+    import bench
+    bs, nb, P = 64, 3, 2
+    tri = bs * (bs + 1) // 2
+    mats = (4 * nb - 2) * tri
+    vecs = (4 * nb - 2) * 2 * bs + (2 * nb - 2) * bs
+    assert bench.sweep_bytes(bs, nb, P, 4) == P * (mats + vecs) * 4
+    assert bench.sweep_bytes(bs, nb, P, 8) == P * (mats + vecs) * 8
+    # FP16 copies: 2-byte factor values, FP32 vectors and one FP32 scale per column
+    assert bench.sweep_bytes(bs, nb, P, 2) == P * (mats * 2 + vecs * 4 + (4 * nb - 2) * bs * 4)
+    # the full-size workload's FP16 sweep reads about half of the FP32 one
+    r = bench.sweep_bytes(3168, 20, 16, 2) / bench.sweep_bytes(3168, 20, 16, 4)
+    assert 0.5 < r < 0.51
