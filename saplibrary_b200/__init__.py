@@ -464,7 +464,12 @@ class SpmvCusp(_Spmv):
 
 # ---- Solver ------------------------------------------------------------------------
 class Solver:
-    """sap::Solver<Array, PrecValueType> (sap/solver.h:153-225)."""
+    """sap::Solver<Array, PrecValueType> (sap/solver.h:153-225).
+
+    prec: the preconditioner's value type, "float" or "double" as the
+    reference's PrecValueType, or the extensions "tf32" (FP32 storage, wide
+    bands factored with TF32 tensor-core products) and "tf32_f16" (as "tf32",
+    with FP16 block-scaled copies of the factor blocks for the sweeps)."""
 
     def __init__(self, numPartitions: int, opts: Options, prec: str = "float"):
         self._opts = opts
