@@ -113,3 +113,19 @@ def test_random_patterns_match_oracle(seed, dtype):
     rp, ci, v = random_sparse(3000 + 517 * seed, seed)
     for P, drop, threads in ((4, 0.0, 1), (7, 1e-3, 6), (12, 1e-2, 3)):
         check_against_oracle(rp, ci, v, P, dtype, drop, threads)
+
+
+def test_invalid_csr_is_rejected():
+    rp, ci, v, _ = convection_diffusion_csr(m=10, fill_reach=30, seed=1)
+    bad_ci = ci.copy()
+    bad_ci[5] = len(rp) + 3  # column out of range
+    with pytest.raises(sap.LibraryError) as ei:
+        sap.reorder_host(rp, bad_ci, v, 2)
+    assert ei.value.code == -100 and "column index" in str(ei.value)
+    bad_rp = rp.copy()
+    bad_rp[3], bad_rp[4] = bad_rp[4], bad_rp[3]  # not monotone
+    with pytest.raises(sap.LibraryError) as ei:
+        sap.reorder_host(bad_rp, ci, v, 2)
+    assert ei.value.code == -100
+    with pytest.raises(ValueError):
+        sap.reorder_host(rp, ci, v, 2, prec="tf32")
