@@ -10,12 +10,22 @@ Solver::setup(A) (DB matching, RCM, drop-off, second-level reordering,
 variable band, partition block LU, spike tips, reduced system) followed by
 Solver::solve(spmv, b, x) from x = 0 (sap/solver.h:339-562).
 
-Two forms are timed by default: the headline precision form (FP32
+Forms timed on it by default: the headline precision form (FP32
 preconditioner whose wide-band block products run on the tensor cores in
-TF32, inside flexible GMRES(50) with FP64 Arnoldi) and the plain FP64 form
-(FP64 preconditioner, the reference's BiCGStab(2)).  A third form
-(tf32_refine: the TF32 preconditioner with FP64 refinement sweeps around
-BiCGStab(2)) can be selected with --forms.
+TF32, FP16 block-scaled sweeps, inside flexible GMRES(50) with FP64
+Arnoldi), the same with FP32 sweeps, and the plain FP64 form (FP64
+preconditioner, the reference's BiCGStab(2)).  A further form (tf32_refine:
+the TF32 preconditioner with FP64 refinement sweeps around BiCGStab(2)) can
+be selected with --forms.
+
+Beside it (key "banded"), the banded workloads: N = 2,000,000, K = 200,
+N(0,1) off-diagonals, dominance 0.8, P = 32, and the reference's banded
+preset N = 200,000, K = 50, U[-1,1], dominance 1.0, P = 10 (both LU_UL,
+x_true = ones), each in plain FP64 + BiCGStab(2), TF32 + FGMRES and FP32 +
+FGMRES.  cpu_baseline is a complete, measured CPU oracle solve of the 2M-row
+banded workload (key "cpu_complete": both banded workloads); the reference
+arm (--impl reference) reports itself unavailable, because one complete CPU
+solve of the 1M-row sparse workload takes tens of minutes.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -49,8 +59,6 @@ FORMS = {
 }
 HEADLINE = "tf32f16_fgmres"
 DEFAULT_FORMS = "tf32f16_fgmres,tf32_fgmres,fp64"
-# rows of the CPU band-LU timing sample (about 5 s at K ~ 3000)
-LU_SAMPLE_ROWS = 400
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) over the
 # algorithmic bytes of one block-sweep k_tgemv launch, measured with ncu on
 # this workload at grid side 310 (block size 3168, the FP32 block size at
@@ -149,8 +157,19 @@ def rank_seed(rank: int) -> int:
     return 1 + rank
 
 
+def problems():
+    """saplibrary_b200/problems.py loaded by path: the generators need numpy
+    only, and importing the package would load the CUDA library (the CPU
+    reference arm must not)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_sap_problems", os.path.join(ROOT, "saplibrary_b200", "problems.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def make_problem(seed: int):
-    from saplibrary_b200.problems import convection_diffusion_csr
+    convection_diffusion_csr = problems().convection_diffusion_csr
     w = WORKLOAD
     rp, ci, v, _ = convection_diffusion_csr(m=w["m"], conv=w["conv"], fill_per_row=w["fill_per_row"],
                                             fill_reach=w["fill_reach"], fill_mag=w["fill_mag"], seed=seed)
@@ -158,66 +177,67 @@ def make_problem(seed: int):
     return rp, ci, v, b
 
 
-def cpu_reference_sample(rp, ci, v, applies: float):
-    """Time-to-solution of the CPU oracle (the reference's algorithm restated)
-    for this workload, from a bounded sample: the full reordering (DB, RCM,
-    drop-off, coupling blocks, second level) is run and timed; the partition
-    band LU is timed on its first LU_SAMPLE_ROWS pivots at the workload's K
-    and scaled to the rows every core factors (partitions in parallel over
-    the host threads); the spike tips are costed as 3 band sweeps of K
-    right-hand sides per interface (3 x the LU's n_p K^2) and every
-    preconditioner apply as 4 triangular band sweeps (4 n K)."""
+# Banded workloads timed beside the headline: the mixed-precision wide band
+# (N = 2,000,000, K = 200, N(0,1) off-diagonals, dominance 0.8, P = 32) and
+# the reference's banded preset (N = 200,000, K = 50, U[-1,1], dominance 1.0,
+# P = 10); both LU_UL on a constant band without reordering, x_true = ones,
+# b = A x_true, solved from x = 0 to FP64 relative residual 1e-10.
+BANDED = {
+    "band_n2000000_k200": dict(n=2_000_000, k=200, d=0.8, dist=2, P=32, seed=1),
+    "band_n200000_k50": dict(n=200_000, k=50, d=1.0, dist=1, P=10, seed=1),
+}
+BANDED_FORMS = {
+    "fp64_bicgstab2": dict(prec="double", solver="BiCGStab2"),
+    "tf32_fgmres": dict(prec="tf32", solver="FGMRES"),
+    "f32_fgmres": dict(prec="float", solver="FGMRES"),
+}
+# the largest workload whose complete CPU oracle run fits the bench (about a
+# minute on 16 host threads); the 1M-row sparse workload takes tens of
+# minutes (its FP64 band LU alone runs at ~7 ms per pivot row at K = 3010)
+CPU_BASELINE_WORKLOAD = "band_n2000000_k200"
+REFERENCE_UNAVAILABLE = (
+    "a complete CPU time-to-solution of the 1M-row sparse workload takes tens of minutes per step (the reference "
+    "has no CPU preconditioner path; the restated FP64 band LU alone runs at ~7 ms per pivot row at K=3010, ~7 min "
+    "for each partition's 62,500 rows), beyond the bench's minutes; complete measured CPU runs of the 2M-row K=200 "
+    "and 200k-row K=50 banded workloads are in the GPU arm's cpu_baseline and cpu_complete")
+
+
+def cpu_complete_banded(name: str, band: np.ndarray):
+    """One complete CPU solve of a banded workload by the oracle (the
+    reference's algorithm restated, sap/solver.h:339-562 with the banded
+    preset of examples/synthetic_banded/driver_banded.cu:166-170): band
+    conversion, partition LU/UL, spike tips, reduced system, then
+    BiCGStab(2) with the FP64 preconditioner to relative residual 1e-10, on
+    all host threads (partitions in parallel).  Nothing is sampled or scaled:
+    the value is the measured wall time of the whole solve."""
     import oracle
-    w = WORKLOAD
+    c = BANDED[name]
+    n, k = c["n"], c["k"]
+    b = oracle.spmv_banded(band, n, k, np.ones(n))
     t0 = time.perf_counter()
-    o = oracle.SparsePrecond(w["P"], dtype="double", dropFrac=w["drop"])
-    rc = o.setup(rp, ci, v, factor=False, band=False)
-    t_reorder = time.perf_counter() - t0
+    pc = oracle.Precond(c["P"], fact=1, dtype="double")
+    rc = pc.setup_banded(band, n, k)
+    t1 = time.perf_counter()
     if rc != 0:
-        raise RuntimeError(f"oracle reordering failed: {o.message}")
-    info = o.info()
-    K, P, n = info.K, info.P, info.n
-    t_lu = oracle.band_lu_sample(K, LU_SAMPLE_ROWS)
-    per_row = t_lu / LU_SAMPLE_ROWS
-    cores = oracle.num_threads()
-    rows_per_core = math.ceil(n / P) * math.ceil(P / cores)
-    t_factor = per_row * rows_per_core
-    t_spikes = 3.0 * t_factor
-    t_solve = per_row * rows_per_core * 4.0 * applies / K
-    total = t_reorder + t_factor + t_spikes + t_solve
-    sample = (f"full oracle reordering ({t_reorder:.2f} s) + FP64 band LU of {LU_SAMPLE_ROWS} pivots at K={K} "
-              f"({per_row * 1e3:.2f} ms/row) scaled to {rows_per_core} rows per core (P={P}, {cores} threads); "
-              f"spike tips costed as 3x the LU, {applies:.0f} applies as 4nK each")
-    parts = {"reorder_s": t_reorder, "factor_s": t_factor, "spikes_s": t_spikes, "solve_s": t_solve}
-    return total, cores, sample, parts, K
+        raise RuntimeError(f"oracle setup failed on {name}: status {rc}")
+    x, res = pc.solve(b, band=band, K=k, L=2, maxit=100, reltol=1e-10)
+    t2 = time.perf_counter()
+    return {"value": t2 - t0, "unit": "s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"complete solve of {name} (setup {t1 - t0:.2f} s + BiCGStab(2) {t2 - t1:.2f} s, "
+                      f"{res.iterations} iterations, relres {res.rel_res_norm:.2e}), FP64 preconditioner, "
+                      f"{oracle.num_threads()} host threads",
+            "setup_s": t1 - t0, "solve_s": t2 - t1, "iterations": res.iterations, "monitor_code": res.code,
+            "rel_residual": res.rel_res_norm, "err_vs_exact": float(np.linalg.norm(x - 1.0) / math.sqrt(n))}, x
 
 
 def run_reference(args, ws, rank):
-    """--impl reference: the oracle port of the reference's CPU path, timed on
-    a bounded sample of the workload per step (see cpu_reference_sample)."""
+    """--impl reference: the CPU path of the reference (restated by the
+    oracle) cannot finish one complete solve of this workload within the
+    bench, and a sampled-and-scaled time is not a measured time-to-solution,
+    so the arm reports itself unavailable with the reason."""
     if rank != 0:
         return
-    rp, ci, v, _ = make_problem(seed=1)
-    applies = 4 * 7.75  # BiCGStab(2) iterations of the plain FP64 form on this workload, 4 applies each
-    for _ in range(args.warmup):
-        cpu_reference_sample(rp, ci, v, applies)
-    vals = []
-    cores, sample, parts, K = 0, "", {}, 0
-    for _ in range(args.steps):
-        t, cores, sample, parts, K = cpu_reference_sample(rp, ci, v, applies)
-        vals.append(t)
-    t = float(np.mean(vals))
-    line = {
-        "impl": "reference", "metric": "time_to_solution", "value": t, "unit": "s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD["name"], "preconditioner": "fp64", "krylov": "BiCGStab2",
-                   "rel_tol": WORKLOAD["relTol"]},
-        "cpu_baseline": {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "parts": parts, "K": K,
-    }
-    print(json.dumps(line), flush=True)
+    print(json.dumps({"impl": "reference", "unavailable": REFERENCE_UNAVAILABLE}), flush=True)
 
 
 def sweep_bytes(bs: int, nb: int, P: int, vbytes: int) -> int:
@@ -235,6 +255,62 @@ def sweep_bytes(bs: int, nb: int, P: int, vbytes: int) -> int:
     return P * (mats + vecs) * vbytes
 
 
+def time_banded(sap, torch, name: str, warm: int, steps: int, ws: int) -> dict:
+    """GPU time-to-solution of every banded form on one banded workload:
+    one step = Solver::setup(A) + solve(spmv, b, x) from x = 0, timed with
+    CUDA events on the solver stream.  Also the error against the exact
+    solution (ones) and the FP64 form's solution (key _x, for the comparison
+    with the CPU oracle's)."""
+    c = BANDED[name]
+    n, k = c["n"], c["k"]
+    A = sap.BandedMatrix(n, k, c["d"], dist=c["dist"], seed=c["seed"])
+    spmv = sap.MVBanded(A)
+    ones = torch.ones(n, dtype=torch.float64, device="cuda")
+    b = torch.empty_like(ones)
+    spmv(ones, b)
+    x = torch.zeros_like(b)
+    out = {"n": n, "K": k, "P": c["P"], "dominance": c["d"], "values": "N(0,1)" if c["dist"] == 2 else "U[-1,1]"}
+    for form, f in BANDED_FORMS.items():
+        opts = sap.Options(solverType=getattr(sap, f["solver"]), performReorder=False, variableBandwidth=False,
+                           applyScaling=False, factMethod=sap.LU_UL, relTol=1e-10, maxNumIterations=400)
+        solver = sap.Solver(c["P"], opts, prec=f["prec"])
+        stream = torch.cuda.ExternalStream(solver.stream())
+
+        def step():
+            solver.setup(A)
+            x.zero_()
+            return solver.solve(spmv, b, x)
+
+        ok = all([step() for _ in range(warm)])
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            ok = step() and ok
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        st = solver.getStats()
+        r = torch.empty_like(b)
+        spmv(x, r)
+        out[form] = {"tts_s": max_over_ranks(ev0.elapsed_time(ev1) / steps / 1e3, ws), "steps": steps, "ok": bool(ok),
+                     "monitor_code": solver.getMonitorCode(), "iterations": st.numIterations,
+                     "true_rel_residual": float(torch.linalg.norm(b - r) / torch.linalg.norm(b)),
+                     "err_vs_exact": float(torch.linalg.norm(x - ones) / math.sqrt(n)),
+                     "setup_ms": round(st.timeSetup, 2), "solve_ms": round(st.timeSolve, 2),
+                     "block_size": solver.blockLayout()[0]}
+        if form == "fp64_bicgstab2":
+            out["_x"] = x.cpu().numpy().copy()
+        del solver, stream
+        torch.cuda.empty_cache()
+    if "fp64_bicgstab2" in out:
+        base = out["fp64_bicgstab2"]["tts_s"]
+        out["speedup_vs_plain_fp64"] = {f: base / out[f]["tts_s"] for f in BANDED_FORMS if f in out}
+    del A, spmv
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -245,6 +321,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--forms", default=DEFAULT_FORMS, help="comma-separated forms to time (" + ", ".join(FORMS) + ")")
     ap.add_argument("--m", type=int, default=WORKLOAD["m"], help="grid side (profiler captures only)")
+    ap.add_argument("--banded", default=",".join(BANDED),
+                    help="banded workloads timed beside the headline (" + ", ".join(BANDED) + "; empty: none)")
     args = ap.parse_args()
     set_grid(args.m)
     ws, rank, local = dist_init()
@@ -401,11 +479,26 @@ def main():
         "clocks": clocks,
         "forms": results,
     }
+    # ---- banded workloads: GPU forms, then the complete CPU oracle runs ----------
+    banded = [b for b in args.banded.split(",") if b]
+    if banded:
+        line["banded"] = {name: time_banded(sap, torch, name, warm, min(args.steps, 3), ws) for name in banded}
     if rank == 0 and not args.no_cpu_baseline:
-        applies = 4 * results["fp64"]["iterations"] if "fp64" in results else 31.0
-        t, cores, sample, parts, _ = cpu_reference_sample(rp, ci, v, applies)
-        line["cpu_baseline"] = {"value": t, "unit": "s", "cores": cores, "kind": "port", "sample": sample,
-                                "parts": parts}
+        cpu_runs = {}
+        for name in banded:
+            c = BANDED[name]
+            band = sap.generate_band_host(c["n"], c["k"], c["d"], c["dist"], seed=c["seed"])
+            run, xo = cpu_complete_banded(name, band)
+            del band
+            gx = line["banded"][name].get("_x")
+            if gx is not None:
+                run["gpu_fp64_x_vs_cpu_x"] = float(np.linalg.norm(gx - xo) / np.linalg.norm(xo))
+            cpu_runs[name] = run
+        if CPU_BASELINE_WORKLOAD in cpu_runs:
+            line["cpu_baseline"] = dict(cpu_runs[CPU_BASELINE_WORKLOAD], workload=CPU_BASELINE_WORKLOAD)
+        line["cpu_complete"] = cpu_runs
+    for name in banded:
+        line["banded"][name].pop("_x", None)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

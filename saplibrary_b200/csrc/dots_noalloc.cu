@@ -12,7 +12,15 @@
 // The scratch is a file-scope __device__ array: every GPU that loads the
 // library holds it (SCRATCH_BYTES below) until the process exits.  Host code
 // cannot use the array's name as a device address; the device address is
-// looked up once per device with cudaGetSymbolAddress and cached.
+// looked up with cudaGetSymbolAddress on the first call made in a device's
+// context and cached with that context.  A call made in another context of
+// the same device (a context the caller created and made current, or the
+// primary context re-created after cudaDeviceReset with a different handle)
+// looks the address up again.  cudaDeviceReset unloads the library's device
+// code: after a reset, the first call should come from a fresh primary
+// context, before any stream capture.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -33,21 +41,42 @@ static __device__ __align__(256) unsigned char g_dots_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 static std::mutex g_scratch_mu;
 static void* g_scratch_addr[kMaxDevices] = {};
+static CUcontext g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of the scratch on the current device (looked up on the
-// first call made on that device).
+// The calling thread's current driver context (the runtime makes the
+// device's primary context current on its first call); reached through the
+// runtime's driver entry-point table, so the library does not link libcuda.
+static CUcontext current_context() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  static GetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCurrent>(f);
+  }();
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) throw Error(SAP_ERR_CUDA, "cuCtxGetCurrent is not available");
+  return c;
+}
+
+// Device address of the scratch in the current context of the current
+// device (looked up on the first call made in that context).
 static unsigned char* scratch_on_current_device() {
   int dev = 0;
   SAPB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) throw Error(SAP_ERR_UNSUPPORTED, "device ordinal beyond 63");
+  const CUcontext ctx = current_context();  // null before the runtime's first context is made current
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!ctx || !g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_dots_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_dots_scratch);  // makes the primary context current if none is
     if (e != cudaSuccess || !p)
       throw Error(SAP_ERR_CUDA, std::string("cudaGetSymbolAddress of the dot-product scratch failed: ") +
                                     cudaGetErrorString(e));
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = current_context();
   }
   return static_cast<unsigned char*>(g_scratch_addr[dev]);
 }

@@ -26,19 +26,27 @@ k_spmv_banded(const double* __restrict__ A, const double* __restrict__ x, double
 }
 
 // y = A x, FP64 CSR (the product SpmvCusp delegates to, sap/spmv.h:110-121):
-// a group of LANES threads per row.
+// a group of LANES threads per row.  The row loop runs over warp-uniform
+// bases (a warp serves 32 / LANES consecutive rows per step), so every lane
+// of a warp takes the same number of steps and the full-mask shuffles never
+// name a lane that has left the loop; rows past n contribute nothing.
 template <int LANES>
 __global__ void __launch_bounds__(256)
 k_spmv_csr(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
            const double* __restrict__ x, double* __restrict__ y, int n) {
-  const int sub = threadIdx.x % LANES;
-  const int groups = (gridDim.x * blockDim.x) / LANES;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / LANES; i < n; i += groups) {
+  constexpr int kRowsPerWarp = 32 / LANES;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % LANES;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long stride = (((long long)gridDim.x * blockDim.x) >> 5) * kRowsPerWarp;
+  for (long long i0 = warp * kRowsPerWarp; i0 < n; i0 += stride) {
+    const long long i = i0 + lane / LANES;
     double acc = 0.0;
-    for (int p = rp[i] + sub; p < rp[i + 1]; p += LANES) acc += v[p] * __ldg(x + ci[p]);
+    if (i < n)
+      for (int p = rp[i] + sub; p < rp[i + 1]; p += LANES) acc += v[p] * __ldg(x + ci[p]);
 #pragma unroll
     for (int off = LANES / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, LANES);
-    if (sub == 0) y[i] = acc;
+    if (sub == 0 && i < n) y[i] = acc;
   }
 }
 

@@ -55,6 +55,53 @@ def convection_diffusion_csr(m: int = 1000, conv: float = 0.3, fill_per_row: int
     return rp.astype(np.int32), cols.astype(np.int32), vals, perm
 
 
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser on uint64 arrays (wrap-around arithmetic)."""
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return x ^ (x >> np.uint64(31))
+
+
+def banded_rowmajor(n: int, k: int, d: float, dist: int = 1, seed: int = 0, rows_per_chunk: int = 1 << 16):
+    """Row-major band ((2k+1) values per row, A(i, j) at i*(2k+1) + k + j - i)
+    of the seeded counter-based banded generator: every off-diagonal (i, j)
+    with |i - j| <= k inside the matrix is drawn from a hash of (seed, i, j),
+    U[-1, 1] (dist 1) or N(0, 1) by Box-Muller (dist 2); the diagonal is
+    d * sum_j |A(i, j)|.  The same matrix as the library's
+    sap_generate_band_host with these arguments: value for value for dist 1;
+    for dist 2 up to the last-bit rounding of numpy's log and cos against the C
+    library's."""
+    if dist not in (1, 2):
+        raise ValueError("dist must be 1 (uniform) or 2 (normal)")
+    sw = 2 * k + 1
+    out = np.zeros((n, sw))
+    s0 = _splitmix64(np.array([np.uint64(seed) ^ np.uint64(0x5A5A5A5A12345678)], dtype=np.uint64))[0]
+    offs = np.arange(-k, k + 1, dtype=np.int64)
+    for r0 in range(0, n, rows_per_chunk):
+        r = np.arange(r0, min(n, r0 + rows_per_chunk), dtype=np.int64)
+        c = r[:, None] + offs[None, :]
+        ok = (c >= 0) & (c < n) & (offs[None, :] != 0)
+        key = (r[:, None].astype(np.uint64) << np.uint64(32)) | (c.astype(np.uint64) & np.uint64(0xFFFFFFFF))
+        h = _splitmix64(s0 ^ _splitmix64(key))
+        u = (h >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+        if dist == 1:
+            val = -1.0 + 2.0 * u
+        else:
+            u2 = (_splitmix64(h) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+            u1 = np.maximum(u, 1e-300)
+            val = np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+        val = np.where(ok, val, 0.0)
+        # the diagonal sums |off-diagonals| in column order, as the generator does
+        rs = np.zeros(len(r))
+        for j in range(sw):
+            rs += np.abs(val[:, j])
+        val[:, k] = d * rs
+        out[r0:r0 + len(r)] = val
+    return out
+
+
 def csr_matvec(rp, ci, v, x):
     """y = A x for a CSR matrix (numpy)."""
     rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))

@@ -1,4 +1,6 @@
 """Host-side pieces of the learned settings and the batched ensemble (no GPU)."""
+import os
+
 import numpy as np
 
 import saplibrary_b200 as sap
@@ -44,3 +46,35 @@ def test_sweep_bytes_counts_triangles_vectors_and_scales():
     # the full-size workload's FP16 sweep reads about half of the FP32 one
     r = bench.sweep_bytes(3168, 20, 16, 2) / bench.sweep_bytes(3168, 20, 16, 4)
     assert 0.5 < r < 0.51
+
+
+def test_numpy_band_generator_matches_the_library_generator():
+    # the CPU reference side of the bench generates the banded workloads with
+    # numpy (without loading the CUDA library): the same matrices as the
+    # library's generator, bit for bit for uniform values
+    from saplibrary_b200 import problems
+    for n, k, d in ((1000, 7, 1.0), (3000, 50, 0.8), (300, 200, 1.2)):
+        a = problems.banded_rowmajor(n, k, d, dist=1, seed=11, rows_per_chunk=997)
+        b = sap.generate_band_host(n, k, d, 1, seed=11).reshape(n, 2 * k + 1)
+        assert np.array_equal(a, b)
+        a2 = problems.banded_rowmajor(n, k, d, dist=2, seed=3)
+        b2 = sap.generate_band_host(n, k, d, 2, seed=3).reshape(n, 2 * k + 1)
+        assert np.allclose(a2, b2, rtol=1e-13, atol=1e-13)
+
+
+def test_bench_reference_arm_reports_unavailable_without_the_cuda_library():
+    # the CPU reference arm must not load libsap_b200 (checked in a fresh
+    # process) and reports why no complete CPU solve of the 1M-row workload runs
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference'];\n"
+            "runpy.run_path('bench.py', run_name='__main__');\n"
+            "maps = open('/proc/self/maps').read(); print('LOADED' if 'libsap_b200' in maps else 'CLEAN')")
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = out.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and "tens of minutes" in line["unavailable"]
+    assert lines[-1] == "CLEAN"
