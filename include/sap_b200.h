@@ -194,6 +194,20 @@ int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y,
 int sap_blas_dots_noalloc(int n, int nq, const double* const* x, const double* const* y, double* out,
                           void* stream);
 
+/* ---- tensor-core GEMM (no reference counterpart) ----------------------------
+ * The batched product the wide-band block factorization, its spike slabs
+ * and reduced systems run on in the TF32 forms, exposed for tests and
+ * measurement: C_b = alpha A_b B_b + beta C_b for b < batch, column-major
+ * FP32 device matrices (A m x k, B k x n, C m x n; leading dimensions lda,
+ * ldb, ldc and batch strides sA, sB, sC in elements), TF32 inputs (rounded
+ * to nearest) and FP32 accumulation on the sm_100 tensor cores (tcgen05,
+ * operands staged by TMA).  A and B must be 16-byte aligned with lda, ldb,
+ * sA, sB multiples of 4 (else SAP_ERR_UNSUPPORTED, nothing launched).  The
+ * call enqueues on `stream` and waits for it; SAP_ERR_DEVICE_TIMEOUT if a
+ * bounded wait inside the kernel ran out. */
+int sap_tc_gemm_batched(int m, int n, int k, float alpha, const float* A, int lda, long long sA, const float* B,
+                        int ldb, long long sB, float beta, float* C, int ldc, long long sC, int batch, void* stream);
+
 /* ---- solver --------------------------------------------------------------- */
 /* Solver(numPartitions, opts) (sap/solver.h:157-158, 268-297).  prec_dtype
  * is the preconditioner's PrecValueType: SAP_PREC_FLOAT or SAP_PREC_DOUBLE,

@@ -135,6 +135,8 @@ _sig = {
     "sap_reorder_host": (_i, [_i, _i, _vp, _vp, _vp, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_blas_dots_noalloc": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
+    "sap_tc_gemm_batched": (_i, [_i, _i, _i, ctypes.c_float, _vp, _i, ctypes.c_longlong, _vp, _i, ctypes.c_longlong,
+                                 ctypes.c_float, _vp, _i, ctypes.c_longlong, _i, _vp]),
     "sap_profile_select": (_i, [ctypes.c_char_p]),
     "sap_profile_read": (_i, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
 }
@@ -297,6 +299,19 @@ def blas_dots(xs, ys, out, stream: int = 0) -> None:
     xa = (ctypes.c_void_p * nq)(*[t.data_ptr() for t in xs])
     ya = (ctypes.c_void_p * nq)(*[t.data_ptr() for t in ys])
     _check(_lib.sap_blas_dots(n, nq, xa, ya, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(stream)))
+
+
+def tc_gemm_batched(m: int, n: int, k: int, alpha: float, A, lda: int, sA: int, B, ldb: int, sB: int, beta: float,
+                    C, ldc: int, sC: int, batch: int, stream: int = 0) -> None:
+    """C_b = alpha A_b B_b + beta C_b on the tensor cores (TF32 inputs, FP32
+    accumulation): the library's batched product of the wide-band
+    factorization (sap_tc_gemm_batched).  A, B, C are CUDA float32 tensors or
+    device addresses; the views are column-major with the given leading
+    dimensions and batch strides (elements).  Waits for the stream."""
+    def addr(t):
+        return t if isinstance(t, int) else t.data_ptr()
+    _check(_lib.sap_tc_gemm_batched(m, n, k, alpha, addr(A), lda, sA, addr(B), ldb, sB, beta, addr(C), ldc, sC,
+                                    batch, stream or None))
 
 
 def generate_band_host(n: int, k: int, d: float, dist: int = 1, seed: int = 0) -> np.ndarray:

@@ -1794,6 +1794,34 @@ int sap_blas_dots(int n, int nq, const double* const* x, const double* const* y,
   });
 }
 
+int sap_tc_gemm_batched(int m, int n, int k, float alpha, const float* A, int lda, long long sA, const float* B,
+                        int ldb, long long sB, float beta, float* C, int ldc, long long sC, int batch, void* stream) {
+  SAP_TRY({
+    SAP_REQUIRE(m >= 0 && n >= 0 && k >= 0 && batch >= 0 && lda >= std::max(1, m) && ldb >= std::max(1, k) &&
+                    ldc >= std::max(1, m) && A && B && C,
+                "invalid GEMM arguments");
+    if (!umma::available()) throw Error(SAP_ERR_UNSUPPORTED, "the tensor-core GEMM needs an sm_100 device");
+    static DBuf<int> err;  // error word of the kernel's bounded waits (one per process)
+    cudaStream_t st = (cudaStream_t)stream;
+    if (err.size() == 0) {
+      err.alloc(1);
+      err.zero(st);
+    }
+    umma::prepare();
+    if (!umma::gemm(m, n, k, alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, batch, err.get(), st))
+      throw Error(SAP_ERR_UNSUPPORTED,
+                  "operand views break the TMA rules (16-byte aligned bases, leading dimensions and batch strides "
+                  "multiples of 4 values)");
+    int e = 0;
+    SAPB_CUDA(cudaMemcpyAsync(&e, err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    if (e) {
+      err.zero(st);
+      throw Error(SAP_ERR_DEVICE_TIMEOUT, "a tensor-core GEMM wait ran out of its iteration limit");
+    }
+  });
+}
+
 int sap_solver_create(int P, const sap_options* opts, int prec_dtype, sap_solver** out) {
   SAP_TRY({
     SAP_REQUIRE(out && opts && P >= 1, "invalid solver arguments");

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "umma_gemm.cuh"
 #include "wide_band.cuh"
 
 namespace sapb {
@@ -67,7 +68,15 @@ class BlockLU {
   int* flag = nullptr;
   Mat<T> W;  // workspace, >= n x n per batch element (the inverse-block temporaries of rec)
 
+  // tc: TF32 products on this library's tensor-core kernel (umma::gemm);
+  // otherwise, and for a view that does not meet the TMA rules, cuBLAS
+  bool tc = false;
+  int* gerr = nullptr;  // error word of the tensor-core kernel's bounded waits
   void gemm(int m, int n, int k, T alpha, Mat<T> A, Mat<T> B, T beta, Mat<T> C) {
+    if constexpr (sizeof(T) == 4) {
+      if (tc && umma::gemm(m, n, k, alpha, A.p, A.ld, A.s, B.p, B.ld, B.s, beta, C.p, C.ld, C.s, batch, gerr, st))
+        return;
+    }
     Gemm<T>::run(h, m, n, k, alpha, A.p, A.ld, A.s, B.p, B.ld, B.s, beta, C.p, C.ld, C.s, batch);
   }
   void copy(Mat<T> src, Mat<T> dst, int m, int n, T scale = T(1)) {
@@ -343,6 +352,27 @@ class WideBand {
   // tf32: FP32 block products on the tensor cores (TF32 inputs, FP32
   // accumulation) for the partition factors, spikes and reduced systems.
   bool tf32 = false;
+  // The TF32 products run on this library's tcgen05 kernel (umma_gemm.cuh)
+  // on sm_100; SAPB_TC_GEMM=0 hands them to cuBLAS's TF32 mode instead.
+  static bool tc_gemm_enabled() {
+    const char* e = std::getenv("SAPB_TC_GEMM");
+    return !(e && std::atoi(e) == 0) && umma::available();
+  }
+  bool tc_on() const { return tf32 && tc_gemm_enabled(); }
+  DBuf<int> gemm_err;
+  // after a synchronisation: a bounded wait of the tensor-core kernel that
+  // ran out is reported (and the word cleared)
+  void check_gemm() {
+    if (gemm_err.size() == 0) return;
+    int e = 0;
+    SAPB_CUDA(cudaMemcpyAsync(&e, gemm_err.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    if (e) {
+      gemm_err.zero(st);
+      SAPB_CUDA(cudaStreamSynchronize(st));
+      throw Error(SAP_ERR_DEVICE_TIMEOUT, "a tensor-core GEMM wait ran out of its iteration limit");
+    }
+  }
   // h16: the block sweeps of the apply read FP16 copies of the factor
   // blocks with a power-of-two scale per column (half the bytes of FP32);
   // the setup keeps computing in FP32 / TF32.  FP32 storage only.
@@ -418,12 +448,14 @@ class WideBand {
     for (cublasHandle_t x : {h, h2})
       cublas_check(cublasSetMathMode(x, fast ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_PEDANTIC_MATH), "cublasSetMathMode");
   }
-  // the second lane of a recursive factorization
+  // the second lane of a recursive factorization, and the product engine
   void lanes(BlockLU<T>& lu) {
     lu.h2 = h2;
     lu.st2 = st2;
     lu.ev_a = ev_fork;
     lu.ev_b = ev_join;
+    lu.tc = tc_on();
+    lu.gerr = gemm_err.get();
   }
 
   void init(cudaStream_t s, int n_, int bs_, const std::vector<int>& pstart, const std::vector<int>& psize,
@@ -457,6 +489,11 @@ class WideBand {
     }
     spike = false;
     math_mode(tf32);
+    if (gemm_err.size() == 0) {
+      gemm_err.alloc(1);
+      gemm_err.zero(st);
+    }
+    if (tc_on()) umma::prepare();  // kernel attributes, before any capture
     int maxsz = 0;
     for (int v : psize) maxsz = std::max(maxsz, v);
     nb = std::max(1, (maxsz + bs - 1) / bs);
@@ -564,6 +601,7 @@ class WideBand {
     int hf = 0;
     SAPB_CUDA(cudaMemcpyAsync(&hf, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     SAPB_CUDA(cudaStreamSynchronize(st));
+    check_gemm();
     if (hf && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
     make_half();
   }
@@ -993,6 +1031,8 @@ class WideBand {
       ops.st = st;
       ops.batch = nI;
       ops.cut = spike_cut();
+      ops.tc = tc_on();
+      ops.gerr = gemm_err.get();
       const Mat<T> Wm{Wt.get(), bs, (long long)bs * cs};
       const int ib0 = std::max(0, minpos) / bs;
       auto Xb = [&](int i) { return Mat<T>{X.get() + (long long)i * bs, (int)plen, sX}; };
@@ -1025,6 +1065,7 @@ class WideBand {
       }
       SAPB_CUDA(cudaStreamSynchronize(st));
     }
+    check_gemm();
   }
 
   // S_t = I - W_t V_t, factored with its triangular inverses (boosted only
@@ -1059,6 +1100,7 @@ class WideBand {
     lu.flag = sflag.get();
     lu.W = Mat<T>{Ws.get(), ldK, sK};
     lanes(lu);
+    lu.tc = tc_on() && reduced_tf32();
     lu.rws = std::max(1LL, BlockLU<T>::rec_ws(K, lu.leaf));
     Rs.alloc((size_t)nI * lu.rws);
     lu.rw = Rs.get();
@@ -1082,6 +1124,7 @@ class WideBand {
     t1.alloc((size_t)nI * K);
     t2.alloc((size_t)nI * K);
     SAPB_CUDA(cudaStreamSynchronize(st));
+    check_gemm();
   }
 
   // Reduced solve and purification: x holds A_p^-1 f (block layout), F the

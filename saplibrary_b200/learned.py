@@ -24,6 +24,8 @@ from . import (BandedMatrix, Block, FGMRES, LU_UL, LibraryError, MVBanded, Optio
 SETTINGS = [(1, Spike), (4, Spike), (16, Spike), (64, Spike), (4, Block), (16, Block), (64, Block)]
 DEFAULT_SETTING = 2  # 16 partitions, coupled SPIKE
 NUM_FEATURES = 16
+# below this largest class probability the chooser keeps the default setting
+CONFIDENCE = 0.5
 
 
 def band_features(band: np.ndarray, n: int, K: int) -> np.ndarray:
@@ -52,11 +54,12 @@ def band_features(band: np.ndarray, n: int, K: int) -> np.ndarray:
     return np.asarray(f, dtype=np.float32)
 
 
-def measure(band: np.ndarray, n: int, K: int, setting: int, b: np.ndarray, reps: int = 2,
+def measure(band: np.ndarray, n: int, K: int, setting: int, b: np.ndarray, reps: int = 3,
             rel_tol: float = 1e-10) -> float:
-    """Device time-to-solution (s) of setup + FGMRES solve with an FP32
-    preconditioner under one setting (best of `reps`); inf when the solve
-    does not converge."""
+    """Time-to-solution (s) of setup + FGMRES solve with an FP32
+    preconditioner under one setting (best of `reps`, so that a host stall
+    in one repetition does not enter the label); inf when the solve does
+    not converge."""
     import torch
     P, ptype = SETTINGS[setting]
     opts = Options(solverType=FGMRES, performReorder=False, variableBandwidth=False, applyScaling=False,
@@ -160,8 +163,21 @@ class SettingsNet:
         _check(_lib.sap_mlp_train(self._h, Xn.ctypes.data, y.ctypes.data, Xn.shape[0], epochs, lr, ctypes.byref(loss)))
         return loss.value
 
-    def choose(self, X) -> np.ndarray:
-        return self.logits(X).argmax(axis=1)
+    def probabilities(self, X) -> np.ndarray:
+        z = self.logits(X).astype(np.float64)
+        z -= z.max(axis=1, keepdims=True)
+        e = np.exp(z)
+        return e / e.sum(axis=1, keepdims=True)
+
+    def choose(self, X, min_confidence: float = CONFIDENCE) -> np.ndarray:
+        """The setting of the largest logit per matrix; the default heuristic
+        where the network is unsure (largest probability below
+        `min_confidence`), so that a matrix unlike the training set falls
+        back to the method without the network."""
+        p = self.probabilities(X)
+        picks = p.argmax(axis=1)
+        picks[p.max(axis=1) < min_confidence] = DEFAULT_SETTING
+        return picks
 
 
 def labels_from_times(T: np.ndarray) -> np.ndarray:

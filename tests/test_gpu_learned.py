@@ -46,7 +46,7 @@ def test_training_lowers_loss_and_is_deterministic():
     lb = b.train(X, y, epochs=300)
     assert la < 0.5 * l0
     assert la == lb and np.array_equal(a.params(), b.params())
-    assert (a.choose(X) == y).mean() > 0.9
+    assert (a.choose(X, min_confidence=0.0) == y).mean() > 0.9
 
 
 def test_chooser_against_default_on_held_out_sweep():
@@ -57,5 +57,9 @@ def test_chooser_against_default_on_held_out_sweep():
     picks = net.choose(X[held])
     g = learned.gain(T[held], picks)
     print("held-out", g)
+    print("held-out times [matrix, setting] (s):\n", np.array2string(T[held], precision=4))
+    print("picks", picks, "confidence", np.round(net.probabilities(X[held]).max(axis=1), 2))
     assert g["failed_chosen"] <= g["failed_default"]
-    assert g["total_chosen_s"] <= 1.05 * g["total_default_s"]
+    # the trained chooser is at least as fast as the default heuristic in
+    # total over the held-out matrices
+    assert g["total_chosen_s"] <= g["total_default_s"]
