@@ -3,22 +3,31 @@
 // the products of the wide-band block factorization, spike slabs and
 // reduced systems (TF32 inputs, FP32 accumulation in tensor memory).
 //
-// One CTA computes one 128 x BN tile of one batch element:
+// A persistent grid (at most the CTAs that fit on the SMs at once) walks the
+// 128 x BN output tiles of all batch elements; in each CTA
 //   warp 0     TMA producer: 128 x 32 tiles of A (four 32 x 32 boxes, M
 //              contiguous) and BN x 32 tiles of B (one box, K contiguous)
 //              into a ring of shared-memory stages;
-//   warp 1     allocates the tile's accumulator in tensor memory and issues
-//              tcgen05.mma (kind::tf32, M = 128, N = BN, K = 8) from one
-//              thread; tcgen05.commit frees a stage once its MMAs have read it;
-//   warps 2-5  epilogue: tcgen05.ld of the accumulator (warp w reads lanes
-//              32 (w mod 4) ...), alpha / beta, coalesced column stores.
+//   warp 1     allocates two BN-column accumulators in tensor memory and
+//              issues tcgen05.mma (kind::tf32, M = 128, N = BN, K = 8) from
+//              one thread; tcgen05.commit frees a stage once its MMAs have
+//              read it and hands a finished accumulator to the epilogue;
+//   warps 2-5  epilogue: tcgen05.ld of a finished accumulator (warp w reads
+//              lanes 32 (w mod 4) ...), alpha / beta, coalesced column
+//              stores, then the accumulator is free again: the epilogue of
+//              one tile overlaps the MMAs of the next.
 // A is read MN-major (M contiguous) and B K-major, which is what column-major
 // storage gives without a transpose.  An MN-major TF32 operand must use the
 // 128-byte swizzle with 32-byte atoms (TMA SWIZZLE_128B_ATOM_32B, descriptor
 // layout SWIZZLE_128B_BASE32B: 4 K-rows of 128 bytes per atom); the K-major
-// B uses the 128-byte swizzle with 16-byte atoms (8 rows per atom).  The TMA descriptors round FP32 to TF32
-// (round to nearest) on the way into shared memory.  Out-of-range rows and
-// columns of a tile are zero-filled by TMA and not stored.
+// B uses the 128-byte swizzle with 16-byte atoms (8 rows per atom).  The TMA
+// descriptors round FP32 to TF32 (round to nearest) on the way into shared
+// memory.  Out-of-range rows and columns of a tile are zero-filled by TMA and
+// not stored.
+//
+// Launches are programmatic dependent launches: a CTA lets the next kernel
+// of the stream start its prologue at once, and waits for its predecessor
+// (griddepcontrol.wait) before its first global read or write.
 //
 // Every wait on an mbarrier is bounded: when a wait runs out, the kernel
 // raises an error word, drains its own copies and MMAs (again with bounds),
@@ -48,9 +57,9 @@ struct Cfg {
   static constexpr int kABytes = kBM * kBK * 4;  // 16 KB: four 32 x 32 boxes
   static constexpr int kBBytes = BN * kBK * 4;   // BN rows of 128 bytes
   static constexpr int kStage = kABytes + kBBytes;
-  static constexpr int kBarBytes = 256;          // full[], empty[], acc, tmem slot, abort flag
+  static constexpr int kBarBytes = 256;          // full[], empty[], acc_full[2], acc_empty[2], drain, tmem slot, abort
   static constexpr int kSmem = kStages * kStage + kBarBytes + 1024;  // + alignment slack
-  static constexpr int kTmemCols = BN;           // power of two >= 32
+  static constexpr int kTmemCols = 2 * BN;       // two accumulators; a power of two >= 32
 };
 
 // ---- PTX wrappers ---------------------------------------------------------------
@@ -59,6 +68,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 }
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -146,28 +158,36 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
 template <int BN>
 __global__ void __launch_bounds__(kThreads, 1)
 k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float* __restrict__ C,
-            int ldc, long long sC, int M, int N, int K, float alpha, float beta, int* err) {
+            int ldc, long long sC, int M, int N, int K, int batch, float alpha, float beta, int* err) {
   using G = Cfg<BN>;
   extern __shared__ unsigned char smem_raw[];
   // stage buffers on a 1024-byte boundary of the shared window (swizzle atoms)
   unsigned char* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   unsigned char* stage_base = smem;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::kStages * G::kStage);
-  // bars[0, S): full, bars[S, 2S): empty, bars[2S]: accumulator ready
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * G::kStages + 1);
+  constexpr int S = G::kStages;
+  // bars: [0, S) full, [S, 2S) empty, [2S, 2S+2) accumulator full,
+  // [2S+2, 2S+4) accumulator empty, [2S+4] drain
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN, bz = blockIdx.z;
   const int KT = (K + kBK - 1) / kBK;
-  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + G::kStages), accb = smem_u32(bars + 2 * G::kStages);
+  const int tiles_m = (M + kBM - 1) / kBM, tiles_n = (N + BN - 1) / BN;
+  const int tiles_mn = tiles_m * tiles_n, tiles = tiles_mn * batch;
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + S);
+  const uint32_t accf0 = smem_u32(bars + 2 * S), acce0 = smem_u32(bars + 2 * S + 2), drain = smem_u32(bars + 2 * S + 4);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < G::kStages; s++) {
+    for (int s = 0; s < S; s++) {
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(accb, 1);
+    for (int a = 0; a < 2; a++) {
+      mbar_init(accf0 + 8 * a, 1);
+      mbar_init(acce0 + 8 * a, kEpiWarps);
+    }
+    mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
@@ -184,29 +204,35 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // the next kernel of the stream may start its prologue
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
   if (warp == 0 && lane == 0) {
     // ---- producer ----------------------------------------------------------------
-    int issued = 0;
-    for (int kt = 0; kt < KT; kt++) {
-      const int s = kt % G::kStages;
-      const uint32_t ph = (uint32_t)(kt / G::kStages) & 1u;
-      if (!wait_bar(empty0 + 8 * s, ph ^ 1u, abort_flag, err)) break;
-      const uint32_t fb = full0 + 8 * s;
-      mbar_expect_tx(fb, (uint32_t)G::kStage);
-      const uint32_t a_dst = smem_u32(stage_base + (size_t)s * G::kStage);
-      const uint32_t b_dst = a_dst + G::kABytes;
-      const int k0 = kt * kBK;
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // A and B may come from the previous kernel
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x) {
+      const int bz = t / tiles_mn, r = t - bz * tiles_mn;
+      const int m0 = (r % tiles_m) * kBM, n0 = (r / tiles_m) * BN;
+      for (int kt = 0; kt < KT; kt++, it++) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!wait_bar(empty0 + 8 * s, ph ^ 1u, abort_flag, err)) break;
+        const uint32_t fb = full0 + 8 * s;
+        mbar_expect_tx(fb, (uint32_t)G::kStage);
+        const uint32_t a_dst = smem_u32(stage_base + (size_t)s * G::kStage);
+        const uint32_t b_dst = a_dst + G::kABytes;
+        const int k0 = kt * kBK;
 #pragma unroll
-      for (int i = 0; i < 4; i++) tma_load_3d(a_dst + 4096u * i, &tmA, fb, m0 + 32 * i, k0, bz);
-      tma_load_3d(b_dst, &tmB, fb, k0, n0, bz);
-      issued = kt + 1;
+        for (int i = 0; i < 4; i++) tma_load_3d(a_dst + 4096u * i, &tmA, fb, m0 + 32 * i, k0, bz);
+        tma_load_3d(b_dst, &tmB, fb, k0, n0, bz);
+      }
     }
     if (*abort_flag) {
       // drain: every stage of the last round still owed bytes by TMA
-      for (int kt = (issued > G::kStages ? issued - G::kStages : 0); kt < issued; kt++) {
-        const uint32_t fb = full0 + 8 * (kt % G::kStages);
-        const uint32_t ph = (uint32_t)(kt / G::kStages) & 1u;
+      for (int j = (it > S ? it - S : 0); j < it; j++) {
+        const uint32_t fb = full0 + 8 * (j % S);
+        const uint32_t ph = (uint32_t)(j / S) & 1u;
         for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(fb, ph); i++) {
         }
       }
@@ -214,39 +240,54 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer --------------------------------------------------------------
     constexpr uint32_t idesc = instr_desc<BN>();
-    for (int kt = 0; kt < KT; kt++) {
-      const int s = kt % G::kStages;
-      const uint32_t ph = (uint32_t)(kt / G::kStages) & 1u;
-      if (!wait_bar(full0 + 8 * s, ph, abort_flag, err)) break;
+    int it = 0, lt = 0;
+    for (int t = blockIdx.x; t < tiles && !*abort_flag; t += gridDim.x, lt++) {
+      const int a = lt & 1;
+      const uint32_t aph = (uint32_t)(lt >> 1) & 1u;
+      if (!wait_bar(acce0 + 8 * a, aph ^ 1u, abort_flag, err)) break;  // the epilogue has read it
       tc_fence_after();
-      const uint32_t a_base = smem_u32(stage_base + (size_t)s * G::kStage);
-      const uint32_t b_base = a_base + G::kABytes;
+      const uint32_t d = tmem + (uint32_t)(a * BN);
+      for (int kt = 0; kt < KT; kt++, it++) {
+        const int s = it % S;
+        const uint32_t ph = (uint32_t)(it / S) & 1u;
+        if (!wait_bar(full0 + 8 * s, ph, abort_flag, err)) break;
+        tc_fence_after();
+        const uint32_t a_base = smem_u32(stage_base + (size_t)s * G::kStage);
+        const uint32_t b_base = a_base + G::kABytes;
 #pragma unroll
-      for (int kk = 0; kk < kBK / 8; kk++) {
-        // A: 8 K-rows per instruction = two 512-byte atoms of 4 rows (SBO);
-        // the M groups of 32 are the 4096-byte boxes (LBO).  B: 8 K values =
-        // 32 bytes along each 128-byte row; 8-row groups 1024 bytes apart.
-        const uint64_t ad = smem_desc(a_base + 1024u * kk, 4096u, 512u, kLayoutSW128Base32);
-        const uint64_t bd = smem_desc(b_base + 32u * kk, 16u, 1024u, kLayoutSW128);
-        tc_mma_tf32(tmem, ad, bd, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+        for (int kk = 0; kk < kBK / 8; kk++) {
+          // A: 8 K-rows per instruction = two 512-byte atoms of 4 rows (SBO);
+          // the M groups of 32 are the 4096-byte boxes (LBO).  B: 8 K values =
+          // 32 bytes along each 128-byte row; 8-row groups 1024 bytes apart.
+          const uint64_t ad = smem_desc(a_base + 1024u * kk, 4096u, 512u, kLayoutSW128Base32);
+          const uint64_t bd = smem_desc(b_base + 32u * kk, 16u, 1024u, kLayoutSW128);
+          tc_mma_tf32(d, ad, bd, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+        }
+        tc_commit(empty0 + 8 * s);  // the stage is free once these MMAs have read it
       }
-      tc_commit(empty0 + 8 * s);  // the stage is free once these MMAs have read it
+      tc_commit(accf0 + 8 * a);  // the accumulator is complete once all MMAs above are
     }
-    tc_commit(accb);  // all MMAs issued above (none on an abort before the first) complete
-    if (*abort_flag)  // the epilogue may stop waiting early: no MMA may run into the dealloc
-      for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(accb, 0u); i++) {
-      }
+    // no MMA may still run when the tensor memory is freed
+    tc_commit(drain);
+    for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(drain, 0u); i++) {
+    }
   } else if (warp >= 2) {
     // ---- epilogue ----------------------------------------------------------------
-    const bool ok = wait_bar(accb, 0u, abort_flag, err) && !*abort_flag;
-    tc_fence_after();
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // C may be read or written by the previous kernel
     const int q = warp & 3;  // the TMEM lane quadrant this warp may read
-    const int m = m0 + 32 * q + lane;
-    float* Cb = C + (long long)bz * sC;
-    if (ok && KT > 0) {
+    int lt = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, lt++) {
+      const int a = lt & 1;
+      const uint32_t aph = (uint32_t)(lt >> 1) & 1u;
+      if (!wait_bar(accf0 + 8 * a, aph, abort_flag, err) || *abort_flag) break;
+      tc_fence_after();
+      const int bz = t / tiles_mn, r = t - bz * tiles_mn;
+      const int m0 = (r % tiles_m) * kBM, n0 = (r / tiles_m) * BN;
+      const int m = m0 + 32 * q + lane;
+      float* Cb = C + (long long)bz * sC;
       for (int c0 = 0; c0 < BN && n0 + c0 < N; c0 += 32) {
         float v[32];
-        tc_ld_32cols(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+        tc_ld_32cols(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(a * BN + c0), v);
         if (m < M) {
           float* col = Cb + (long long)(n0 + c0) * ldc + m;
           const int nc = min(32, N - n0 - c0);
@@ -256,15 +297,20 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUt
             for (int j = 0; j < 32; j++)
               if (j < nc) col[(long long)j * ldc] = alpha * v[j];
           } else {
+            // all 32 loads of C first, then the stores: interleaved, every
+            // load would wait for the store before it (they may alias)
+            float c[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++) c[j] = j < nc ? col[(long long)j * ldc] : 0.f;
 #pragma unroll
             for (int j = 0; j < 32; j++)
-              if (j < nc) {
-                float* p = col + (long long)j * ldc;
-                *p = alpha * v[j] + beta * *p;
-              }
+              if (j < nc) col[(long long)j * ldc] = alpha * v[j] + beta * c[j];
           }
         }
       }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce0 + 8 * a);  // this warp is done with the accumulator
     }
   }
   tc_fence_before();
@@ -353,18 +399,47 @@ inline void set_smem_attr() {
     done = true;
   }
 }
+
+// CTAs of one tile width that fit on the device at once (the persistent grid)
+template <int BN>
+inline int resident_ctas() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0, sms = 0, occ = 0;
+    SAPB_CUDA(cudaGetDevice(&dev));
+    SAPB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SAPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_umma_gemm<BN>, kThreads, Cfg<BN>::kSmem));
+    n = std::max(1, sms * std::max(1, occ));
+  }
+  return n;
+}
+
+// kernel attributes and grid sizes, set once outside any stream capture
 inline void prepare() {
   set_smem_attr<64>();
   set_smem_attr<128>();
   set_smem_attr<256>();
+  resident_ctas<64>();
+  resident_ctas<128>();
+  resident_ctas<256>();
 }
 
 template <int BN>
 inline void launch_bn(const CUtensorMap& ta, const CUtensorMap& tb, float* C, int ldc, long long sC, int m, int n,
                       int k, float alpha, float beta, int batch, int* err, cudaStream_t st) {
   set_smem_attr<BN>();
-  const dim3 grid((m + kBM - 1) / kBM, (n + BN - 1) / BN, batch);
-  k_umma_gemm<BN><<<grid, kThreads, Cfg<BN>::kSmem, st>>>(ta, tb, C, ldc, sC, m, n, k, alpha, beta, err);
+  const long long tiles = (long long)((m + kBM - 1) / kBM) * ((n + BN - 1) / BN) * batch;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)std::min<long long>(tiles, resident_ctas<BN>()));
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = Cfg<BN>::kSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SAPB_CUDA(cudaLaunchKernelEx(&cfg, k_umma_gemm<BN>, ta, tb, C, ldc, sC, m, n, k, batch, alpha, beta, err));
   SAPB_LAUNCHED();
 }
 
@@ -377,7 +452,6 @@ inline int pick_bn(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 256); }
 inline bool gemm(int m, int n, int k, float alpha, const float* A, int lda, long long sA, const float* B, int ldb,
                  long long sB, float beta, float* C, int ldc, long long sC, int batch, int* err, cudaStream_t st) {
   if (m <= 0 || n <= 0 || batch <= 0) return true;
-  if (batch > 65535) return false;
   if (k <= 0) {
     if (beta == 1.f) return true;
     k_gemm_scale<<<dim3((m + 255) / 256, std::min(n, 1024), batch), 256, 0, st>>>(C, ldc, sC, m, n, beta);

@@ -204,10 +204,13 @@ class BlockLU {
     return n1;
   }
   int leaf = leaf_size<T>();  // largest leaf of the recursion
+  // leading dimension of an n-row workspace panel: a multiple of 4 values,
+  // so that every panel view meets the TMA rules of the tensor-core GEMM
+  static int pad4(int n) { return (n + 3) / 4 * 4; }
   static long long rec_ws(int n, int leaf) {
     if (n <= leaf) return 0;
     const int n1 = split(n), n2 = n - n1;
-    return std::max(rec_ws(n1, leaf), 2LL * n1 * n2 + rec_ws(n2, leaf));
+    return std::max(rec_ws(n1, leaf), (long long)n1 * n2 + (long long)pad4(n2) * n1 + rec_ws(n2, leaf));
   }
   template <int NL>
   void leaf_launch(Mat<T> M, Mat<T> Li, Mat<T> Ui, int n) {
@@ -238,15 +241,15 @@ class BlockLU {
     const int n1 = split(n), n2 = n - n1;
     rec(M, Li, Ui, n1, wo);
     // U12 = L11^-1 A12, L21 = A21 U11^-1 (independent); A22 -= L21 U12
-    const Mat<T> U12{rw + wo, n1, rws}, L21{rw + wo + (long long)n1 * n2, n2, rws};
+    const Mat<T> U12{rw + wo, n1, rws}, L21{rw + wo + (long long)n1 * n2, pad4(n2), rws};
     fork();
     prod_LF(n1, n2, T(1), Li, M.at(0, n1), T(0), U12);
     lane2([&] { prod_FU(n2, n1, T(1), M.at(n1, 0), Ui, T(0), L21); });
     join();
     gemm(n2, n2, n1, T(-1), L21, U12, T(1), M.at(n1, n1));
-    rec(M.at(n1, n1), Li.at(n1, n1), Ui.at(n1, n1), n2, wo + 2LL * n1 * n2);
+    rec(M.at(n1, n1), Li.at(n1, n1), Ui.at(n1, n1), n2, wo + (long long)n1 * n2 + (long long)pad4(n2) * n1);
     // (L^-1)21 = -L22^-1 L21 L11^-1, (U^-1)12 = -U11^-1 U12 U22^-1 (independent)
-    const Mat<T> Tl{W.p, n2, W.s}, Tu{W.p + (long long)n1 * n2, n1, W.s};
+    const Mat<T> Tl{W.p, pad4(n2), W.s}, Tu{W.p + (long long)pad4(n2) * n1, n1, W.s};
     fork();
     prod_FL(n2, n1, T(1), L21, Li, T(0), Tl);
     prod_LF(n2, n1, T(-1), Li.at(n1, n1), Tl, T(0), Li.at(n1, 0));

@@ -9,7 +9,8 @@ accumulation), far below a layout, swizzle or descriptor error, which shows
 as O(1) errors; against the product of the inputs rounded to nearest TF32
 the bound is 2^-18 (|A| |B|)_ij, the FP32 accumulation alone.  Shapes cover ragged tiles in every
 dimension, the three tile widths, sub-matrix views with leading dimensions
-larger than the rows, batches, alpha / beta, and K not a multiple of 32."""
+larger than the rows, batches, alpha / beta, K not a multiple of 32, and
+grids with more tiles than resident CTAs (the persistent loop)."""
 import numpy as np
 import pytest
 
@@ -63,7 +64,9 @@ def run_case(m, n, k, batch, alpha, beta, pad=(0, 0, 0), seed=0):
 
 @pytest.mark.parametrize("m,n,k,batch", [
     (128, 256, 32, 1), (1, 1, 1, 1), (31, 47, 5, 2), (129, 257, 33, 3), (128, 64, 64, 4), (200, 100, 300, 2),
-    (384, 512, 1024, 2), (3168, 96, 64, 1), (96, 3168, 160, 1), (1000, 1000, 1000, 1)])
+    (384, 512, 1024, 2), (3168, 96, 64, 1), (96, 3168, 160, 1), (1000, 1000, 1000, 1),
+    # more tiles than resident CTAs: every CTA walks several tiles, both accumulators in turn
+    (800, 800, 96, 16), (1000, 50, 64, 40), (300, 120, 40, 70)])
 def test_tc_gemm_matches_fp64_of_tf32_inputs(m, n, k, batch):
     run_case(m, n, k, batch, 1.0, 0.0, seed=m + n + k)
 
