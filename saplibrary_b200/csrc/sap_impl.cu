@@ -280,8 +280,10 @@ class PrecondT : public PrecBase {
     wide_active = true;
   }
 
-  // spikes and reduced system of the block path
-  // (offd: the row-major coupling blocks on the device, released afterwards)
+  // spikes and reduced system of the block path (offd: the row-major
+  // coupling blocks on the device, kept for the next setup of the same
+  // layout: at the 1M-row workload it is 1.2 GB, whose allocation and
+  // release every setup cost a device synchronisation each)
   void wide_couple(const std::vector<int>& iface) {
     auto t0 = Clock::now();
     wide->spikes(offd.get(), iface, K);
@@ -289,7 +291,6 @@ class PrecondT : public PrecBase {
     t0 = Clock::now();
     wide->reduced(offd.get(), iface, o.safeFactorization != 0);
     t_fullLU = ms_since(t0);
-    offd.release();
   }
 
   void setup_rowmajor(const double* A_dev, int n_, int K_) override {
