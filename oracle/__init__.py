@@ -242,3 +242,88 @@ class SparsePrecond:
         _sparse_lib().orc_sparse_solve(self.h, b.size, _p(rp), _p(ci), _p(v), _p(b), _p(x), L, maxit, reltol,
                                        abstol, ctypes.byref(res))
         return x, res
+
+
+# ---- the reference's own reordering pipeline (sap/graph.h) -----------------------
+# oracle/_ref/libref_graph.so is sap/graph.h of the reference compiled from its
+# source tree against the CUSP stand-in in oracle/ref_graph (build_ref.sh);
+# it needs a GPU at run time (DB's device vectors and weight kernel).
+REF_LIB = os.path.join(HERE, "_ref", "libref_graph.so")
+REF_SRC = "/root/reference"
+
+
+def build_ref(force: bool = False) -> str | None:
+    """Compile the reference's graph.h when the reference tree is present
+    (this container); on a machine without it the prebuilt library is used."""
+    if not os.path.isdir(REF_SRC):
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    srcs = [os.path.join(HERE, "ref_graph", "ref_graph_driver.cu"), os.path.join(HERE, "ref_graph", "cusp", "shim.h")]
+    newest = max(os.path.getmtime(s) for s in srcs)
+    if force or not os.path.exists(REF_LIB) or os.path.getmtime(REF_LIB) < newest:
+        subprocess.run(["sh", os.path.join(HERE, "ref_graph", "build_ref.sh"), REF_SRC], check=True)
+    return REF_LIB
+
+
+class RefInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("K", ctypes.c_int), ("P", ctypes.c_int), ("k_db", ctypes.c_int),
+                ("k_reorder", ctypes.c_int), ("varBand", ctypes.c_int), ("status", ctypes.c_int),
+                ("drop_actual", ctypes.c_double)]
+
+
+_ref = None
+
+
+def ref_lib():
+    """The reference's graph.h pipeline (None when its library is absent)."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            return None
+        L = ctypes.CDLL(REF_LIB)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.ref_graph_run.restype = vp
+        L.ref_graph_run.argtypes = [i, vp, vp, vp, i, i, d, i, i, i, i, ctypes.c_char_p, i]
+        L.ref_graph_info_get.argtypes = [vp, ctypes.POINTER(RefInfo)]
+        L.ref_graph_ints.restype = ctypes.c_longlong
+        L.ref_graph_ints.argtypes = [vp, i, vp]
+        L.ref_graph_destroy.argtypes = [vp]
+        _ref = L
+    return _ref
+
+
+class RefGraph:
+    """One run of the reference's reorder pipeline (Graph::reorder, dropOff,
+    assembleOffDiagMatrices, secondLevelReordering, assembleBandedMatrix and
+    the permutation composition of Precond::transformToBandedMatrix) on a
+    CSR matrix; the integer outputs use the names of INT_NAMES."""
+
+    def __init__(self, rp, ci, v, P, dtype="float", doDB=True, scale=True, dropFrac=0.0, maxBandwidth=2**31 - 1,
+                 varBand=True):
+        L = ref_lib()
+        if L is None:
+            raise RuntimeError("oracle/_ref/libref_graph.so is not built")
+        self._csr = [np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32),
+                     np.ascontiguousarray(v, np.float64)]
+        msg = ctypes.create_string_buffer(256)
+        self.h = L.ref_graph_run(self._csr[0].size - 1, *[_p(a) for a in self._csr], 0 if dtype == "float" else 1,
+                                 int(P), float(dropFrac), int(doDB), int(scale), int(maxBandwidth), int(varBand),
+                                 msg, 256)
+        self.message = msg.value.decode()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref_lib().ref_graph_destroy(self.h)
+            self.h = None
+
+    def info(self) -> RefInfo:
+        s = RefInfo()
+        ref_lib().ref_graph_info_get(self.h, ctypes.byref(s))
+        return s
+
+    def ints(self, name: str) -> np.ndarray:
+        w = INT_NAMES.index(name)
+        cnt = ref_lib().ref_graph_ints(self.h, w, None)
+        out = np.empty(cnt, np.int32)
+        if cnt:
+            ref_lib().ref_graph_ints(self.h, w, _p(out))
+        return out

@@ -461,7 +461,9 @@ static int dropOff(Graph<T>& g, T frac, int maxBandwidth, T& frac_actual) {
   }
   frac_actual = T(1) - norm_out / norm_in;
   nnz -= first;
-  // rebuild: stable counting sort by column, then (stable, from the end) by row
+  // rebuild: stable counting sort by column, then by row with a forward pass
+  // that takes slots from the end of each row (graph.h:719-733), which leaves
+  // every row in decreasing column order
   std::fill(bucket.begin(), bucket.end(), 0);
   for (int l = 0; l < nnz; l++) bucket[cc[l]]++;
   {
@@ -479,7 +481,7 @@ static int dropOff(Graph<T>& g, T frac, int maxBandwidth, T& frac_actual) {
   for (int d = 1; d < n; d++) bucket[d] += bucket[d - 1];
   std::vector<int> rr(nnz), rc(nnz);
   std::vector<T> rv(nnz);
-  for (int l = nnz - 1; l >= 0; l--) {
+  for (int l = 0; l < nnz; l++) {
     int idx = --bucket[tr[l]];
     rr[idx] = tr[l]; rc[idx] = tc[l]; rv[idx] = tv[l];
   }
@@ -563,9 +565,10 @@ static void assembleOffDiag(Graph<T>& g, int K, int P, std::vector<T>& WV, std::
 
 // partitionedRCM (graph.h:1593-1757) on the diagonal matrix's edges
 // [e0, e1) and nodes [nb, ne).  Quirks kept: BFS priority is the symmetrised
-// topology degree, the start node uses the CSR row lengths, a later trial's
-// start uses the degrees of the partition's first `count` nodes, and
-// max_level is the level of the last node assigned.
+// topology degree, the start node uses the CSR row lengths (the partition's
+// last node counted with length 0), a later trial's start uses the degrees
+// of the partition's first `count` nodes, and max_level is the level of the
+// last node assigned.
 template <typename T>
 static void partitionedRCM(Graph<T>& g, int e0, int e1, int nb, int ne, std::vector<int>& optReordering,
                            std::vector<int>& optPerm, const std::vector<int>& row_idx) {
@@ -578,8 +581,10 @@ static void partitionedRCM(Graph<T>& g, int e0, int e1, int nb, int ne, std::vec
   const int MAX_NUM_TRIAL = 5, BANDWIDTH_THRESHOLD = 128;
   std::vector<char> tried(n, 0);
   std::vector<int> pushed(ne, -1), levels(n, 0);
-  std::vector<int> ori_degrees(ne - nb);
-  for (int i = nb; i < ne; i++) ori_degrees[i - nb] = g.drp[i + 1] - g.drp[i];
+  // graph.h:1622-1625: the transform over row_offsets[nb+1 .. ne) fills
+  // ne - nb - 1 of the ne - nb degrees; the last node's stays 0
+  std::vector<int> ori_degrees(ne - nb, 0);
+  for (int i = nb; i < ne - 1; i++) ori_degrees[i - nb] = g.drp[i + 1] - g.drp[i];
   int max_level = 0, p_max_level = 0;  // the reference leaves these uninitialised
   std::vector<int>& buf = g.buffer_reordering;
   for (int trial = 0; trial < MAX_NUM_TRIAL; trial++) {
@@ -1076,7 +1081,9 @@ int orc_sparse_setup(void* h, int n, const int* rp, const int* ci, const double*
     try {
       orc::sparse_reorder(sp, n, rp, ci, v, factor != 2);
       if (factor == 2) factor = 0;
-      if (!sp.varBand && sp.P > 1) { sp.status = -103; sp.msg = "constant band with reordering not restated"; }
+      // the permutations of a constant band are restated; its factorisation
+      // after reordering is not
+      if (factor && !sp.varBand && sp.P > 1) { sp.status = -103; sp.msg = "constant band with reordering not restated"; }
       else if (factor) orc::sparse_factor(sp);
     } catch (const orc::DBError& e) {
       sp.status = e.code;

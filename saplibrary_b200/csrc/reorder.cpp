@@ -693,8 +693,10 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     }
   }
   drop_actual = T(1) - kept / total;
-  // kept: every entry within distance g, sorted by row, then column (what
-  // the reference's two stable counting sorts of the kept list give)
+  // kept: every entry within distance g, by row and, inside a row, by
+  // decreasing column: the reference counting-sorts the kept list by column,
+  // then places it by row in a forward pass that fills each row from its end
+  // (graph.h:705-733)
   const int dkeep = g;
   tmp_rp.swap(m_rp);
   tmp_ci.swap(m_ci);
@@ -718,9 +720,9 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     int w = a;
     for (int e = rp0[i]; e < rp0[i + 1]; e++) {
       if (std::abs(i - ci0[e]) > dkeep) continue;
-      // insertion by column (columns of a row are distinct)
+      // insertion by decreasing column (columns of a row are distinct)
       int t = w++;
-      while (t > a && m_ci[t - 1] > ci0[e]) {
+      while (t > a && m_ci[t - 1] < ci0[e]) {
         m_ci[t] = m_ci[t - 1];
         m_val[t] = m_val[t - 1];
         t--;
@@ -837,8 +839,12 @@ void Pipeline<T>::second_level(int K, int P) {
     std::vector<int> off, adj;
     const int obase = serial ? 0 : nb;
     symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj, obase);
-    std::vector<int> rowlen(ne - nb);
-    for (int i = nb; i < ne; i++) rowlen[i - nb] = d_rp[i + 1] - d_rp[i];
+    // row lengths of the partition's nodes as the reference computes them:
+    // its transform covers row_offsets[nb+1 .. ne), one element short, so the
+    // partition's last node keeps degree 0 (graph.h:1622-1625), which makes
+    // it the first trial's root unless a node has no entries at all
+    std::vector<int> rowlen(ne - nb, 0);
+    for (int i = nb; i < ne - 1; i++) rowlen[i - nb] = d_rp[i + 1] - d_rp[i];
     std::vector<char> tried_own;
     std::vector<int> pushed_own, level_own;
     if (serial) {
