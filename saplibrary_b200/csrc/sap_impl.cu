@@ -248,7 +248,8 @@ class PrecondT : public PrecBase {
     size_t fr = 0, tot = 0;
     SAPB_CUDA(cudaMemGetInfo(&fr, &tot));
     if (wide) fr += wide->bytes_held();  // reused (or released) by the new setup
-    const double need = WideBand<T>::factor_bytes(n, P, kmax, h16 && sizeof(T) == 4);
+    const double need = WideBand<T>::factor_bytes(n, P, kmax, h16 && sizeof(T) == 4,
+                                                  tf32 && sizeof(T) == 4 && WideBand<T>::tc_gemm_enabled());
     if (need > 0.92 * (double)fr)
       throw Error(SAP_ERR_OUT_OF_MEMORY, "wide-band factors need " + std::to_string(need / 1e9) + " GB, " +
                                              std::to_string((double)fr / 1e9) + " GB free");
@@ -276,7 +277,8 @@ class PrecondT : public PrecBase {
       pz[p] = parts_h[p].size;
     }
     if (!wide) wide = std::make_unique<WideBand<T>>();
-    wide->init(st, n, WideBand<T>::block_size(kmax), ps, pz, tf32, h16);
+    wide->init(st, n, WideBand<T>::block_size(kmax, tf32 && sizeof(T) == 4 && WideBand<T>::tc_gemm_enabled()), ps, pz,
+               tf32, h16);
     wide_active = true;
   }
 

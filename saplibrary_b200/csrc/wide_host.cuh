@@ -342,12 +342,24 @@ class WideBand {
   cublasHandle_t h2 = nullptr;                  // bound to st2 (second lane of the factorization)
 
   // Block size bs >= the largest half-bandwidth, a multiple of the leaf size.
-  static int block_size(int kmax) { return std::max(kLeaf, ((kmax + kLeaf - 1) / kLeaf) * kLeaf); }
+  // Larger blocks mean fewer block rows, hence fewer dependent launches per
+  // partition, for more factor flops and sweep bytes; with the tensor-core
+  // TF32 products the flops are cheap and bs is at least 448 (2M-row K = 200
+  // workload, TF32 + FGMRES: 0.154 s at bs 448 against 0.221 / 0.179 / 0.182 s
+  // at 224 / 672 / 896; FP32 and FP64 are fastest at the smallest bs).
+  // SAPB_BLOCK_SIZE raises it further.
+  static int block_size(int kmax, bool tf32_products = false) {
+    int bs = std::max(kLeaf, ((kmax + kLeaf - 1) / kLeaf) * kLeaf);
+    if (tf32_products) bs = std::max(bs, 448);
+    const char* e = std::getenv("SAPB_BLOCK_SIZE");
+    if (e && std::atoi(e) > bs) bs = ((std::atoi(e) + kLeaf - 1) / kLeaf) * kLeaf;
+    return bs;
+  }
 
   // Device bytes of the factors, their FP16 copies (h16) and the
   // factorization workspaces for n rows in P partitions (for the memory check).
-  static double factor_bytes(int n, int P, int kmax, bool h16 = false) {
-    const double b = block_size(kmax);
+  static double factor_bytes(int n, int P, int kmax, bool h16 = false, bool tf32_products = false) {
+    const double b = block_size(kmax, tf32_products);
     const double nbp = std::ceil((double)(n / P + 1) / b);
     return ((4.0 * nbp + 3.0) * sizeof(T) + (h16 ? 4.0 * nbp * 2.0 : 0.0)) * P * b * b;
   }
