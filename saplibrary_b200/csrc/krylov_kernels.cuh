@@ -25,29 +25,75 @@ k_spmv_banded(const double* __restrict__ A, const double* __restrict__ x, double
   }
 }
 
-// y = A x, FP64 CSR (the product SpmvCusp delegates to, sap/spmv.h:110-121):
-// a group of LANES threads per row.  The row loop runs over warp-uniform
-// bases (a warp serves 32 / LANES consecutive rows per step), so every lane
-// of a warp takes the same number of steps and the full-mask shuffles never
-// name a lane that has left the loop; rows past n contribute nothing.
-template <int LANES>
-__global__ void __launch_bounds__(256)
-k_spmv_csr(const int* __restrict__ rp, const int* __restrict__ ci, const double* __restrict__ v,
-           const double* __restrict__ x, double* __restrict__ y, int n) {
-  constexpr int kRowsPerWarp = 32 / LANES;
-  const int lane = threadIdx.x & 31;
-  const int sub = lane % LANES;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long stride = (((long long)gridDim.x * blockDim.x) >> 5) * kRowsPerWarp;
-  for (long long i0 = warp * kRowsPerWarp; i0 < n; i0 += stride) {
-    const long long i = i0 + lane / LANES;
-    double acc = 0.0;
-    if (i < n)
-      for (int p = rp[i] + sub; p < rp[i + 1]; p += LANES) acc += v[p] * __ldg(x + ci[p]);
+// y = A x, FP64 CSR by row blocks (the product SpmvCusp delegates to,
+// sap/spmv.h:110-121).  The rows are cut on the host into blocks of at most
+// kSpmvRows rows and kSpmvNnz entries (csr_row_blocks); a row longer than
+// kSpmvNnz is a block of its own.  A CTA streams its block's entries with
+// fully coalesced loads of values and column indices, several per thread
+// before their gathers of x, keeps the products in shared memory, then one
+// thread per row adds its row's products in entry order.  A long row is
+// summed by the whole CTA (strided partial sums, then a fixed-order
+// reduction).
+constexpr int kSpmvRows = 256;   // threads per CTA, rows per block at most
+constexpr int kSpmvNnz = 2048;   // entries per block at most (16 KB of products)
+
+static __global__ void __launch_bounds__(kSpmvRows)
+k_spmv_csr_blocks(const int* __restrict__ blk, const int* __restrict__ rp, const int* __restrict__ ci,
+                  const double* __restrict__ v, const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double prod[kSpmvNnz];
+  const int r0 = blk[blockIdx.x], r1 = blk[blockIdx.x + 1];
+  const int e0 = rp[r0], cnt = rp[r1] - e0;
+  const int t = threadIdx.x;
+  if (cnt <= kSpmvNnz) {
+    constexpr int U = kSpmvNnz / kSpmvRows;
+    int c[U];
+    double a[U];
 #pragma unroll
-    for (int off = LANES / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, LANES);
-    if (sub == 0 && i < n) y[i] = acc;
+    for (int u = 0; u < U; u++) {
+      const int k = t + u * kSpmvRows;
+      c[u] = k < cnt ? __ldg(ci + e0 + k) : 0;
+      a[u] = k < cnt ? __ldg(v + e0 + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int k = t + u * kSpmvRows;
+      if (k < cnt) prod[k] = a[u] * __ldg(x + c[u]);
+    }
+    __syncthreads();
+    const int row = r0 + t;
+    if (row < r1) {
+      const int a0 = rp[row] - e0, a1 = rp[row + 1] - e0;
+      double s = 0.0;
+      for (int k = a0; k < a1; k++) s += prod[k];
+      y[row] = s;
+    }
+  } else {  // one long row
+    double s = 0.0;
+    for (int k = t; k < cnt; k += kSpmvRows) s += __ldg(v + e0 + k) * __ldg(x + __ldg(ci + e0 + k));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if ((t & 31) == 0) prod[t >> 5] = s;
+    __syncthreads();
+    if (t == 0) {
+      double tot = 0.0;
+      for (int w = 0; w < kSpmvRows / 32; w++) tot += prod[w];
+      y[r0] = tot;
+    }
   }
+}
+
+// Row blocks of k_spmv_csr_blocks: boundaries b[0] = 0 < b[1] < ... = n, each
+// block at most kSpmvRows rows and kSpmvNnz entries, or one longer row.
+inline std::vector<int> csr_row_blocks(int n, const int* rp) {
+  std::vector<int> b(1, 0);
+  int r = 0;
+  while (r < n) {
+    const int r0 = r;
+    while (r < n && r - r0 < kSpmvRows && rp[r + 1] - rp[r0] <= kSpmvNnz) r++;
+    if (r == r0) r = r0 + 1;  // a row longer than kSpmvNnz
+    b.push_back(r);
+  }
+  return b;
 }
 
 // z = a*x + b*y (cusp::blas::axpby)

@@ -78,6 +78,8 @@ struct Csr {
   int n = 0, nnz = 0;
   DBuf<int> rp, ci;
   DBuf<double> v;
+  DBuf<int> blk;  // row blocks of k_spmv_csr_blocks
+  int nblk = 0;
   std::vector<int> rp_h, ci_h;  // host copies of the pattern (reordering runs on the host)
   std::vector<double> v_h;
 };
@@ -96,12 +98,8 @@ struct Spmv {
       SAPB_LAUNCHED();
     } else if (kind == 1) {
       SAPB_PROF("spmv_csr", s);
-      double avg = csr->n ? (double)csr->nnz / csr->n : 0;
-      if (avg <= 12) {
-        k_spmv_csr<4><<<grid_for((long long)csr->n * 4, 256, 148 * 64), 256, 0, s>>>(csr->rp.get(), csr->ci.get(), csr->v.get(), x, y, csr->n);
-      } else {
-        k_spmv_csr<32><<<grid_for((long long)csr->n * 32, 256, 148 * 64), 256, 0, s>>>(csr->rp.get(), csr->ci.get(), csr->v.get(), x, y, csr->n);
-      }
+      k_spmv_csr_blocks<<<csr->nblk, kSpmvRows, 0, s>>>(csr->blk.get(), csr->rp.get(), csr->ci.get(), csr->v.get(),
+                                                         x, y);
       SAPB_LAUNCHED();
     } else {
       fn(ctx, x, y, (void*)s);
@@ -1721,6 +1719,11 @@ int sap_csr_create(int n, int nnz, const int* rp, const int* ci, const double* v
     h->c.rp.upload(h->c.rp_h, nullptr);
     h->c.ci.upload(h->c.ci_h, nullptr);
     h->c.v.upload(h->c.v_h, nullptr);
+    {
+      const std::vector<int> blk = csr_row_blocks(n, h->c.rp_h.data());
+      h->c.nblk = (int)blk.size() - 1;
+      h->c.blk.upload(blk, nullptr);
+    }
     SAPB_CUDA(cudaDeviceSynchronize());
     *out = h.release();
   });

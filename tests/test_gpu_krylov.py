@@ -49,3 +49,26 @@ def test_minres_matches_oracle_on_spd_band(n, K, P):
     assert s.getMonitorCode() > 0
     assert s.getStats().numIterations == res.iterations
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-9
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_csr_spmv_row_blocks_with_empty_and_long_rows(seed):
+    # the row-block CSR SpMV: rows of 0 .. 11 entries, empty rows, a few rows
+    # longer than one block's entry budget (the CTA-wide branch), ragged sizes
+    rng = np.random.default_rng(seed)
+    n = 30011
+    lens = rng.integers(0, 12, n)
+    lens[rng.integers(0, n, 50)] = 0
+    lens[rng.integers(0, n, 3)] = 5000 + seed
+    lens[-1] = 3000
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens]).astype(np.int32)
+    v = rng.standard_normal(rp[-1])
+    A = sap.CsrMatrix(rp, ci, v)
+    x = rng.standard_normal(n)
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    sap.SpmvCusp(A)(torch.tensor(x, device="cuda"), y)
+    rows = np.repeat(np.arange(n), lens)
+    ref = np.bincount(rows, weights=v * x[ci], minlength=n)
+    scale = np.bincount(rows, weights=np.abs(v * x[ci]), minlength=n)
+    assert np.all(np.abs(y.cpu().numpy() - ref) <= 1e-14 * scale + 1e-300)
