@@ -173,6 +173,190 @@ k_factor_smem(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restri
   }
 }
 
+// Blocked form of k_factor_smem for K <= 32 R - NB: the same elimination,
+// every element receiving the same updates in the same order (hence the same
+// factors bit for bit), with two CTA barriers per panel of NB pivots instead
+// of two per pivot.
+//
+// Panel p covers columns j0 = p NB .. j0 + NB - 1.  Warp 0 factors it in
+// registers: lane l holds rows j0 + l + 32 t (t < R) of the NB panel columns,
+// each pivot is broadcast by a shuffle, its column is divided by it and the
+// rest of the panel receives the rank-1 update.  After a barrier the warps
+// apply the panel to the K columns right of it, four columns per warp at once
+// (the columns' rows in registers, the U element of each pivot broadcast from
+// the lane holding that row, each L entry read once from shared memory for
+// the four), pivots in order.  While warp 0 factors, the other warps write
+// back the previous panel (post-divided by the pivots of its U rows) and
+// fetch, with cp.async into the freed slots, the NB columns that panel p + DPF
+// will first touch.  The ring holds W = K + NB (1 + DPF) column slots; slots
+// advance by additions, with no modulo.
+template <typename T, int NB, int R>
+__global__ void __launch_bounds__(512)
+k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restrict__ B2,
+               int do_boost, int* __restrict__ zero_flag, int DPF) {
+  constexpr int CPW = 4;  // columns a warp applies a panel to at once
+  const FactorJob jb = jobs[blockIdx.x];
+  const int K = jb.K, SW = 2 * K + 1, np = jb.e - jb.s, W = K + NB * (1 + DPF);
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* win = reinterpret_cast<T*>(sm_raw);
+  T* piv = win + (size_t)W * SW;  // piv[r % W]: the pivot of row r
+  T* band = (jb.target ? B2 : B) + jb.boff;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int ct = tid - 32, nct = blockDim.x - 32;  // copy threads: warps 1..
+  const bool mir = jb.mirror != 0;
+  auto gidx = [&](int i, int p) -> long long {
+    int col = mir ? (np - 1 - i) : i;
+    int pos = mir ? (2 * K - p) : p;
+    return (long long)col * SW + pos;
+  };
+  auto wrap = [&](int s) { return s >= W ? s - W : s; };  // for 0 <= s < 2 W
+  // column `col` from ring slot `sl` to the band, its U entries post-divided
+  auto out = [&](int col, int sl, int p) {
+    T v = win[sl * SW + p];
+    if (p < K && col - K + p >= 0) {
+      int pr = sl + p - K;
+      v /= piv[pr < 0 ? pr + W : pr];
+    }
+    band[gidx(col, p)] = v;
+  };
+  if (ct >= 0) {  // columns [0, K + NB), then one panel's new columns per group; all in slots == column
+    for (int g = 0; g < DPF; g++) {
+      const int c0 = g == 0 ? 0 : K + g * NB, c1 = min(np, K + (g + 1) * NB);
+      for (int e = ct; e < (c1 - c0) * SW; e += nct) {
+        const int c = c0 + e / SW, p = e - (c - c0) * SW;
+        cp_async_val<T>(&win[c * SW + p], band + gidx(c, p));
+      }
+      cp_async_commit();
+    }
+  }
+  int j0 = 0, s0 = 0;  // s0 = j0 % W
+  for (; j0 < np; j0 += NB, s0 = wrap(s0 + NB)) {
+    const int nb = min(NB, np - j0);
+    if (DPF == 2) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();
+    if (warp != 0) {
+      // write back panel p-1 and fetch the columns of panel p+DPF into its slots
+      // (the thread that reads a slot element issues the copy into it)
+      const int nf0 = j0 + DPF * NB + K;
+      const int sp = s0 - NB < 0 ? s0 - NB + W : s0 - NB;
+      for (int e = ct; e < NB * SW; e += nct) {
+        const int c = e / SW, p = e - c * SW, sl = wrap(sp + c);
+        if (j0 > 0) out(j0 - NB + c, sl, p);
+        if (nf0 + c < np) cp_async_val<T>(&win[sl * SW + p], band + gidx(nf0 + c, p));
+      }
+      cp_async_commit();
+    } else {
+      T a[R][NB];
+#pragma unroll
+      for (int c = 0; c < NB; c++) {
+        const T* colp = win + wrap(s0 + c) * SW;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+          const int pos = K + lane + 32 * t - c;  // row j0 + lane + 32 t
+          a[t][c] = (c < nb && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) ? colp[pos] : T(0);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+        if (k < nb) {
+          const int w = min(K, np - 1 - (j0 + k));
+          T p = __shfl_sync(0xffffffffu, a[0][k], k);
+          if (do_boost) p = boost_pivot(p);
+          else if (lane == 0 && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
+          T u[NB];
+#pragma unroll
+          for (int c = k + 1; c < NB; c++) u[c] = __shfl_sync(0xffffffffu, a[0][c], k);
+#pragma unroll
+          for (int t = 0; t < R; t++) {
+            const int rr = lane + 32 * t - k;  // row - pivot row
+            if (rr == 0) {
+              a[t][k] = p;
+            } else if (rr >= 1 && rr <= w) {
+              const T l = a[t][k] / p;
+              a[t][k] = l;
+#pragma unroll
+              for (int c = k + 1; c < NB; c++)
+                if (c - k <= w) a[t][c] -= l * u[c];
+            }
+          }
+          if (lane == 0) piv[wrap(s0 + k)] = p;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NB; c++) {
+        T* colp = win + wrap(s0 + c) * SW;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+          const int pos = K + lane + 32 * t - c;
+          if (c < nb && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) colp[pos] = a[t][c];
+        }
+      }
+    }
+    __syncthreads();
+    // the panel applied to the (up to K) columns right of it, CPW columns per warp at once,
+    // pivots in order: x(r, jc) -= L(r, j) U(j, jc)
+    const int nt = min(K, np - j0 - nb);
+    for (int q0 = warp * CPW; q0 < nt; q0 += nw * CPW) {
+      T x[CPW][R];
+      T* colp[CPW];
+      int kst[CPW];
+#pragma unroll
+      for (int i = 0; i < CPW; i++) {
+        const int q = q0 + i;  // column j0 + nb + q
+        colp[i] = win + wrap(s0 + nb + q) * SW;
+        kst[i] = q < nt ? max(0, nb + q - K) : NB;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+          const int pos = K + lane + 32 * t - nb - q;
+          x[i][t] = (q < nt && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) ? colp[i][pos] : T(0);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+        if (k < nb) {
+          const int w = min(K, np - 1 - (j0 + k));
+          const T* lc = win + wrap(s0 + k) * SW + K;
+          T L[R];
+#pragma unroll
+          for (int t = 0; t < R; t++) {
+            const int rr = lane + 32 * t - k;
+            L[t] = (rr >= 1 && rr <= w) ? lc[rr] : T(0);
+          }
+#pragma unroll
+          for (int i = 0; i < CPW; i++) {
+            if (k >= kst[i]) {
+              const T U = __shfl_sync(0xffffffffu, x[i][0], k);
+#pragma unroll
+              for (int t = 0; t < R; t++) {
+                const int rr = lane + 32 * t - k;
+                if (rr >= 1 && rr <= w) x[i][t] -= L[t] * U;
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < CPW; i++) {
+        const int q = q0 + i;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+          const int pos = K + lane + 32 * t - nb - q;
+          if (q < nt && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) colp[i][pos] = x[i][t];
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // the last panel: columns [j0 - NB, np) in slots from s0 - NB on
+  const int jl = j0 - NB, sl0 = s0 - NB < 0 ? s0 - NB + W : s0 - NB;
+  for (int e = tid; e < (np - jl) * SW; e += blockDim.x) {
+    const int c = e / SW;
+    out(jl + c, wrap(sl0 + c), e - c * SW);
+  }
+}
+
 // Same factorisation operating directly on the band in global memory, for
 // half-bandwidths whose window does not fit in shared memory.
 template <typename T>

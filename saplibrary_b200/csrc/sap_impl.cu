@@ -820,7 +820,29 @@ class PrecondT : public PrecBase {
     NT = std::max(NT, 64);
     constexpr int D = 8;
     size_t smem = ((size_t)(Kmax + 1 + D) * (2 * Kmax + 1) + (Kmax + 1 + D)) * sizeof(T);
-    if (smem <= 200 * 1024) {
+    constexpr int NB = 8;
+    const char* fk = std::getenv("SAPB_FACTOR_KERNEL");
+    const bool ring_only = fk && std::string(fk) == "ring";
+    const int R = (Kmax + NB + 31) / 32;
+    auto panel_smem = [&](int dpf) {
+      return (size_t)(Kmax + NB * (1 + dpf)) * (2 * Kmax + 2) * sizeof(T);
+    };
+    if (!ring_only && R <= 4 && panel_smem(1) <= 227 * 1024) {
+      const int dpf = panel_smem(2) <= 227 * 1024 ? 2 : 1;
+      const size_t psm = panel_smem(dpf);
+      const int nt = 32 * std::min(16, std::max(2, (Kmax + 3) / 4));  // four trailing columns per warp
+      auto launch = [&](auto kern) {
+        SAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+        SAPB_PROF("factor", st);
+        kern<<<(int)jobs.size(), nt, psm, st>>>(jobs_d.get(), B.get(), B2.get(), boost ? 1 : 0, flag.get(), dpf);
+      };
+      switch (R) {
+        case 1: launch(k_factor_panel<T, NB, 1>); break;
+        case 2: launch(k_factor_panel<T, NB, 2>); break;
+        case 3: launch(k_factor_panel<T, NB, 3>); break;
+        default: launch(k_factor_panel<T, NB, 4>); break;
+      }
+    } else if (smem <= 200 * 1024) {
       SAPB_CUDA(cudaFuncSetAttribute(k_factor_smem<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       SAPB_PROF("factor", st);
       k_factor_smem<T, D><<<(int)jobs.size(), NT, smem, st>>>(jobs_d.get(), B.get(), B2.get(), boost ? 1 : 0,
