@@ -5,9 +5,10 @@ the benchmark workload.
     python -m saplibrary_b200.spmv_bench [--m 1000] [--reps 20]
 
 Prints one JSON line: the best and median device time of y = A x over
-`reps` launches (CUDA events on the calling stream around one launch each,
-the L2 flushed before every launch by writing a 256 MB buffer, whose kernel
-also covers the host's launch latency), the algorithmic bytes of one
+`reps` launches (the library's CUDA events around the kernel on its
+launching stream; before every launch the L2 is flushed by writing a 256 MB
+buffer and then reading another, which leaves no dirty lines behind), the
+algorithmic bytes of one
 product, 12 nnz + 4 (n + 1) + 8 n (x) + 8 n (y): values and column indices,
 row offsets, the source and the result vector, and the achieved GB/s
 against the measured HBM copy bandwidth recorded in MEASURED_PEAKS.json
@@ -46,18 +47,21 @@ def main() -> None:
     xh = np.random.default_rng(2).standard_normal(n)
     x = torch.tensor(xh, device="cuda")
     y = torch.empty_like(x)
+    from . import profile_read, profile_select
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    clean = torch.ones(64 << 20, dtype=torch.float32, device="cuda")
     spmv(x, y)  # warm-up
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     times = []
     for _ in range(a.reps):
         flush.fill_(1.0)
-        e0.record()
-        spmv(x, y)
-        e1.record()
+        clean.sum()
         torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+        profile_select("spmv_csr")
+        spmv(x, y)
+        ms, cnt = profile_read()
+        profile_select(None)
+        times.append(ms / max(cnt, 1))
     ref = csr_matvec(rp, ci, v, xh)
     err = float(np.abs(y.cpu().numpy() - ref).max() / np.abs(ref).max())
     bytes_ = 12 * nnz + 4 * (n + 1) + 16 * n
