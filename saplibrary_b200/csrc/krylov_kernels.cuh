@@ -173,6 +173,73 @@ k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ c
 }
 
 
+// Classical Gram-Schmidt of the Arnoldi step (flexible GMRES), one launch per
+// pass instead of one dot and one axpy per basis vector:
+//   k_mdot:  h[i] = V_i . w for i < m (blockIdx.y = i); block partials in
+//            part[i][blockIdx.x], reduced in block order by the last block of
+//            each vector to finish (deterministic for a given grid), whose
+//            counter returns to zero;
+//   k_maxpy: w[r] -= h[0] V_0[r] + ... in order i = 0..m-1, one row per
+//            thread (the basis pointers and h staged in shared memory).
+constexpr int kMdotBlocks = 64;
+constexpr int kMdotThreads = 256;
+constexpr int kMaxBasis = 64;
+static __global__ void __launch_bounds__(kMdotThreads)
+k_mdot(int n, const double* const* __restrict__ vs, const double* __restrict__ w, double* __restrict__ part,
+       unsigned int* __restrict__ ctr, double* __restrict__ h) {
+  __shared__ double red[kMdotThreads / 32];
+  __shared__ bool last;
+  const int i = blockIdx.y;
+  const double* v = vs[i];
+  double acc = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) acc += v[r] * w[r];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < kMdotThreads / 32; k++) s += red[k];
+    part[(size_t)i * gridDim.x + blockIdx.x] = s;
+    __threadfence();
+    last = atomicAdd(&ctr[i], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    volatile const double* pp = part + (size_t)i * gridDim.x;
+    double s = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) s += pp[b];
+    h[i] = s;
+    ctr[i] = 0u;
+  }
+}
+
+static __global__ void k_maxpy(int n, int m, const double* const* __restrict__ vs, const double* __restrict__ h,
+                               double* __restrict__ w) {
+  __shared__ const double* sv[kMaxBasis];
+  __shared__ double sh[kMaxBasis];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    sv[i] = vs[i];
+    sh[i] = h[i];
+  }
+  __syncthreads();
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double x = w[r];
+    for (int i = 0; i < m; i++) x -= sh[i] * sv[i][r];
+    w[r] = x;
+  }
+}
+
+// w <- w / sqrt(nn[0]) when nn[0] > 0 (the Arnoldi normalisation, with the
+// norm left on the device)
+static __global__ void k_scale_inv_norm(int n, double* __restrict__ w, const double* __restrict__ nn) {
+  const double hn = sqrt(nn[0]);
+  if (!(hn > 0)) return;
+  const double a = 1.0 / hn;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) w[r] = a * w[r] + 0.0 * w[r];
+}
+
 // out = a x + b y + c z (cusp::blas::axpbypcz); out may alias an input
 static __global__ void k_axpbypcz(int n, double a, const double* x, double b, const double* y, double c,
                                   const double* z, double* out) {

@@ -1064,6 +1064,11 @@ class Solver {
   // Krylov workspace
   DBuf<double> dots_part, dots_out;
   DBuf<unsigned int> dots_ctr;
+  // classical Gram-Schmidt of flexible GMRES: basis pointers, partials,
+  // counters, the two passes' coefficients
+  DBuf<const double*> gs_v;
+  DBuf<double> gs_part, gs_h;
+  DBuf<unsigned int> gs_ctr;
   double* pinned = nullptr;
   DBuf<double> bvec, xvec;
   // persistent Krylov vectors (allocated at the first solve of size n)
@@ -1090,7 +1095,7 @@ class Solver {
     dots_out.alloc(4);
     dots_ctr.alloc(1);
     dots_ctr.zero(st);
-    SAPB_CUDA(cudaMallocHost(&pinned, 8 * sizeof(double)));
+    SAPB_CUDA(cudaMallocHost(&pinned, (2 * kMaxBasis + 8) * sizeof(double)));
     init_stats();
   }
   ~Solver() {
@@ -1136,6 +1141,27 @@ class Solver {
     dots(1, &x, &y, &r);
     return r;
   }
+  // ||w||^2 into dots_out[0] on the device, no synchronisation
+  void sqnorm_dev(const double* w) {
+    DotArgs a{};
+    a.nq = 1;
+    a.x[0] = w;
+    a.y[0] = w;
+    SAPB_PROF("dots", st);
+    k_dots<<<kDotBlocks, kDotThreads, 0, st>>>(n, a, dots_part.get(), dots_ctr.get(), dots_out.get());
+    SAPB_LAUNCHED();
+  }
+  // one classical Gram-Schmidt pass against basis vectors 0..m-1 (device
+  // pointer array vs): h = V^T w, w -= V h
+  void cgs_pass(int m, const double* const* vs, double* w, double* h) {
+    {
+      SAPB_PROF("dots", st);
+      k_mdot<<<dim3(kMdotBlocks, m), kMdotThreads, 0, st>>>(n, vs, w, gs_part.get(), gs_ctr.get(), h);
+      SAPB_LAUNCHED();
+    }
+    k_maxpy<<<grid_for(n, 256), 256, 0, st>>>(n, m, vs, h, w);
+    SAPB_LAUNCHED();
+  }
   double nrm2(const double* x) { return std::sqrt(dot(x, x)); }
 
   // bicgstabl<..., L> (sap/bicgstab2.h:32-360)
@@ -1143,16 +1169,32 @@ class Solver {
 
   // Flexible GMRES(m) (Saad, SIAM J. Sci. Comput. 14 (1993) 461-469):
   // right preconditioning with the preconditioned directions z_j kept, so
-  // the preconditioner may vary between applies; FP64 Arnoldi with modified
-  // Gram-Schmidt, Givens rotations for the least-squares residual, the true
-  // residual b - A x checked after every cycle.  Monitor: 1 converged,
-  // -1 iteration budget, -2 NaN, -3 a cycle that did not lower the residual.
+  // the preconditioner may vary between applies; FP64 Arnoldi with classical
+  // Gram-Schmidt applied twice (CGS2: Giraud, Langou, Rozloznik, Comput.
+  // Math. Appl. 50 (2005) 1069-1075 -- orthogonal to working precision like
+  // modified Gram-Schmidt), each pass one multi-dot and one multi-axpy launch
+  // with the coefficients kept on the device, the norm and normalisation on
+  // the device, and one host synchronisation per Arnoldi step; Givens
+  // rotations for the least-squares residual, the true residual b - A x
+  // checked after every cycle.  Monitor: 1 converged, -1 iteration budget,
+  // -2 NaN, -3 a cycle that did not lower the residual.
   void fgmres(const Spmv& A, double* x, const double* b, int m) {
+    if (m + 1 > kMaxBasis) throw Error(SAP_ERR_UNSUPPORTED, "FGMRES restart length above the Gram-Schmidt limit");
     const double tol = mon.tol();
     double* r = wsv(39);
     std::vector<double*> Vb(m + 1), Zb(m);
     for (int i = 0; i <= m; i++) Vb[i] = wsv(40 + i);
     for (int i = 0; i < m; i++) Zb[i] = wsv(41 + m + i);
+    std::vector<const double*> vptr(Vb.begin(), Vb.end());
+    gs_v.upload(vptr, st);
+    gs_part.ensure((size_t)kMdotBlocks * kMaxBasis);
+    gs_h.ensure(2 * kMaxBasis);
+    if (gs_ctr.size() < (size_t)kMaxBasis) {
+      gs_ctr.alloc(kMaxBasis);
+      gs_ctr.zero(st);
+    }
+    double* h1 = gs_h.get();
+    double* h2 = gs_h.get() + kMaxBasis;
     std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m, 0.0), sn(m, 0.0), g(m + 1, 0.0);
     auto h = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
     auto residual = [&]() {
@@ -1175,14 +1217,19 @@ class Solver {
       while (j < m && total < mon.maxIt) {
         pcp->apply(Vb[j], Zb[j]);
         A.apply(Zb[j], Vb[j + 1], st);
-        for (int i = 0; i <= j; i++) {
-          const double hij = dot(Vb[j + 1], Vb[i]);
-          h(i, j) = hij;
-          axpy(Vb[i], Vb[j + 1], -hij);
-        }
-        const double hn = nrm2(Vb[j + 1]);
+        cgs_pass(j + 1, gs_v.get(), Vb[j + 1], h1);
+        cgs_pass(j + 1, gs_v.get(), Vb[j + 1], h2);
+        sqnorm_dev(Vb[j + 1]);
+        k_scale_inv_norm<<<grid_for(n, 256), 256, 0, st>>>(n, Vb[j + 1], dots_out.get());
+        SAPB_LAUNCHED();
+        SAPB_CUDA(cudaMemcpyAsync(pinned, gs_h.get(), (size_t)(j + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        SAPB_CUDA(cudaMemcpyAsync(pinned + kMaxBasis, h2, (size_t)(j + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                                  st));
+        SAPB_CUDA(cudaMemcpyAsync(pinned + 2 * kMaxBasis, dots_out.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+        SAPB_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i <= j; i++) h(i, j) = pinned[i] + pinned[kMaxBasis + i];
+        const double hn = std::sqrt(pinned[2 * kMaxBasis]);
         h(j + 1, j) = hn;
-        if (hn > 0) axpby(Vb[j + 1], Vb[j + 1], Vb[j + 1], 1.0 / hn, 0.0);
         for (int i = 0; i < j; i++) {  // previous rotations on column j
           const double a = h(i, j), c = h(i + 1, j);
           h(i, j) = cs[i] * a + sn[i] * c;
