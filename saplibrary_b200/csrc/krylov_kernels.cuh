@@ -173,6 +173,45 @@ k_dots(int n, DotArgs a, double* __restrict__ part, unsigned int* __restrict__ c
 }
 
 
+// y += a x, then out[0] = y . y, in one pass: the update of the residual
+// followed by its norm in BiCGStab(L).  Same grid, thread-to-row mapping and
+// reduction order as k_dots, so out[0] equals k_dots(y, y) after k_axpy.
+static __global__ void __launch_bounds__(kDotThreads)
+k_axpy_sqnorm(int n, double a, const double* __restrict__ x, double* __restrict__ y, double* __restrict__ part,
+              unsigned int* __restrict__ counter, double* __restrict__ out) {
+  __shared__ double red[kDotThreads / 32];
+  __shared__ bool last;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = y[i] + a * x[i];
+    y[i] = v;
+    acc += v * v;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if (lane == 0) red[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0;
+    for (int w = 0; w < kDotThreads / 32; w++) v += red[w];
+    part[blockIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    if (threadIdx.x == 0) {
+      volatile double* pp = part;
+      double v = 0;
+      for (int b = 0; b < (int)gridDim.x; b++) v += pp[b];
+      out[0] = v;
+      *counter = 0u;
+    }
+  }
+}
+
 // Classical Gram-Schmidt of the Arnoldi step (flexible GMRES), one launch per
 // pass instead of one dot and one axpy per basis vector:
 //   k_mdot:  h[i] = V_i . w for i < m (blockIdx.y = i); block partials in

@@ -1163,6 +1163,17 @@ class Solver {
     SAPB_LAUNCHED();
   }
   double nrm2(const double* x) { return std::sqrt(dot(x, x)); }
+  // y += a x and ||y|| from one pass (the values of axpy then nrm2)
+  double axpy_nrm2(const double* x, double* y, double a) {
+    {
+      SAPB_PROF("dots", st);
+      k_axpy_sqnorm<<<kDotBlocks, kDotThreads, 0, st>>>(n, a, x, y, dots_part.get(), dots_ctr.get(), dots_out.get());
+      SAPB_LAUNCHED();
+    }
+    SAPB_CUDA(cudaMemcpyAsync(pinned, dots_out.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+    SAPB_CUDA(cudaStreamSynchronize(st));
+    return std::sqrt(pinned[0]);
+  }
 
   // bicgstabl<..., L> (sap/bicgstab2.h:32-360)
   void bicgstabl(const Spmv& A, double* x, const double* b, int L);
@@ -1513,8 +1524,8 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
       double gam = dot(uu[j + 1].get(), r0.get());
       if (gam == 0) { mon.stop(-11, "gamma is zero"); break; }
       alpha = rho0 / gam;
-      for (int i = 0; i <= j; i++) axpy(uu[i + 1].get(), rr[i].get(), -alpha);
-      r_norm_act = r_norm = nrm2(rr[0].get());
+      r_norm_act = r_norm = axpy_nrm2(uu[1].get(), rr[0].get(), -alpha);  // rr_0 -= alpha uu_1, ||rr_0||
+      for (int i = 1; i <= j; i++) axpy(uu[i + 1].get(), rr[i].get(), -alpha);
       Pm(rr[j].get(), Pv.get());
       Am(Pv.get(), rr[j + 1].get());
       stag_check(alpha, uu[0].get());
@@ -1553,9 +1564,8 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
     }
     stag_check(gamma[1], rr[0].get());
     axpy(rr[0].get(), xx.get(), gamma[1]);
-    axpy(rr[L].get(), rr[0].get(), -gp[L]);
+    r_norm_act = r_norm = axpy_nrm2(rr[L].get(), rr[0].get(), -gp[L]);
     axpy(uu[L].get(), uu[0].get(), -gamma[L]);
-    r_norm_act = r_norm = nrm2(rr[0].get());
     mon.it += 0.25f;
     if (mon.needCheck(r_norm)) {
       recheck();
@@ -1568,8 +1578,7 @@ void Solver::bicgstabl(const Spmv& A, double* x, const double* b, int L) {
       axpy(uu[j].get(), uu[0].get(), -gamma[j]);
       stag_check(gpp[j], rr[j].get());
       axpy(rr[j].get(), xx.get(), gpp[j]);
-      axpy(rr[j].get(), rr[0].get(), -gp[j]);
-      r_norm_act = r_norm = nrm2(rr[0].get());
+      r_norm_act = r_norm = axpy_nrm2(rr[j].get(), rr[0].get(), -gp[j]);
       if (mon.needCheck(r_norm)) {
         recheck();
         if (mon.finished(r_norm_act)) break;
