@@ -47,6 +47,33 @@ __global__ void k_band_from_rowmajor(const double* __restrict__ A, T* __restrict
   }
 }
 
+// Diagonal scaling of the TF32 forms: s_r = 2^k with k = -floor(e / 2) for
+// |a_rr| = f 2^e (f in [0.5, 1)), so that s_r^2 |a_rr| lies in [0.5, 2)
+// (s_r = 1 for a zero or non-finite diagonal).  Powers of two scale without
+// rounding, so the factors of S A S are those of A scaled exactly; what
+// changes is that the pivot-boost and zero-pivot thresholds see pivots near 1.
+template <typename T>
+__global__ void k_diag_pow2(const T* __restrict__ B, int n, int K, T* __restrict__ s) {
+  const long long SW = 2LL * K + 1;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const double d = fabs((double)B[(long long)r * SW + K]);
+    int e = 0;
+    if (d > 0 && isfinite(d)) frexp(d, &e);
+    s[r] = (T)ldexp(1.0, -(e >> 1));
+  }
+}
+// B(i, j) *= s_i s_j over the column-major band
+template <typename T>
+__global__ void k_band_scale(T* __restrict__ B, int n, int K, const T* __restrict__ s) {
+  const long long SW = 2LL * K + 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < SW * n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long c = e / SW;
+    const long long r = c + (e - c * SW) - K;
+    if (r >= 0 && r < n) B[e] *= s[r] * s[c];
+  }
+}
+
 // COO/CSR scatter into the column-major band (copyFromCOOMatrixToBandedMatrix,
 // sap/device/data_transfer.cuh:423-448): one thread per row.
 template <typename T>
@@ -617,7 +644,7 @@ __global__ void k_pass1(const PartDev* __restrict__ parts, const ChunkDev* __res
     if (vin) {
       // leftTrans (precond.h:1535-1544): band row `row` takes input row gin[row], scaled
       if (gin) v = (T)vin[gin[row]] * sin[row];
-      else v = (T)vin[row];
+      else v = sin ? (T)vin[row] * sin[row] : (T)vin[row];
       F[row] = v;
     }
     else v = F[row];
@@ -686,7 +713,7 @@ __global__ void k_pass3(const PartDev* __restrict__ parts, const ChunkDev* __res
     if (zout) {
       // rightTrans (precond.h:1550-1559): band column `row` is input column sout[row], scaled
       if (sout) zout[sout[row]] = (double)(xs[K + i] * cout[row]);
-      else zout[row] = (double)xs[K + i];
+      else zout[row] = (double)(cout ? xs[K + i] * cout[row] : xs[K + i]);
     } else {
       gout[row] = xs[K + i];
     }

@@ -189,6 +189,12 @@ class PrecondT : public PrecBase {
   DBuf<T> T1, T2, tails1, tails2, carry1, carry2;
   DBuf<T> F, Gv, Y;
   DBuf<T> sin_d, cout_d;  // DB row / column scales in band order (reordered path)
+  // TF32 forms without reordering: power-of-two diagonal scales (band order),
+  // the factors being those of S A S; the apply scales its input and output by S
+  DBuf<T> dscale;
+  bool dscaled = false;
+  const T* in_scale() const { return reordered ? sin_d.get() : (dscaled ? dscale.get() : nullptr); }
+  const T* out_scale() const { return reordered ? cout_d.get() : (dscaled ? dscale.get() : nullptr); }
   DBuf<int> flag;
   int maxChunk = 0, sweepThreads = 32, scanG = 1;
   // Numeric inputs of a CSR setup, on the device: the entries of the
@@ -713,9 +719,19 @@ class PrecondT : public PrecBase {
     ptype = o.precondType;
     spike = (ptype == SAP_PRECOND_SPIKE && P > 1);
     lu_ul = spike && o.factMethod == SAP_LU_UL;
+    dscaled = false;
     if (ptype == SAP_PRECOND_NONE) return;
     init_parts_const();
     if (K == 0) return;
+    if (tf32 && !reordered) {
+      dscaled = true;
+      dscale.alloc(n);
+      k_diag_pow2<T><<<grid_for(n, 256), 256, 0, st>>>(B.get(), n, K, dscale.get());
+      SAPB_LAUNCHED();
+      k_band_scale<T><<<grid_for((long long)(2 * K + 1) * n, 256, 148 * 32), 256, 0, st>>>(B.get(), n, K,
+                                                                                        dscale.get());
+      SAPB_LAUNCHED();
+    }
     auto t0 = Clock::now();
     if (spike) {
       offd.alloc((size_t)2 * (P - 1) * K * K);
@@ -942,7 +958,7 @@ class PrecondT : public PrecBase {
     {
       SAPB_PROF("pass1", st);
       k_pass1<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), koff_d.get(), B.get(), vin, F.get(), tails1.get(),
-                                          reordered ? gin_d.get() : nullptr, reordered ? sin_d.get() : nullptr);
+                                          reordered ? gin_d.get() : nullptr, in_scale());
       SAPB_LAUNCHED();
     }
     {
@@ -967,7 +983,7 @@ class PrecondT : public PrecBase {
       SAPB_PROF("pass3", st);
       k_pass3<T, 16><<<nch, NT, s1, st>>>(parts_d.get(), chunks_d.get(), first2_d.get(), koff_d.get(), B.get(), Y.get(),
                                           carry2.get(), zout, gout, reordered ? sout_d.get() : nullptr,
-                                          reordered ? cout_d.get() : nullptr);
+                                          out_scale());
       SAPB_LAUNCHED();
     }
   }
@@ -990,8 +1006,8 @@ class PrecondT : public PrecBase {
       return;
     }
     if (wide_active) {
-      wide->apply(v, z, reordered ? gin_d.get() : nullptr, reordered ? sin_d.get() : nullptr,
-                  reordered ? sout_d.get() : nullptr, reordered ? cout_d.get() : nullptr);
+      wide->apply(v, z, reordered ? gin_d.get() : nullptr, in_scale(), reordered ? sout_d.get() : nullptr,
+                  out_scale());
       return;
     }
     if (spike) {

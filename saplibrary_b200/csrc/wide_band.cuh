@@ -732,7 +732,7 @@ template <typename T>
 __global__ void k_wb_in(const double* __restrict__ v, const int* __restrict__ gin, const T* __restrict__ sin,
                         T* __restrict__ F, int n) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
-    F[r] = gin ? (T)v[gin[r]] * sin[r] : (T)v[r];
+    F[r] = gin ? (T)v[gin[r]] * sin[r] : (sin ? (T)v[r] * sin[r] : (T)v[r]);
 }
 // rightTrans out of the padded block vectors: z[sout[row]] = x(row) * cout[row]
 template <typename T>
@@ -743,7 +743,7 @@ __global__ void k_wb_out(const T* __restrict__ xb, const int* __restrict__ rowpa
     const int p = rowpart[r];
     const T x = xb[p * plen + (r - pstart[p])];
     if (sout) z[sout[r]] = (double)(x * cout[r]);
-    else z[r] = (double)x;
+    else z[r] = (double)(cout ? x * cout[r] : x);
   }
 }
 
