@@ -1,31 +1,66 @@
-"""Learned solver settings: a small MLP (16 features -> 64 -> 64 -> one logit
-per setting) that picks the partition count and the coupled (SPIKE) or
-decoupled (block-Jacobi) preconditioner for a banded matrix, trained on the
-GPU by this library's kernels (`sap_mlp_*`) from the outcomes the solver
-itself produces when swept over those settings.  The default heuristic (the
-setting used without the network) is `DEFAULT_SETTING`.
+"""Learned solver settings: small MLPs (16 features -> 64 -> 64 -> one logit
+per setting) that pick the solver settings for a matrix, trained on the GPU by
+this library's kernels (`sap_mlp_*`) from the outcomes the solver itself
+produces when swept over those settings.  The setting used without the
+network (the default heuristic) is each family's `default`, and the chooser
+falls back to it where the network is unsure.  Two families:
 
-    feats = band_features(band, n, K)           # host, numpy
-    table = sweep(bands, ...)                   # measured time-to-solution per setting
-    net = SettingsNet(); net.train(X, labels)   # GPU kernels
-    pick = net.choose(X)                        # index into SETTINGS
+* `BANDED`: banded matrices (no reordering).  Settings: partition count
+  P in {1, 4, 16, 64}; coupled (SPIKE) with LU_UL or LU_only, or decoupled
+  (block-Jacobi).  Features: `band_features` (size, bandwidth, diagonal
+  dominance, decay of the off-diagonal magnitudes, sign mix).
+* `SPARSE`: sparse matrices set up with the DB / RCM / drop-off reordering
+  (the stencil + fill family of the 1M-row workload, at smaller sizes).
+  Settings: P in {4, 16, 64}; coupled or decoupled; drop-off fraction in
+  {0, 1e-4, 1e-2}.  Features: `csr_features` (size, nonzero profile,
+  dominance of each row's largest entry, and the bandwidths after DB and
+  after RCM from the host reordering, `reorder_host`).
+
+    X, T = sweep(BANDED, count, seed)              # features, measured times
+    net = SettingsNet(BANDED); net.train(X, labels_from_times(T))
+    pick = net.choose(X)                           # index into BANDED.settings
+    gain(BANDED, T, pick)                          # against the default
+
+Labels are the settings with the lowest measured time-to-solution (setup +
+flexible GMRES with an FP32 preconditioner to relres 1e-10, best of a few
+repetitions); a setting that fails or does not converge costs infinity.
 """
 from __future__ import annotations
 
 import ctypes
 import math
 import time
+from dataclasses import dataclass
 
 import numpy as np
 
-from . import (BandedMatrix, Block, FGMRES, LU_UL, LibraryError, MVBanded, Options, Solver, Spike, _check, _lib)
+from . import (Block, BandedMatrix, CsrMatrix, FGMRES, LU_UL, LU_only, LibraryError, MVBanded, Options, Solver,
+               Spike, SpmvCusp, _check, _lib, reorder_host)
 
-# settings the network chooses from: (partitions, preconditioner type)
-SETTINGS = [(1, Spike), (4, Spike), (16, Spike), (64, Spike), (4, Block), (16, Block), (64, Block)]
-DEFAULT_SETTING = 2  # 16 partitions, coupled SPIKE
 NUM_FEATURES = 16
 # below this largest class probability the chooser keeps the default setting
 CONFIDENCE = 0.5
+
+
+@dataclass(frozen=True)
+class Family:
+    """A matrix family: its settings (partitions, preconditioner type,
+    factorisation method, drop-off fraction) and the default one."""
+    name: str
+    settings: tuple
+    default: int
+
+
+BANDED = Family("banded", (
+    (1, Spike, LU_UL, 0.0), (4, Spike, LU_UL, 0.0), (16, Spike, LU_UL, 0.0), (64, Spike, LU_UL, 0.0),
+    (4, Spike, LU_only, 0.0), (16, Spike, LU_only, 0.0), (64, Spike, LU_only, 0.0),
+    (4, Block, LU_UL, 0.0), (16, Block, LU_UL, 0.0), (64, Block, LU_UL, 0.0)), default=2)
+_SPARSE_SETTINGS = tuple((P, pt, LU_UL, dr) for P in (4, 16, 64) for pt in (Spike, Block) for dr in (0.0, 1e-4, 1e-2))
+SPARSE = Family("sparse", _SPARSE_SETTINGS, default=_SPARSE_SETTINGS.index((16, Spike, LU_UL, 1e-4)))
+
+# the banded family under its earlier names
+SETTINGS = BANDED.settings
+DEFAULT_SETTING = BANDED.default
 
 
 def band_features(band: np.ndarray, n: int, K: int) -> np.ndarray:
@@ -54,27 +89,46 @@ def band_features(band: np.ndarray, n: int, K: int) -> np.ndarray:
     return np.asarray(f, dtype=np.float32)
 
 
-def measure(band: np.ndarray, n: int, K: int, setting: int, b: np.ndarray, reps: int = 3,
-            rel_tol: float = 1e-10) -> float:
-    """Time-to-solution (s) of setup + FGMRES solve with an FP32
-    preconditioner under one setting (best of `reps`, so that a host stall
-    in one repetition does not enter the label); inf when the solve does
-    not converge."""
+def csr_features(rp: np.ndarray, ci: np.ndarray, v: np.ndarray) -> np.ndarray:
+    """16 features of a sparse matrix (CSR): size, nonzero profile, how much
+    each row's largest entry dominates it (rows may be permuted, so the
+    diagonal is not known before the DB matching), value spread and signs,
+    and the bandwidths after DB and after RCM of the host reordering."""
+    n = rp.size - 1
+    nnz = int(rp[-1])
+    cnt = np.diff(rp).astype(np.float64)
+    a = np.abs(np.asarray(v, np.float64))
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    rmax = np.zeros(n)
+    np.maximum.at(rmax, rows, a)
+    rsum = np.bincount(rows, weights=a, minlength=n)
+    dom = rmax / np.maximum(rsum - rmax, 1e-300)
+    info = reorder_host(rp, ci, v, 16, Options(dropOffFraction=0.0))
+    kdb, kre = max(int(info["k_db"]), 1), max(int(info["k_reorder"]), 1)
+    med = float(np.median(a / np.maximum(rmax[rows], 1e-300)))
+    f = [
+        math.log10(n), nnz / n, float(cnt.max()), math.log10(kdb), math.log10(kre), 1000.0 * kre / n,
+        float(dom.min()), float(dom.mean()), float(dom.std()), float((dom > 1.0).mean()), med,
+        math.log10(max(nnz, 1)), kre / kdb, float((np.asarray(v) < 0).mean()), math.log10(n / kre),
+        float(cnt.std()),
+    ]
+    return np.asarray(f, dtype=np.float32)
+
+
+def _time_solves(make_solver, setup_arg, spmv, b, reps: int) -> float:
     import torch
-    P, ptype = SETTINGS[setting]
-    opts = Options(solverType=FGMRES, performReorder=False, variableBandwidth=False, applyScaling=False,
-                   factMethod=LU_UL, precondType=ptype, relTol=rel_tol, maxNumIterations=300)
-    A = BandedMatrix.from_array(band, n, K)
-    spmv = MVBanded(A)
     bd = torch.tensor(b, device="cuda")
     best = math.inf
-    s = Solver(P, opts, prec="float")
+    try:
+        s = make_solver()
+    except LibraryError:
+        return best
     for _ in range(reps):
         x = torch.zeros_like(bd)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         try:
-            s.setup(A)
+            s.setup(setup_arg)
             ok = s.solve(spmv, bd, x)
         except LibraryError:
             ok = False
@@ -83,6 +137,28 @@ def measure(band: np.ndarray, n: int, K: int, setting: int, b: np.ndarray, reps:
         if ok:
             best = min(best, t)
     return best
+
+
+def measure(band: np.ndarray, n: int, K: int, setting: int, b: np.ndarray, reps: int = 3,
+            rel_tol: float = 1e-10) -> float:
+    """Time-to-solution (s) of setup + FGMRES solve of a banded matrix with
+    an FP32 preconditioner under BANDED.settings[setting] (best of `reps`,
+    so that a host stall in one repetition does not enter the label); inf
+    when the solve fails or does not converge."""
+    P, ptype, fact, _ = BANDED.settings[setting]
+    opts = Options(solverType=FGMRES, performReorder=False, variableBandwidth=False, applyScaling=False,
+                   factMethod=fact, precondType=ptype, relTol=rel_tol, maxNumIterations=300)
+    A = BandedMatrix.from_array(band, n, K)
+    return _time_solves(lambda: Solver(P, opts, prec="float"), A, MVBanded(A), b, reps)
+
+
+def measure_sparse(A: CsrMatrix, setting: int, b: np.ndarray, reps: int = 2, rel_tol: float = 1e-10) -> float:
+    """As `measure`, for a CSR matrix set up with the reordering under
+    SPARSE.settings[setting]."""
+    P, ptype, fact, drop = SPARSE.settings[setting]
+    opts = Options(solverType=FGMRES, dropOffFraction=drop, factMethod=fact, precondType=ptype, relTol=rel_tol,
+                   maxNumIterations=300)
+    return _time_solves(lambda: Solver(P, opts, prec="float"), A, SpmvCusp(A), b, reps)
 
 
 def random_band(rng: np.random.Generator, n_range=(20000, 200000), k_range=(10, 120), d_range=(0.5, 1.5)):
@@ -97,25 +173,52 @@ def random_band(rng: np.random.Generator, n_range=(20000, 200000), k_range=(10, 
     return band, n, K
 
 
-def sweep(count: int, seed: int, **family) -> tuple[np.ndarray, np.ndarray]:
-    """Features [count, 16] and measured time-to-solution [count, settings]."""
-    from . import generate_band_host  # noqa: F401
+def random_sparse(rng: np.random.Generator, m_range=(60, 160)):
+    """A matrix of the stencil + fill family (convection-diffusion on an
+    m x m grid, random fill, rows permuted): m uniform, convection, fill
+    count, reach and magnitude drawn per matrix."""
+    from .problems import convection_diffusion_csr
+    m = int(rng.integers(m_range[0], m_range[1] + 1))
+    rp, ci, v, _ = convection_diffusion_csr(m=m, conv=float(rng.uniform(0.1, 0.8)),
+                                            fill_per_row=int(rng.integers(1, 4)),
+                                            fill_reach=int(m * rng.uniform(1.0, 8.0)),
+                                            fill_mag=float(rng.uniform(0.02, 0.3)), seed=int(rng.integers(1 << 31)))
+    return rp, ci, v
+
+
+def sweep(family, count: int | None = None, seed: int = 0, **kw) -> tuple[np.ndarray, np.ndarray]:
+    """Features [count, 16] and measured time-to-solution [count, settings]
+    of `count` seeded matrices of the family (BANDED or SPARSE; an integer
+    first argument is read as the banded family's count, the earlier form)."""
+    if not isinstance(family, Family):
+        family, count = BANDED, family
     rng = np.random.default_rng(seed)
     X, T = [], []
     for _ in range(count):
-        band, n, K = random_band(rng, **family)
-        b = np.random.default_rng(n + K).standard_normal(n)
-        X.append(band_features(band, n, K))
-        T.append([measure(band, n, K, s, b) for s in range(len(SETTINGS))])
+        if family is BANDED:
+            band, n, K = random_band(rng, **kw)
+            b = np.random.default_rng(n + K).standard_normal(n)
+            X.append(band_features(band, n, K))
+            T.append([measure(band, n, K, s, b) for s in range(len(family.settings))])
+        else:
+            rp, ci, v = random_sparse(rng, **kw)
+            n = rp.size - 1
+            b = np.random.default_rng(n).standard_normal(n)
+            X.append(csr_features(rp, ci, v))
+            A = CsrMatrix(rp, ci, v)
+            T.append([measure_sparse(A, s, b) for s in range(len(family.settings))])
     return np.asarray(X, np.float32), np.asarray(T, np.float64)
 
 
 class SettingsNet:
     """The MLP on the GPU (sap_mlp_*), with feature standardisation."""
 
-    def __init__(self, hidden=(64, 64), seed: int = 7):
+    def __init__(self, family: Family = BANDED, hidden=(64, 64), seed: int = 7):
+        if not isinstance(family, Family):  # the earlier form SettingsNet(seed=...) passed by keyword only
+            raise TypeError("family must be BANDED or SPARSE")
+        self.family = family
         h = ctypes.c_void_p()
-        _check(_lib.sap_mlp_create(NUM_FEATURES, hidden[0], hidden[1], len(SETTINGS), seed, ctypes.byref(h)))
+        _check(_lib.sap_mlp_create(NUM_FEATURES, hidden[0], hidden[1], len(family.settings), seed, ctypes.byref(h)))
         self._h = h
         self.mu = np.zeros(NUM_FEATURES, np.float32)
         self.sd = np.ones(NUM_FEATURES, np.float32)
@@ -140,7 +243,7 @@ class SettingsNet:
 
     def logits(self, X, normalise: bool = True) -> np.ndarray:
         Xn = self._norm(X) if normalise else np.ascontiguousarray(X, np.float32)
-        out = np.empty((Xn.shape[0], len(SETTINGS)), np.float32)
+        out = np.empty((Xn.shape[0], len(self.family.settings)), np.float32)
         _check(_lib.sap_mlp_forward(self._h, Xn.ctypes.data, Xn.shape[0], out.ctypes.data))
         return out
 
@@ -176,7 +279,7 @@ class SettingsNet:
         back to the method without the network."""
         p = self.probabilities(X)
         picks = p.argmax(axis=1)
-        picks[p.max(axis=1) < min_confidence] = DEFAULT_SETTING
+        picks[p.max(axis=1) < min_confidence] = self.family.default
         return picks
 
 
@@ -185,12 +288,14 @@ def labels_from_times(T: np.ndarray) -> np.ndarray:
     return np.argmin(T, axis=1).astype(np.int32)
 
 
-def gain(T: np.ndarray, picks: np.ndarray) -> dict:
-    """Total time-to-solution of the picked settings against the default
-    setting and the per-matrix best, over the matrices of T."""
+def gain(*args) -> dict:
+    """gain(family, T, picks) (or gain(T, picks) for the banded family):
+    total time-to-solution of the picked settings against the family's
+    default setting and the per-matrix best, over the matrices of T."""
+    family, T, picks = (args if len(args) == 3 else (BANDED,) + args)
     rows = np.arange(T.shape[0])
     chosen = T[rows, picks]
-    default = T[:, DEFAULT_SETTING]
+    default = T[:, family.default]
     best = T.min(axis=1)
     finite = np.isfinite(chosen) & np.isfinite(default)
     return {"total_chosen_s": float(chosen[finite].sum()), "total_default_s": float(default[finite].sum()),
@@ -200,15 +305,15 @@ def gain(T: np.ndarray, picks: np.ndarray) -> dict:
             "picked_best": float((picks == np.argmin(T, axis=1)).mean())}
 
 
-def evaluate(train: int, held: int, seed: int, **family) -> dict:
-    """Sweep train + held matrices, train on the first `train`, report the
-    held-out gain over the default setting."""
-    X, T = sweep(train + held, seed, **family)
-    net = SettingsNet(seed=seed)
+def evaluate(family: Family, train: int, held: int, seed: int, **kw) -> dict:
+    """Sweep train + held matrices of the family, train on the first
+    `train`, report the held-out gain over the default setting."""
+    X, T = sweep(family, train + held, seed, **kw)
+    net = SettingsNet(family, seed=seed)
     loss = net.train(X[:train], labels_from_times(T[:train]), epochs=600)
-    g = gain(T[train:], net.choose(X[train:]))
-    g.update({"train": train, "held_out": held, "final_train_loss": loss, "settings": len(SETTINGS),
-              "default_setting": SETTINGS[DEFAULT_SETTING][0]})
+    g = gain(family, T[train:], net.choose(X[train:]))
+    g.update({"family": family.name, "train": train, "held_out": held, "final_train_loss": loss,
+              "settings": len(family.settings), "default_setting": list(family.settings[family.default])})
     return g
 
 
@@ -216,9 +321,13 @@ if __name__ == "__main__":
     import argparse
     import json
     ap = argparse.ArgumentParser(description="measured settings sweep, training and held-out gain")
+    ap.add_argument("--family", default="banded", choices=["banded", "sparse"])
     ap.add_argument("--train", type=int, default=160)
     ap.add_argument("--held", type=int, default=40)
     ap.add_argument("--seed", type=int, default=2024)
     a = ap.parse_args()
-    print(json.dumps(evaluate(a.train, a.held, a.seed, n_range=(20000, 200000), k_range=(10, 150),
-                              d_range=(0.5, 1.5))))
+    if a.family == "banded":
+        print(json.dumps(evaluate(BANDED, a.train, a.held, a.seed, n_range=(20000, 200000), k_range=(10, 150),
+                                  d_range=(0.5, 1.5))))
+    else:
+        print(json.dumps(evaluate(SPARSE, a.train, a.held, a.seed, m_range=(60, 200))))

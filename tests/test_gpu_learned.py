@@ -1,7 +1,9 @@
 """Learned solver settings: the GPU MLP kernels against the FP64 numpy
 oracle (forward logits, loss and every gradient), training that lowers the
-loss, and the chooser's time-to-solution against the default setting on
-held-out matrices of a measured settings sweep."""
+loss, and, for both matrix families (banded: partitions, coupled or
+decoupled, LU_UL or LU_only; sparse with reordering: partitions, coupled or
+decoupled, drop-off fraction), the chooser's time-to-solution against the
+default setting on held-out matrices of a measured settings sweep."""
 import numpy as np
 import pytest
 
@@ -62,4 +64,18 @@ def test_chooser_against_default_on_held_out_sweep():
     assert g["failed_chosen"] <= g["failed_default"]
     # the trained chooser is at least as fast as the default heuristic in
     # total over the held-out matrices
+    assert g["total_chosen_s"] <= g["total_default_s"]
+
+
+def test_sparse_chooser_against_default_on_held_out_sweep():
+    fam = learned.SPARSE
+    X, T = learned.sweep(fam, 40, seed=13, m_range=(60, 140))
+    train, held = slice(0, 30), slice(30, 40)
+    net = learned.SettingsNet(fam, seed=9)
+    net.train(X[train], learned.labels_from_times(T[train]), epochs=500)
+    picks = net.choose(X[held])
+    g = learned.gain(fam, T[held], picks)
+    print("sparse held-out", g)
+    print("picks", [fam.settings[p] for p in picks])
+    assert g["failed_chosen"] <= g["failed_default"]
     assert g["total_chosen_s"] <= g["total_default_s"]
