@@ -153,6 +153,36 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// a / b from y = 1 / b (itself correctly rounded) with one multiply and two
+// FMAs: Markstein's quotient correction (P. Markstein, IBM J. Res. Dev.
+// 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic,
+// Markstein's theorem): q0 = RN(a y) is within one ulp of a / b, the
+// remainder r = a - b q0 is exact through the FMA, and RN(q0 + r y) =
+// RN(a / b) as long as nothing underflows or overflows; for a = 0, q0 = +-0
+// is the quotient.  `ok` is false outside exponent ranges that guarantee
+// this (non-finite, subnormal, very large or very small operands), where the
+// caller must use the division; with ok true the result equals a / b.
+template <typename T>
+struct DivRange;
+template <>
+struct DivRange<double> {
+  static constexpr double lo_a = 0x1p-960, lo = 0x1p-1000, hi = 0x1p1000;
+};
+template <>
+struct DivRange<float> {
+  static constexpr float lo_a = 0x1p-96f, lo = 0x1p-120f, hi = 0x1p120f;
+};
+template <typename T>
+__device__ __forceinline__ T div_rcp_fast(T a, T b, T y, bool& ok) {
+  using L = DivRange<T>;
+  const T q0 = a * y;
+  const T r = fma(-q0, b, a);
+  const T q = fma(r, y, q0);
+  const T aa = fabs(a), aq = fabs(q0), ay = fabs(y);
+  ok = ay >= L::lo && ay <= L::hi && (a == T(0) || (aa >= L::lo_a && aq >= L::lo && aq <= L::hi));
+  return a == T(0) ? q0 : q;
+}
+
 // boostValue (sap/device/factor_band_const.cuh:29-40): pivots with
 // |p| <= BURST_VALUE are replaced by +-BURST_NEW_VALUE.
 template <typename T>

@@ -226,7 +226,6 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
   const int K = jb.K, SW = 2 * K + 1, np = jb.e - jb.s, W = K + NB * (1 + DPF);
   extern __shared__ __align__(16) unsigned char sm_raw[];
   T* win = reinterpret_cast<T*>(sm_raw);
-  T* piv = win + (size_t)W * SW;  // piv[r % W]: the pivot of row r
   T* band = (jb.target ? B2 : B) + jb.boff;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const int ct = tid - 32, nct = blockDim.x - 32;  // copy threads: warps 1..
@@ -238,14 +237,9 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
   };
   auto wrap = [&](int s) { return s >= W ? s - W : s; };  // for 0 <= s < 2 W
   // column `col` from ring slot `sl` to the band, its U entries post-divided
-  auto out = [&](int col, int sl, int p) {
-    T v = win[sl * SW + p];
-    if (p < K && col - K + p >= 0) {
-      int pr = sl + p - K;
-      v /= piv[pr < 0 ? pr + W : pr];
-    }
-    band[gidx(col, p)] = v;
-  };
+  // column `col` from ring slot `sl` to the band (its U entries are divided
+  // by their rows' pivots afterwards, k_factor_postdiv)
+  auto out = [&](int col, int sl, int p) { band[gidx(col, p)] = win[sl * SW + p]; };
   if (ct >= 0) {  // columns [0, K + NB), then one panel's new columns per group; all in slots == column
     for (int g = 0; g < DPF; g++) {
       const int c0 = g == 0 ? 0 : K + g * NB, c1 = min(np, K + (g + 1) * NB);
@@ -256,6 +250,7 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
       cp_async_commit();
     }
   }
+  bool zero_seen = false;
   int j0 = 0, s0 = 0;  // s0 = j0 % W
   for (; j0 < np; j0 += NB, s0 = wrap(s0 + NB)) {
     const int nb = min(NB, np - j0);
@@ -275,39 +270,77 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
       cp_async_commit();
     } else {
       T a[R][NB];
+      auto load_panel = [&]() {
 #pragma unroll
-      for (int c = 0; c < NB; c++) {
-        const T* colp = win + wrap(s0 + c) * SW;
+        for (int c = 0; c < NB; c++) {
+          const T* colp = win + wrap(s0 + c) * SW;
 #pragma unroll
-        for (int t = 0; t < R; t++) {
-          const int pos = K + lane + 32 * t - c;  // row j0 + lane + 32 t
-          a[t][c] = (c < nb && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) ? colp[pos] : T(0);
+          for (int t = 0; t < R; t++) {
+            const int pos = K + lane + 32 * t - c;  // row j0 + lane + 32 t
+            a[t][c] = (c < nb && j0 + lane + 32 * t < np && pos >= 0 && pos <= 2 * K) ? colp[pos] : T(0);
+          }
         }
-      }
+      };
+      load_panel();
+      // fast path: each quotient from the pivot's reciprocal with Markstein's
+      // correction (div_rcp_fast, equal to the division inside its range),
+      // without branches; `bad` records a lane whose operands left the range
+      bool bad = false;
 #pragma unroll
       for (int k = 0; k < NB; k++) {
         if (k < nb) {
           const int w = min(K, np - 1 - (j0 + k));
           T p = __shfl_sync(0xffffffffu, a[0][k], k);
           if (do_boost) p = boost_pivot(p);
-          else if (lane == 0 && fabs((double)p) < 1e-7) atomicOr(zero_flag, 1);
+          else zero_seen |= fabs((double)p) < 1e-7;
+          const T y = T(1) / p;
           T u[NB];
 #pragma unroll
           for (int c = k + 1; c < NB; c++) u[c] = __shfl_sync(0xffffffffu, a[0][c], k);
 #pragma unroll
           for (int t = 0; t < R; t++) {
             const int rr = lane + 32 * t - k;  // row - pivot row
-            if (rr == 0) {
-              a[t][k] = p;
-            } else if (rr >= 1 && rr <= w) {
-              const T l = a[t][k] / p;
-              a[t][k] = l;
+            const bool in = rr >= 1 && rr <= w;
+            bool ok;
+            const T l = div_rcp_fast(a[t][k], p, y, ok);
+            bad |= in && !ok;
+            a[t][k] = rr == 0 ? p : (in ? l : a[t][k]);
 #pragma unroll
-              for (int c = k + 1; c < NB; c++)
-                if (c - k <= w) a[t][c] -= l * u[c];
+            for (int c = k + 1; c < NB; c++) {
+              if (c - k <= w) {
+                const T nv = a[t][c] - l * u[c];
+                a[t][c] = in ? nv : a[t][c];
+              }
             }
           }
-          if (lane == 0) piv[wrap(s0 + k)] = p;
+        }
+      }
+      if (__any_sync(0xffffffffu, bad)) {
+        // some quotient left the range: the panel again with the division
+        load_panel();
+#pragma unroll
+        for (int k = 0; k < NB; k++) {
+          if (k < nb) {
+            const int w = min(K, np - 1 - (j0 + k));
+            T p = __shfl_sync(0xffffffffu, a[0][k], k);
+            if (do_boost) p = boost_pivot(p);
+            T u[NB];
+#pragma unroll
+            for (int c = k + 1; c < NB; c++) u[c] = __shfl_sync(0xffffffffu, a[0][c], k);
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+              const int rr = lane + 32 * t - k;
+              if (rr == 0) {
+                a[t][k] = p;
+              } else if (rr >= 1 && rr <= w) {
+                const T l = a[t][k] / p;
+                a[t][k] = l;
+#pragma unroll
+                for (int c = k + 1; c < NB; c++)
+                  if (c - k <= w) a[t][c] -= l * u[c];
+              }
+            }
+          }
         }
       }
 #pragma unroll
@@ -374,6 +407,7 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
       }
     }
   }
+  if (zero_seen && tid == 0) atomicOr(zero_flag, 1);
   cp_async_wait<0>();
   __syncthreads();
   // the last panel: columns [j0 - NB, np) in slots from s0 - NB on
@@ -381,6 +415,29 @@ k_factor_panel(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restr
   for (int e = tid; e < (np - jl) * SW; e += blockDim.x) {
     const int c = e / SW;
     out(jl + c, wrap(sl0 + c), e - c * SW);
+  }
+}
+
+// Post-divide of the panel kernel's factors (bandLUUL_post_divide,
+// sap/device/factor_band_const.cuh:1717-1779): every U entry of a job
+// (band position p < K of column i with row i - K + p >= 0, in the job's
+// own order, mirrored for UL jobs) divided by the pivot of its row, the
+// same operands as the one-pivot kernel's write-back.  Pivots (position K)
+// are only read.
+template <typename T>
+__global__ void k_factor_postdiv(const FactorJob* __restrict__ jobs, T* __restrict__ B, T* __restrict__ B2) {
+  const FactorJob jb = jobs[blockIdx.y];
+  const int K = jb.K, SW = 2 * K + 1, np = jb.e - jb.s;
+  T* band = (jb.target ? B2 : B) + jb.boff;
+  const bool mir = jb.mirror != 0;
+  const long long total = (long long)np * K;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / K), p = (int)(e - (long long)i * K);
+    const int r = i - K + p;
+    if (r < 0) continue;
+    const long long col = mir ? np - 1 - i : i, pos = mir ? 2 * K - p : p, rcol = mir ? np - 1 - r : r;
+    band[col * SW + pos] /= band[rcol * SW + K];
   }
 }
 

@@ -828,7 +828,7 @@ class PrecondT : public PrecBase {
     }
     DBuf<FactorJob> jobs_d;
     jobs_d.upload(jobs, st);
-    flag.alloc(1);
+    flag.alloc(1);  // a zero pivot seen
     flag.zero(st);
     const int Kmax = parts_maxK();
     int G = std::max(1, std::min(Kmax, 512 / std::max(Kmax, 1)));
@@ -840,24 +840,30 @@ class PrecondT : public PrecBase {
     const char* fk = std::getenv("SAPB_FACTOR_KERNEL");
     const bool ring_only = fk && std::string(fk) == "ring";
     const int R = (Kmax + NB + 31) / 32;
-    auto panel_smem = [&](int dpf) {
-      return (size_t)(Kmax + NB * (1 + dpf)) * (2 * Kmax + 2) * sizeof(T);
+    int maxrows = 0;
+    for (const auto& jb : jobs) maxrows = std::max(maxrows, jb.e - jb.s);
+    auto postdiv = [&]() {
+      SAPB_LAUNCHED();
+      k_factor_postdiv<T><<<dim3(grid_for((long long)maxrows * Kmax, 256, 1024), (int)jobs.size()), 256, 0, st>>>(
+          jobs_d.get(), B.get(), B2.get());
     };
+    auto panel_smem = [&](int dpf) { return (size_t)(Kmax + NB * (1 + dpf)) * (2 * Kmax + 1) * sizeof(T); };
     if (!ring_only && R <= 4 && panel_smem(1) <= 227 * 1024) {
       const int dpf = panel_smem(2) <= 227 * 1024 ? 2 : 1;
       const size_t psm = panel_smem(dpf);
       const int nt = 32 * std::min(16, std::max(2, (Kmax + 3) / 4));  // four trailing columns per warp
       auto launch = [&](auto kern) {
         SAPB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-        SAPB_PROF("factor", st);
         kern<<<(int)jobs.size(), nt, psm, st>>>(jobs_d.get(), B.get(), B2.get(), boost ? 1 : 0, flag.get(), dpf);
       };
+      SAPB_PROF("factor", st);  // the factor kernel and its post-divide pass
       switch (R) {
         case 1: launch(k_factor_panel<T, NB, 1>); break;
         case 2: launch(k_factor_panel<T, NB, 2>); break;
         case 3: launch(k_factor_panel<T, NB, 3>); break;
         default: launch(k_factor_panel<T, NB, 4>); break;
       }
+      postdiv();
     } else if (smem <= 200 * 1024) {
       SAPB_CUDA(cudaFuncSetAttribute(k_factor_smem<T, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       SAPB_PROF("factor", st);
@@ -871,7 +877,8 @@ class PrecondT : public PrecBase {
     int hflag = 0;
     SAPB_CUDA(cudaMemcpyAsync(&hflag, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
     SAPB_CUDA(cudaStreamSynchronize(st));
-    if (hflag && !o.safeFactorization && !boost) throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
+    if (hflag && !o.safeFactorization && !boost)
+      throw Error(SAP_ZERO_PIVOTING, "Found a pivot equal to zero (partBandedLU).");
   }
 
   void build_sweeps() {

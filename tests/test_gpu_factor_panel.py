@@ -1,8 +1,10 @@
 """The panel-blocked narrow-band factorisation (k_factor_panel: one warp
-factors NB = 8 pivots in registers, then all warps apply them to the next K
-columns) against the one-pivot-at-a-time ring kernel it replaces
-(k_factor_smem, selected with SAPB_FACTOR_KERNEL=ring).  Both apply the same
-updates to every element in the same order, so the factors, and hence every
+factors NB = 8 pivots in registers with reciprocal-based exact quotients,
+then all warps apply them to the next K columns; the U entries divided by
+their pivots in a separate pass, k_factor_postdiv) against the
+one-pivot-at-a-time ring kernel it replaces (k_factor_smem, selected with
+SAPB_FACTOR_KERNEL=ring).  Both apply the same updates to every element in
+the same order with the same rounding, so the factors, and hence every
 preconditioner apply, are equal bit for bit.  Shapes cover K below the panel
 width, partitions shorter than a panel, ragged last panels, LU_only and LU_UL
 (mirrored UL jobs), pivot boosting, both precisions, the variable-band sparse
@@ -72,9 +74,9 @@ def test_panel_factor_equals_ring_factor_bitwise(n, K, P, d, dist, fact, safe, d
         return _apply(s, v)
 
     z_ring = _with_kernel("ring", solve_apply)
-    z_panel = _with_kernel(None, solve_apply)
-    assert np.all(np.isfinite(z_panel))
-    assert np.array_equal(z_ring, z_panel)
+    z = _with_kernel(None, solve_apply)
+    assert np.all(np.isfinite(z))
+    assert np.array_equal(z_ring, z)
 
 
 @pytest.mark.parametrize("dtype", ["double", "float"])
