@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <memory>
+#include <utility>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -105,6 +107,30 @@ class DBuf {
   T* p_ = nullptr;
   size_t n_ = 0;
 };
+
+// Allocator whose value construction leaves trivially constructible elements
+// uninitialised: a HostVec resized to hold a copy is first touched by the
+// (parallel) copy itself instead of being zero-filled by one thread.
+template <typename T>
+struct DefaultInitAllocator : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = DefaultInitAllocator<U>;
+  };
+  DefaultInitAllocator() = default;
+  template <typename U>
+  DefaultInitAllocator(const DefaultInitAllocator<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <typename T>
+using HostVec = std::vector<T, DefaultInitAllocator<T>>;
 
 // Page-locked host buffer (grow-only) for device->host copies at full speed.
 template <typename T>

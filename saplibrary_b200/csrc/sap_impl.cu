@@ -80,8 +80,8 @@ struct Csr {
   DBuf<double> v;
   DBuf<int> blk;  // row blocks of k_spmv_csr_blocks
   int nblk = 0;
-  std::vector<int> rp_h, ci_h;  // host copies of the pattern (reordering runs on the host)
-  std::vector<double> v_h;
+  HostVec<int> rp_h, ci_h;  // host copies of the pattern (reordering runs on the host)
+  HostVec<double> v_h;
 };
 
 struct Spmv {
@@ -333,7 +333,7 @@ class PrecondT : public PrecBase {
         for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) rows[e] = i;
       for (int e = 0; e < A.nnz; e++) src[e] = e;
       co_row.upload(rows, st);
-      co_col.upload(A.ci_h, st);
+      co_col.upload(A.ci_h.data(), A.ci_h.size(), st);
       co_src.upload(src, st);
       co_scale.upload(std::vector<T>(A.nnz, T(1)), st);
       co_val.alloc(A.nnz);
@@ -1800,11 +1800,12 @@ int sap_csr_create(int n, int nnz, const int* rp, const int* ci, const double* v
       SAPB_CUDA(cudaMemcpy(h->c.rp_h.data(), rp, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
       SAPB_CUDA(cudaMemcpy(h->c.ci_h.data(), ci, (size_t)nnz * sizeof(int), cudaMemcpyDeviceToHost));
       SAPB_CUDA(cudaMemcpy(h->c.v_h.data(), v, (size_t)nnz * sizeof(double), cudaMemcpyDeviceToHost));
-    } else {  // host copies in parallel chunks
-      std::copy(rp, rp + n + 1, h->c.rp_h.begin());
+    } else {  // host copies in parallel chunks (the first touch of the uninitialised vectors)
       _Pragma("omp parallel for schedule(static)")
       for (int c = 0; c < 64; c++) {
         const long long a = (long long)nnz * c / 64, e = (long long)nnz * (c + 1) / 64;
+        const long long ra = (long long)(n + 1) * c / 64, re = (long long)(n + 1) * (c + 1) / 64;
+        std::copy(rp + ra, rp + re, h->c.rp_h.begin() + ra);
         std::copy(ci + a, ci + e, h->c.ci_h.begin() + a);
         std::copy(v + a, v + e, h->c.v_h.begin() + a);
       }
@@ -1817,9 +1818,9 @@ int sap_csr_create(int n, int nnz, const int* rp, const int* ci, const double* v
     _Pragma("omp parallel for schedule(static) reduction(| : bad_ci)")
     for (int p = 0; p < nnz; p++) bad_ci |= h->c.ci_h[p] < 0 || h->c.ci_h[p] >= n;
     SAP_REQUIRE(!bad_ci, "column index out of range");
-    h->c.rp.upload(h->c.rp_h, nullptr);
-    h->c.ci.upload(h->c.ci_h, nullptr);
-    h->c.v.upload(h->c.v_h, nullptr);
+    h->c.rp.upload(h->c.rp_h.data(), h->c.rp_h.size(), nullptr);
+    h->c.ci.upload(h->c.ci_h.data(), h->c.ci_h.size(), nullptr);
+    h->c.v.upload(h->c.v_h.data(), h->c.v_h.size(), nullptr);
     {
       const std::vector<int> blk = csr_row_blocks(n, h->c.rp_h.data());
       h->c.nblk = (int)blk.size() - 1;
