@@ -1058,7 +1058,9 @@ class WideBand {
       const int kt = std::min(1024, ((K + 31) / 32) * 32);
       for (int j0 = 0; j0 < ncol; j0 += cs) {
         const int w = std::min(cs, ncol - j0);
-        SAPB_CUDA(cudaMemsetAsync(X.get(), 0, (size_t)nI * sX * sizeof(T), st));
+        // only block rows ib0.. of each column are written or read below
+        SAPB_CUDA(cudaMemset2DAsync(X.get() + (long long)ib0 * bs, (size_t)plen * sizeof(T), 0,
+                                    (size_t)(plen - (long long)ib0 * bs) * sizeof(T), (size_t)nI * cs, st));
         k_spike_rhs<T><<<dim3(w, nI), kt, 0, st>>>(offd, which, K, cols_d.get(), ncol, j0, pos_d.get(), X.get(), sX,
                                                     plen);
         SAPB_LAUNCHED();
