@@ -25,7 +25,10 @@ x_true = ones), each in plain FP64 + BiCGStab(2), TF32 + FGMRES and FP32 +
 FGMRES.  cpu_baseline is a complete, measured CPU oracle solve of the 2M-row
 banded workload (key "cpu_complete": both banded workloads); the reference
 arm (--impl reference) reports itself unavailable, because one complete CPU
-solve of the 1M-row sparse workload takes tens of minutes.
+solve of the 1M-row sparse workload takes tens of minutes.  Key "ensemble":
+128 independent banded systems (N log-uniform in [2e3, 2e5], K in
+{8, 16, 32, 64, 128}) solved by one batched call and one by one (--ensemble
+sets the count, 0 skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -326,6 +329,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--forms", default=DEFAULT_FORMS, help="comma-separated forms to time (" + ", ".join(FORMS) + ")")
     ap.add_argument("--m", type=int, default=WORKLOAD["m"], help="grid side (profiler captures only)")
+    ap.add_argument("--ensemble", type=int, default=128,
+                    help="systems of the batched-ensemble comparison (0: skip)")
     ap.add_argument("--banded", default=",".join(BANDED),
                     help="banded workloads timed beside the headline (" + ", ".join(BANDED) + "; empty: none)")
     args = ap.parse_args()
@@ -514,6 +519,12 @@ def main():
     banded = [b for b in args.banded.split(",") if b]
     if banded:
         line["banded"] = {name: time_banded(sap, torch, name, warm, max(args.steps, 5), ws) for name in banded}
+    if args.ensemble > 0:
+        # batched ensemble of independent banded systems (N log-uniform in
+        # [2e3, 2e5], K in {8..128}, FP32 preconditioner, FGMRES to 1e-10):
+        # one solve_batch call against the same systems solved one by one
+        from saplibrary_b200 import ensemble
+        line["ensemble"] = ensemble.run(count=args.ensemble, seed=3, P=8, prec="float")
     if rank == 0 and not args.no_cpu_baseline:
         cpu_runs = {}
         for name in banded:
