@@ -414,31 +414,37 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
 // scanned.  A node queued from a batch belongs to the first node of the
 // batch, in FIFO order, that meets it unqueued (smallest claim), and every
 // claimer queues its nodes through the same degree heap in its adjacency
-// order, so the concatenation equals the serial queue.  Small batches are
-// scanned serially.  claim[] is INT_MAX everywhere on entry and on return.
+// order, so the concatenation equals the serial queue.  Every thread owns a
+// contiguous range of the batch: one scan of its nodes' adjacency lowers the
+// claims and records, per node, the neighbours it claimed at that moment;
+// after a barrier each node keeps those it still holds (in adjacency order)
+// and queues them through the heap into the thread's buffer, and the
+// buffers, concatenated in thread order, are the next batch.  Small batches
+// are scanned serially.  claim[] is INT_MAX everywhere on entry and on
+// return.
 static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& off, const std::vector<int>& adj,
                           const std::vector<int>& degree, std::vector<int>& pushed, std::vector<int>& level,
-                          std::vector<int>& order, std::vector<int>& claim, std::vector<int>& meta) {
+                          std::vector<int>& order, std::vector<int>& claim) {
   constexpr int kSerialBatch = 384;
   const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
-  int h0 = 0, t0 = 1, scan = 0, total = 0;
+  int h0 = 0, t0 = 1, scan = 0, serial_total = 0;
   bool ok = true;
   level[root] = 0;
   pushed[root] = trial;
   order[0] = root;
-  meta.resize(3 * ((size_t)n + 1));  // per batch position: thread, start in its buffer, count
   int* cl = claim.data();
-  std::vector<std::vector<int>> bufs(nt);
+  std::vector<int> made(nt + 1, 0);  // nodes queued by each thread in this batch
   using Kids = std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree>;
 #pragma omp parallel num_threads(nt)
   {
     Kids kids;
-    const int tid = omp_get_thread_num();
-    std::vector<int>& buf = bufs[tid];
+    const int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+    std::vector<int> cand, per_node, out;  // claimed neighbours, their count per node, queued nodes
     for (;;) {
-      const int m = t0 - h0;  // shared, stable between barriers
+      const int m = t0 - h0, next = t0;  // shared, stable until the closing single
       if (m == 0) break;
-      if (m < kSerialBatch) {
+      const bool serial = m < kSerialBatch;
+      if (serial) {
 #pragma omp single
         {
           int tail = t0;
@@ -456,64 +462,61 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
               kids.pop();
             }
           }
-          total = tail - t0;
+          serial_total = tail - t0;
         }
       } else {
-        // claims: the smallest batch position meeting the node
-#pragma omp for schedule(dynamic, 64)
-        for (int k = h0; k < t0; k++) {
+        const int k0 = h0 + (int)((long long)m * tid / nth), k1 = h0 + (int)((long long)m * (tid + 1) / nth);
+        cand.clear();
+        per_node.resize(k1 - k0);
+        for (int k = k0; k < k1; k++) {
           const int u = order[k];
+          const size_t c0 = cand.size();
           for (int e = off[u]; e < off[u + 1]; e++) {
             const int t = adj[e];
             if (pushed[t] == trial) continue;
             int cur = __atomic_load_n(cl + t, __ATOMIC_RELAXED);
-            while (k < cur && !__atomic_compare_exchange_n(cl + t, &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+            while (k < cur) {
+              if (__atomic_compare_exchange_n(cl + t, &cur, k, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+                cand.push_back(t);
+                break;
+              }
             }
           }
+          per_node[k - k0] = (int)(cand.size() - c0);
         }
-        // every claimer takes its nodes (each once) through the heap into
-        // its thread's buffer
-        buf.clear();
-#pragma omp for schedule(dynamic, 64)
-        for (int k = h0; k < t0; k++) {
-          const int u = order[k], lv = level[u];
-          for (int e = off[u]; e < off[u + 1]; e++) {
-            const int t = adj[e];
+#pragma omp barrier
+        // a neighbour is kept by the node whose claim survived (one node of
+        // one thread holds it); the others see another claim or INT_MAX
+        out.clear();
+        size_t c = 0;
+        for (int k = k0; k < k1; k++) {
+          const int lv = level[order[k]] + 1;
+          for (const size_t c1 = c + per_node[k - k0]; c < c1; c++) {
+            const int t = cand[c];
             if (__atomic_load_n(cl + t, __ATOMIC_RELAXED) != k) continue;
             __atomic_store_n(cl + t, INT_MAX, __ATOMIC_RELAXED);
             pushed[t] = trial;
-            level[t] = lv + 1;
+            level[t] = lv;
             kids.push(std::make_pair(t, degree[t]));
           }
-          int* md = meta.data() + 3 * (size_t)(k - h0);
-          md[0] = tid;
-          md[1] = (int)buf.size();
           while (!kids.empty()) {
-            buf.push_back(kids.top().first);
+            out.push_back(kids.top().first);
             kids.pop();
           }
-          md[2] = (int)buf.size() - md[1];
         }
-#pragma omp single
-        {
-          int run = 0;
-          for (int k = 0; k < m; k++) {
-            int* md = meta.data() + 3 * (size_t)k;
-            const int c = md[2];
-            md[2] = run;  // now: position in the next batch
-            run += c;
-          }
-          total = run;
-        }
-#pragma omp for schedule(static)
-        for (int k = 0; k < m; k++) {
-          const int* md = meta.data() + 3 * (size_t)k;
-          const int end = k + 1 < m ? md[5] : total;
-          std::copy(bufs[md[0]].begin() + md[1], bufs[md[0]].begin() + md[1] + (end - md[2]), order.begin() + t0 + md[2]);
-        }
+        made[tid + 1] = (int)out.size();
+#pragma omp barrier
+        int start = next;  // (t0 may already be advanced by the closing single)
+        for (int u = 1; u <= tid; u++) start += made[u];
+        std::copy(out.begin(), out.end(), order.begin() + start);
       }
 #pragma omp single
       {
+        int total = serial_total;
+        if (!serial) {
+          total = 0;
+          for (int u = 1; u <= nth; u++) total += made[u];
+        }
         h0 = t0;
         t0 += total;
         if (t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
@@ -567,6 +570,7 @@ int Pipeline<T>::rcm() {
   std::vector<int>& order = pfill(bfs_order, n, 0);
   std::vector<int>& claim = pfill(bfs_claim, n, INT_MAX);
   const int tracked_level = 0;  // never advanced (graph.h:1413-1414)
+  bool kept = false;
   for (int trial = 0; trial < 5; trial++) {
     int root;
     if (trial == 0) {
@@ -585,7 +589,7 @@ int Pipeline<T>::rcm() {
       while (tried[root]) root = (root + 1) % n;
     }
     tried[root] = 1;
-    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, ws_i2)) break;
+    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim)) break;
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
     int bw = 0;
@@ -594,12 +598,16 @@ int Pipeline<T>::rcm() {
     if (best_bw > bw) {
       best_bw = bw;
       rcm_order = order;
+      kept = true;
     }
     if (trial > 0) break;            // tracked level never grows: the second trial is the last
     if (best_bw <= 256) break;       // BANDWIDTH_THRESHOLD
   }
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < n; k++) rcm_pos[rcm_order[k]] = k;
+  // no trial lowered the bandwidth: the order is the identity and the
+  // permuted matrix would equal the current one entry for entry
+  if (!kept) return best_bw;
   tmp_rp.swap(m_rp);
   tmp_ci.swap(m_ci);
   tmp_val.swap(m_val);
