@@ -62,26 +62,35 @@ void csr_from_keys(int n, const std::vector<int>& key, const std::vector<int>& c
 // with its entries in their order and columns relabelled through colmap
 // (none when null).  This is exactly what the stable counting sort by
 // key = newpos[row] (csr_from_keys) produces, built row-parallel.
-template <typename V>
-void permute_rows(int n, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<V>& val,
-                  const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
-                  std::vector<int>& out_ci, std::vector<V>& out_val) {
+// value_of(r, e) gives the value written for entry e of row r.
+template <typename V, typename F>
+void permute_rows_with(int n, const std::vector<int>& rp, const std::vector<int>& ci, F value_of,
+                       const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
+                       std::vector<int>& out_ci, std::vector<V>& out_val) {
   out_rp.resize(n + 1);
   out_rp[0] = 0;
 #pragma omp parallel for schedule(static)
   for (int r = 0; r < n; r++) out_rp[newpos[r] + 1] = rp[r + 1] - rp[r];
   for (int i = 0; i < n; i++) out_rp[i + 1] += out_rp[i];
   out_ci.resize(ci.size());
-  out_val.resize(val.size());
+  out_val.resize(ci.size());
   const int* cm = colmap ? colmap->data() : nullptr;
 #pragma omp parallel for schedule(static, 4096)
   for (int r = 0; r < n; r++) {
     int d = out_rp[newpos[r]];
     for (int e = rp[r]; e < rp[r + 1]; e++, d++) {
       out_ci[d] = cm ? cm[ci[e]] : ci[e];
-      out_val[d] = val[e];
+      out_val[d] = value_of(r, e);
     }
   }
+}
+
+template <typename V>
+void permute_rows(int n, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<V>& val,
+                  const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
+                  std::vector<int>& out_ci, std::vector<V>& out_val) {
+  const V* v = val.data();
+  permute_rows_with(n, rp, ci, [v](int, int e) { return v[e]; }, newpos, colmap, out_rp, out_ci, out_val);
 }
 
 int partition_of(int r, int q, int rem) {
@@ -112,7 +121,7 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   std::vector<double>& u = pfill(db_u, n, 0.0);
   std::vector<double>& v = pfill(db_v, n, kInf);
   std::vector<int>& match = pfill(db_match, n, 0);
-  std::vector<int>& rev_match = pfill(ws_i0, nnz, 0);
+  std::vector<int>& rev_match = pfill(ws_i0, n, 0);  // per column: its matched entry
   std::vector<char>& row_done = pfill(db_rowdone, n, (char)0);
   std::vector<char>& col_done = pfill(db_coldone, n, (char)0);
   // initial duals: u = per-row minimum weight (reduce_by_key over CSR rows)
@@ -124,11 +133,12 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   }
   // greedy initial matching (init_reduced_cval, graph.h:1890-1918): every
   // column's smallest reduced weight and its entry are independent of the
-  // others (parallel); the claims are then made in column order
-  // (each column's best entry and that entry's row, so that the ordered
-  // claims below read sequential arrays)
+  // others (parallel); the claims, made in column order there, give each
+  // row to the lowest column whose best entry lies in it, which is what the
+  // parallel minimum over those columns (owner) gives
   std::vector<int>& best_e = ws_i1;
   std::vector<int>& best_r = ws_i2;
+  std::vector<int>& owner = pfill(db_owner, n, INT_MAX);
   best_e.resize(n);
   best_r.resize(n);
 #pragma omp parallel for schedule(static, 4096)
@@ -144,9 +154,19 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     best_e[i] = best;
     best_r[i] = best >= 0 ? Ci[best] : -1;
   }
+  int* own = owner.data();
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     const int r = best_r[i];
-    if (r >= 0 && !row_done[r]) {
+    if (r < 0) continue;
+    int cur = __atomic_load_n(own + r, __ATOMIC_RELAXED);
+    while (i < cur && !__atomic_compare_exchange_n(own + r, &cur, i, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+    }
+  }
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    const int r = best_r[i];
+    if (r >= 0 && own[r] == i) {
       col_done[i] = 1;
       row_done[r] = 1;
       match[r] = i;
@@ -256,13 +276,14 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
 #pragma omp parallel for schedule(static)
   for (int c = 0; c < n; c++) db_row_perm[match[c]] = c;
   // permuted (and scaled) matrix, rows in the new order, entries stable
-  std::vector<T>& val = ws_t0;
-  val.resize(nnz);
-#pragma omp parallel for schedule(static, 4096)
-  for (int i = 0; i < n; i++)
-    for (int e = Rp[i]; e < Rp[i + 1]; e++)
-      val[e] = scale ? (T)(row_scale[i] * col_scale[Ci[e]]) * in_val[e] : in_val[e];
-  permute_rows(n, Rp, Ci, val, db_row_perm, nullptr, m_rp, m_ci, m_val);
+  const double* rs = row_scale.data();
+  const double* cs = col_scale.data();
+  const int* cip = Ci.data();
+  const T* a = in_val.data();
+  const bool sc = scale;
+  permute_rows_with(
+      n, Rp, Ci, [=](int i, int e) { return sc ? (T)(rs[i] * cs[cip[e]]) * a[e] : a[e]; }, db_row_perm, nullptr,
+      m_rp, m_ci, m_val);
 }
 
 // Symmetrised adjacency of edges [e0, e1) without self loops (duplicates

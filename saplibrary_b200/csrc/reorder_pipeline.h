@@ -64,7 +64,7 @@ class Pipeline {
   // per-node state of the DB search and of the BFS trials (refilled in
   // parallel by every run)
   std::vector<double> db_u, db_v, db_dist;
-  std::vector<int> db_match, db_bset, db_irn, db_prev;
+  std::vector<int> db_match, db_bset, db_irn, db_prev, db_owner;
   std::vector<char> db_rowdone, db_coldone, db_inb, db_visited;
   std::vector<char> bfs_tried;
   std::vector<int> bfs_pushed, bfs_level, bfs_order, bfs_claim;

@@ -129,3 +129,30 @@ def test_invalid_csr_is_rejected():
     assert ei.value.code == -100
     with pytest.raises(ValueError):
         sap.reorder_host(rp, ci, v, 2, prec="tf32")
+
+
+def random_unscaled(n, seed, reach=60, per=6):
+    """Entries of random magnitude within +-reach of the diagonal, no
+    dominant diagonal: several rows have their largest entry in the same
+    column, so the DB's greedy pass leaves rows for the augmenting-path
+    search."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for i in range(n):
+        cs = set(rng.integers(max(0, i - reach), min(n, i + reach + 1), size=per).tolist())
+        cs.add(i)
+        for c in sorted(cs):
+            rows.append(i)
+            cols.append(c)
+            vals.append(float(rng.uniform(-1, 1)))
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, np.asarray(rows) + 1, 1)
+    return np.cumsum(rp).astype(np.int32), np.asarray(cols, np.int32), np.asarray(vals)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_db_greedy_conflicts_match_oracle(seed):
+    rp, ci, v = random_unscaled(4000 + 313 * seed, seed)
+    for dtype, threads in (("float", 1), ("double", 5), ("float", 8)):
+        check_against_oracle(rp, ci, v, 6, dtype, 1e-3, threads)
+
