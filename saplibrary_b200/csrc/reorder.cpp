@@ -443,9 +443,15 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
 // buffers, concatenated in thread order, are the next batch.  Small batches
 // are scanned serially.  claim[] is INT_MAX everywhere on entry and on
 // return.
+// A queued node's neighbours placed before it are its claimer and nodes
+// after the claimer (an earlier neighbour would have queued it sooner), so
+// the order's bandwidth is the largest distance from a node to its claimer.
+// With give_up > 0 the search stops (returns false, *gave_up set) once that
+// distance reaches give_up: the order cannot have a bandwidth below it.
 static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& off, const std::vector<int>& adj,
                           const std::vector<int>& degree, std::vector<int>& pushed, std::vector<int>& level,
-                          std::vector<int>& order, std::vector<int>& claim) {
+                          std::vector<int>& order, std::vector<int>& claim, int give_up = 0,
+                          bool* gave_up = nullptr, int* bandwidth = nullptr) {
   constexpr int kSerialBatch = 384;
   const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
   int h0 = 0, t0 = 1, scan = 0, serial_total = 0;
@@ -455,6 +461,9 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
   order[0] = root;
   int* cl = claim.data();
   std::vector<int> made(nt + 1, 0);  // nodes queued by each thread in this batch
+  std::vector<int> reach(nt, 0);     // per thread: largest position - claimer position in this batch
+  int bw = 0;
+  if (gave_up) *gave_up = false;
   using Kids = std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree>;
 #pragma omp parallel num_threads(nt)
   {
@@ -478,6 +487,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
               kids.push(std::make_pair(t, degree[t]));
               level[t] = lv + 1;
             }
+            if (!kids.empty()) bw = std::max(bw, tail + (int)kids.size() - 1 - k);
             while (!kids.empty()) {
               order[tail++] = kids.top().first;
               kids.pop();
@@ -510,6 +520,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
         // one thread holds it); the others see another claim or INT_MAX
         out.clear();
         size_t c = 0;
+        int far = INT_MIN;  // largest (index in out) - claimer position
         for (int k = k0; k < k1; k++) {
           const int lv = level[order[k]] + 1;
           for (const size_t c1 = c + per_node[k - k0]; c < c1; c++) {
@@ -520,6 +531,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
             level[t] = lv;
             kids.push(std::make_pair(t, degree[t]));
           }
+          if (!kids.empty()) far = std::max(far, (int)(out.size() + kids.size()) - 1 - k);
           while (!kids.empty()) {
             out.push_back(kids.top().first);
             kids.pop();
@@ -529,6 +541,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
 #pragma omp barrier
         int start = next;  // (t0 may already be advanced by the closing single)
         for (int u = 1; u <= tid; u++) start += made[u];
+        reach[tid] = far == INT_MIN ? 0 : start + far;
         std::copy(out.begin(), out.end(), order.begin() + start);
       }
 #pragma omp single
@@ -536,11 +549,18 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
         int total = serial_total;
         if (!serial) {
           total = 0;
-          for (int u = 1; u <= nth; u++) total += made[u];
+          for (int u = 1; u <= nth; u++) {
+            total += made[u];
+            bw = std::max(bw, reach[u - 1]);
+          }
         }
         h0 = t0;
         t0 += total;
-        if (t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
+        if (give_up > 0 && bw >= give_up) {
+          ok = false;
+          *gave_up = true;
+          h0 = t0;
+        } else if (t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
           int i = scan;
           while (i < n && pushed[i] == trial) i++;
           if (i >= n) {
@@ -555,6 +575,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
       }
     }
   }
+  if (bandwidth) *bandwidth = bw;
   return ok;
 }
 
@@ -610,7 +631,12 @@ int Pipeline<T>::rcm() {
       while (tried[root]) root = (root + 1) % n;
     }
     tried[root] = 1;
-    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim)) break;
+    // the last trial only matters if it lowers the bandwidth: it stops as
+    // soon as it cannot
+    bool gave_up = false;
+    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, trial > 0 ? best_bw : 0,
+                       &gave_up))
+      break;
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
     int bw = 0;
