@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <limits>
 #include <queue>
+#include <thread>
 #include <utility>
 
 #include <omp.h>
@@ -675,6 +676,14 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   // Built in parallel as a stable bucket sort: every thread counts the
   // distances of its block of rows, the counts become per-(distance, thread)
   // offsets, and each thread places its rows' values in order.
+  // The sum of squares of all entries is a sequential sum in entry order
+  // (the reference's order): one extra thread runs it meanwhile.
+  T total = T(0);
+  std::thread squares([&] {
+    T s = T(0);
+    for (int e = 0; e < nz; e++) s = s + m_val[e] * m_val[e];
+    total = s;
+  });
   int dmax = 0;
 #pragma omp parallel for schedule(static, 4096) reduction(max : dmax)
   for (int i = 0; i < n; i++)
@@ -713,8 +722,7 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     for (int i = r0; i < r1; i++)
       for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[c[std::abs(i - m_ci[e])]++] = m_val[e];
   }
-  T total = T(0);
-  for (int e = 0; e < nz; e++) total = total + m_val[e] * m_val[e];
+  squares.join();
   const T keep_min = (T(1) - frac) * total;
   T kept = total;
   // walk the groups from the longest distance down, summing squares from
@@ -805,18 +813,21 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
   // (ocnt), then row offsets, then the entries in row order
   std::vector<int>& ocnt = ws_i1;
   ocnt.assign(n + 1, 0);
+  // partition p holds rows [first(p), first(p + 1)): an entry inside its
+  // row's partition needs no division
+  auto first = [&](int p) { return p * q + std::min(p, rem); };
 #pragma omp parallel for schedule(static)
   for (int j = 0; j < n; j++) {
-    const int pr = partition_of(j, q, rem);
+    const int pr = partition_of(j, q, rem), lo = first(pr), hi = first(pr + 1);
     int dc = 0, oc = 0;
     char right = 0;
     for (int e = m_rp[j]; e < m_rp[j + 1]; e++) {
-      const int pc = partition_of(m_ci[e], q, rem);
-      if (pc == pr) {
+      const int l = m_ci[e];
+      if (l >= lo && l < hi) {
         dc++;
       } else {
         oc++;
-        right |= (char)(pc > pr);
+        right |= (char)(l >= hi);
       }
     }
     d_rp[j + 1] = dc;
@@ -833,15 +844,17 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
   offd_val.resize(ocnt[n]);
 #pragma omp parallel for schedule(static)
   for (int j = 0; j < n; j++) {
-    const int pr = partition_of(j, q, rem);
+    const int pr = partition_of(j, q, rem), lo = first(pr), hi = first(pr + 1);
     int dw = d_rp[j], ow = ocnt[j];
     for (int e = m_rp[j]; e < m_rp[j + 1]; e++) {
       const int l = m_ci[e];
-      const int pc = partition_of(l, q, rem);
-      if (pc == pr) {
+      if (l >= lo && l < hi) {
         d_ci[dw] = l;
         d_val[dw++] = m_val[e];
-      } else if (pc > pr) {
+        continue;
+      }
+      const int pc = partition_of(l, q, rem);
+      if (pc > pr) {
         const int row_end = q * pr + (pr < rem ? pr + q + 1 : rem + q);
         const int col_start = q * pc + (pc < rem ? pc : rem);
         offd_idx[ow] = (long long)(pr * 2 * KK + (size_t)(j + K - row_end) * K + (l - col_start));
