@@ -518,7 +518,10 @@ def main():
     # ---- banded workloads: GPU forms, then the complete CPU oracle runs ----------
     banded = [b for b in args.banded.split(",") if b]
     if banded:
-        line["banded"] = {name: time_banded(sap, torch, name, warm, max(args.steps, 5), ws) for name in banded}
+        # at least 5 timed steps, 15 for the 200k-row preset (~20 ms a step),
+        # whose median a cluster of host stalls can otherwise reach
+        line["banded"] = {name: time_banded(sap, torch, name, warm, max(args.steps, 5 if BANDED[name]["n"] >= 10**6 else 15),
+                                            ws) for name in banded}
     if args.ensemble > 0:
         # batched ensemble of independent banded systems (N log-uniform in
         # [2e3, 2e5], K in {8..128}, FP32 preconditioner, FGMRES to 1e-10):
