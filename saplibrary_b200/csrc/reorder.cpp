@@ -293,7 +293,8 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
 // obase: node x's range is off[x - obase]; 0 gives an array of n + 1 over
 // all nodes, nb one of ne - nb + 1 over the partition's nodes only.
 static void symmetric_adjacency(const std::vector<int>& er, const std::vector<int>& ec, int e0, int e1, int nb,
-                                int ne, int n, std::vector<int>& off, std::vector<int>& adj, int obase = 0) {
+                                int ne, int n, std::vector<int>& off, std::vector<int>& adj, int obase,
+                                std::vector<int>& pos) {
   // each edge (r, c), r != c, contributes (r -> c) then (c -> r); a node's
   // neighbours keep the order of these contributions
   off.assign(obase ? ne - nb + 1 : n + 1, 0);
@@ -306,7 +307,7 @@ static void symmetric_adjacency(const std::vector<int>& er, const std::vector<in
   for (int i = nb + 1; i <= ne; i++) o(i) += o(i - 1);
   for (int i = ne - 1; i >= nb; i--) o(i) = i > nb ? o(i - 1) : 0;  // exclusive starts
   adj.resize(o(ne));
-  std::vector<int> pos(off.begin() + (nb - obase), off.begin() + (ne - obase));
+  pos.assign(off.begin() + (nb - obase), off.begin() + (ne - obase));
   for (int e = e0; e < e1; e++) {
     const int r = er[e], c = ec[e];
     if (r == c) continue;
@@ -389,10 +390,10 @@ static void symmetric_adjacency_csr(int n, const std::vector<int>& rp, const std
 // unvisited node.  Returns false when the queue cannot be refilled.
 static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& offv, const std::vector<int>& adj,
                    const std::vector<int>* fixed_degree, std::vector<int>& pushed, std::vector<int>& level,
-                   std::vector<int>& order, int& last_level, int obase = 0) {
+                   std::vector<int>& order, int& last_level, int obase, std::vector<int>& fifo) {
   auto off = [&](int x) { return offv[x - obase]; };  // node x's range starts at off(x) (see symmetric_adjacency)
   // FIFO as an array: every node enters at most once per trial
-  std::vector<int> fifo((size_t)(ne - nb) + 2);
+  if (fifo.size() < (size_t)(ne - nb) + 2) fifo.resize((size_t)(ne - nb) + 2);
   size_t head = 0, tail = 0;
   std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree> kids;
   level[root] = 0;
@@ -894,6 +895,7 @@ void Pipeline<T>::second_level(int K, int P) {
   std::vector<int>& level_sh = pfill(bfs_level, n, 0);
   std::vector<int> pnb(P + 1, 0);
   for (int p = 0; p < P; p++) pnb[p + 1] = pnb[p] + q + (p < rem ? 1 : 0);
+  if ((int)part_scratch.size() < P) part_scratch.resize(P);
   // One partition.  Returns false, in the parallel pass, when a trial root
   // leaves the partition (the reference's root search walks on to the next
   // index): that trial's writes reach another partition, so every partition
@@ -904,14 +906,17 @@ void Pipeline<T>::second_level(int K, int P) {
     for (int i = nb; i < ne; i++) second_order[i] = i;
     int best_bw = 0;
     for (int e = e0; e < e1; e++) best_bw = std::max(best_bw, std::abs(row[e] - d_ci[e]));
-    std::vector<int> off, adj;
+    PartScratch& sc = part_scratch[p];
+    std::vector<int>& off = sc.off;
+    std::vector<int>& adj = sc.adj;
     const int obase = serial ? 0 : nb;
-    symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj, obase);
+    symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj, obase, sc.pos);
     // row lengths of the partition's nodes as the reference computes them:
     // its transform covers row_offsets[nb+1 .. ne), one element short, so the
     // partition's last node keeps degree 0 (graph.h:1622-1625), which makes
     // it the first trial's root unless a node has no entries at all
-    std::vector<int> rowlen(ne - nb, 0);
+    std::vector<int>& rowlen = sc.rowlen;
+    rowlen.assign(ne - nb, 0);
     for (int i = nb; i < ne - 1; i++) rowlen[i - nb] = d_rp[i + 1] - d_rp[i];
     std::vector<char> tried_own;
     std::vector<int> pushed_own, level_own;
@@ -947,7 +952,7 @@ void Pipeline<T>::second_level(int K, int P) {
       }
       if (!serial && (root < nb || root >= ne)) return false;
       tried[root] = 1;
-      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level, obase)) break;
+      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level, obase, sc.fifo)) break;
       for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
       int bw = 0;
       for (int e = e0; e < e1; e++) bw = std::max(bw, std::abs(second_pos[row[e]] - second_pos[d_ci[e]]));

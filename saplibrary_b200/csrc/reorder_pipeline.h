@@ -68,6 +68,13 @@ class Pipeline {
   std::vector<char> db_rowdone, db_coldone, db_inb, db_visited;
   std::vector<char> bfs_tried;
   std::vector<int> bfs_pushed, bfs_level, bfs_order, bfs_claim;
+  // per partition of the second level: its adjacency, row lengths and BFS
+  // queue (kept, so that the partitions' threads do not allocate and fault
+  // in new pages side by side on every setup)
+  struct PartScratch {
+    std::vector<int> off, adj, pos, rowlen, fifo;
+  };
+  std::vector<PartScratch> part_scratch;
 
   // wall time of the stages of run(), in order (ms)
   std::vector<std::pair<const char*, double>> stage_ms;
