@@ -448,12 +448,16 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
 // A queued node's neighbours placed before it are its claimer and nodes
 // after the claimer (an earlier neighbour would have queued it sooner), so
 // the order's bandwidth is the largest distance from a node to its claimer.
-// With give_up > 0 the search stops (returns false, *gave_up set) once that
-// distance reaches give_up: the order cannot have a bandwidth below it.
+// With give_up > 0 the order is given up (*gave_up set) once that distance
+// reaches give_up: it cannot have a bandwidth below it.  The search then
+// stops (returns false), or, with keep_levels, goes on without ordering to
+// fill level[]: a node's level is its batch's, and the batches hold the same
+// nodes (the unqueued neighbours of the previous batch, or a restart) in
+// whatever order they are queued, so the levels equal the ordered search's.
 static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& off, const std::vector<int>& adj,
                           const std::vector<int>& degree, std::vector<int>& pushed, std::vector<int>& level,
                           std::vector<int>& order, std::vector<int>& claim, int give_up = 0,
-                          bool* gave_up = nullptr, int* bandwidth = nullptr) {
+                          bool* gave_up = nullptr, int* bandwidth = nullptr, bool keep_levels = false) {
   constexpr int kSerialBatch = 384;
   const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
   int h0 = 0, t0 = 1, scan = 0, serial_total = 0;
@@ -465,6 +469,7 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
   std::vector<int> made(nt + 1, 0);  // nodes queued by each thread in this batch
   std::vector<int> reach(nt, 0);     // per thread: largest position - claimer position in this batch
   int bw = 0;
+  bool unordered = false;  // the order was given up: levels only
   if (gave_up) *gave_up = false;
   using Kids = std::priority_queue<std::pair<int, int>, std::vector<std::pair<int, int>>, ByDegree>;
 #pragma omp parallel num_threads(nt)
@@ -475,8 +480,31 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
     for (;;) {
       const int m = t0 - h0, next = t0;  // shared, stable until the closing single
       if (m == 0) break;
-      const bool serial = m < kSerialBatch;
-      if (serial) {
+      const bool serial = m < kSerialBatch, unord = unordered;
+      if (unord) {
+        // levels only: every thread queues the unqueued neighbours of its
+        // range of the batch, each taken once by whichever thread marks it
+        const int k0 = h0 + (int)((long long)m * tid / nth), k1 = h0 + (int)((long long)m * (tid + 1) / nth);
+        out.clear();
+        int* pu = pushed.data();
+        for (int k = k0; k < k1; k++) {
+          const int u = order[k], lv = level[u] + 1;
+          for (int e = off[u]; e < off[u + 1]; e++) {
+            const int t = adj[e];
+            int cur = __atomic_load_n(pu + t, __ATOMIC_RELAXED);
+            if (cur == trial) continue;
+            if (__atomic_compare_exchange_n(pu + t, &cur, trial, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+              level[t] = lv;
+              out.push_back(t);
+            }
+          }
+        }
+        made[tid + 1] = (int)out.size();
+#pragma omp barrier
+        int start = next;
+        for (int u = 1; u <= tid; u++) start += made[u];
+        std::copy(out.begin(), out.end(), order.begin() + start);
+      } else if (serial) {
 #pragma omp single
         {
           int tail = t0;
@@ -549,20 +577,27 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
 #pragma omp single
       {
         int total = serial_total;
-        if (!serial) {
+        if (unord || !serial) {
           total = 0;
           for (int u = 1; u <= nth; u++) {
             total += made[u];
-            bw = std::max(bw, reach[u - 1]);
+            if (!unord) bw = std::max(bw, reach[u - 1]);
           }
         }
         h0 = t0;
         t0 += total;
-        if (give_up > 0 && bw >= give_up) {
-          ok = false;
-          *gave_up = true;
-          h0 = t0;
-        } else if (t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
+        bool stop = false;
+        if (!unord && give_up > 0 && bw >= give_up) {
+          if (gave_up) *gave_up = true;
+          if (keep_levels) {
+            unordered = true;
+          } else {
+            ok = false;
+            stop = true;
+            h0 = t0;
+          }
+        }
+        if (!stop && t0 == h0 && t0 < n) {  // queue empty: restart at the lowest unqueued node
           int i = scan;
           while (i < n && pushed[i] == trial) i++;
           if (i >= n) {
@@ -633,21 +668,24 @@ int Pipeline<T>::rcm() {
       while (tried[root]) root = (root + 1) % n;
     }
     tried[root] = 1;
-    // the last trial only matters if it lowers the bandwidth: it stops as
-    // soon as it cannot
+    // a trial's order only matters if it lowers the bandwidth: the search
+    // gives it up as soon as it cannot; the first trial still fills its
+    // levels (the next trial's root comes from them), the last one stops
     bool gave_up = false;
-    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, trial > 0 ? best_bw : 0,
-                       &gave_up))
+    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, best_bw, &gave_up, nullptr,
+                       trial == 0))
       break;
+    if (!gave_up) {
 #pragma omp parallel for schedule(static)
-    for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
-    int bw = 0;
+      for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
+      int bw = 0;
 #pragma omp parallel for reduction(max : bw) schedule(static)
-    for (int e = 0; e < nz; e++) bw = std::max(bw, std::abs(rcm_pos[row[e]] - rcm_pos[m_ci[e]]));
-    if (best_bw > bw) {
-      best_bw = bw;
-      rcm_order = order;
-      kept = true;
+      for (int e = 0; e < nz; e++) bw = std::max(bw, std::abs(rcm_pos[row[e]] - rcm_pos[m_ci[e]]));
+      if (best_bw > bw) {
+        best_bw = bw;
+        rcm_order = order;
+        kept = true;
+      }
     }
     if (trial > 0) break;            // tracked level never grows: the second trial is the last
     if (best_bw <= 256) break;       // BANDWIDTH_THRESHOLD
