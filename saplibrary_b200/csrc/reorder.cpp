@@ -388,9 +388,16 @@ static void symmetric_adjacency_csr(int n, const std::vector<int>& rp, const std
 // children are queued in increasing `degree` order through a binary heap
 // (ties broken by the heap, as in the reference), restarts take the lowest
 // unvisited node.  Returns false when the queue cannot be refilled.
+// The order's bandwidth is the largest distance from a queued node to the
+// node that queued it (see cm_bfs_levels).  With give_up > 0 the order is
+// given up (*gave_up set) once that distance reaches give_up, and the rest
+// of the search only fills level[] and last_level, queueing children in
+// adjacency order: the levels and the last level do not depend on the
+// order inside a batch.
 static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& offv, const std::vector<int>& adj,
                    const std::vector<int>* fixed_degree, std::vector<int>& pushed, std::vector<int>& level,
-                   std::vector<int>& order, int& last_level, int obase, std::vector<int>& fifo) {
+                   std::vector<int>& order, int& last_level, int obase, std::vector<int>& fifo, int give_up = 0,
+                   bool* gave_up = nullptr) {
   auto off = [&](int x) { return offv[x - obase]; };  // node x's range starts at off(x) (see symmetric_adjacency)
   // FIFO as an array: every node enters at most once per trial
   if (fifo.size() < (size_t)(ne - nb) + 2) fifo.resize((size_t)(ne - nb) + 2);
@@ -400,6 +407,9 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
   pushed[root] = trial;
   fifo[tail++] = root;
   int left = ne - nb, out = nb, scan = nb;
+  bool ordered = true;
+  long long bw = 0;
+  if (gave_up) *gave_up = false;
   while (left--) {
     if (head == tail) {
       left++;
@@ -414,6 +424,17 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
     int node = fifo[head++];
     order[out++] = node;
     int lv = level[node];
+    if (!ordered) {
+      for (int e = off(node); e < off(node + 1); e++) {
+        int t = adj[e];
+        if (pushed[t] == trial) continue;
+        pushed[t] = trial;
+        fifo[tail++] = t;
+        level[t] = lv + 1;
+        last_level = lv + 1;
+      }
+      continue;
+    }
     for (int e = off(node); e < off(node + 1); e++) {
       int t = adj[e];
       if (pushed[t] == trial) continue;
@@ -423,9 +444,14 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
       level[t] = lv + 1;
       last_level = lv + 1;
     }
+    if (!kids.empty()) bw = std::max(bw, (long long)(tail + kids.size() - 1) - (long long)(head - 1));
     while (!kids.empty()) {
       fifo[tail++] = kids.top().first;
       kids.pop();
+    }
+    if (give_up > 0 && bw >= give_up) {
+      ordered = false;
+      if (gave_up) *gave_up = true;
     }
   }
   return true;
@@ -990,13 +1016,20 @@ void Pipeline<T>::second_level(int K, int P) {
       }
       if (!serial && (root < nb || root >= ne)) return false;
       tried[root] = 1;
-      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level, obase, sc.fifo)) break;
-      for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
-      int bw = 0;
-      for (int e = e0; e < e1; e++) bw = std::max(bw, std::abs(second_pos[row[e]] - second_pos[d_ci[e]]));
-      if (best_bw > bw) {
-        best_bw = bw;
-        std::copy(order.begin() + nb, order.begin() + ne, second_order.begin() + nb);
+      // an order that cannot lower the bandwidth is given up early; the
+      // trial still yields its levels for the stopping rule and next root
+      bool gave_up = false;
+      if (!cm_bfs(root, nb, ne, trial, off, adj, nullptr, pushed, level, order, last_level, obase, sc.fifo, best_bw,
+                  &gave_up))
+        break;
+      if (!gave_up) {
+        for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
+        int bw = 0;
+        for (int e = e0; e < e1; e++) bw = std::max(bw, std::abs(second_pos[row[e]] - second_pos[d_ci[e]]));
+        if (best_bw > bw) {
+          best_bw = bw;
+          std::copy(order.begin() + nb, order.begin() + ne, second_order.begin() + nb);
+        }
       }
       if (trial > 0) {
         if (prev_last >= last_level) break;
