@@ -320,56 +320,103 @@ static void symmetric_adjacency(const std::vector<int>& er, const std::vector<in
 // parallel.  Node x's list in the serial builder's order is: the rows r < x
 // of the entries (r, x) in entry order, then row x's own columns, then the
 // rows r > x of the entries (r, x).  The column lists are a stable transpose:
-// every thread counts the columns of its block of rows, the counts are
-// turned into per-(column, thread) offsets, and each thread places its rows
-// in order, so every column lists its rows in entry order without sorting.
+// every thread counts the columns of its block of rows (counters only over
+// the column range its rows reach), the counts are turned into
+// per-(column, thread) offsets, and each thread places its rows in order,
+// so every column lists its rows in entry order without sorting.
 static void symmetric_adjacency_csr(int n, const std::vector<int>& rp, const std::vector<int>& ci,
                                     std::vector<int>& off, std::vector<int>& adj, std::vector<int>& cnt,
                                     std::vector<int>& cstart, std::vector<int>& tr) {
   const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
-  cnt.resize((size_t)nt * n);
-  cstart.assign(n + 1, 0);
-  off.assign(n + 1, 0);
+  cstart.resize(n + 1);
+  off.resize(n + 1);
+  off[0] = 0;
+  cstart[0] = 0;
+  // per thread: the column range [lo, hi] its rows reach (a band matrix
+  // keeps it near the thread's rows), where its counters live
+  std::vector<int> lo(nt, INT_MAX), hi(nt, -1), sa(nt + 1, 0), sb(nt + 1, 0);
+  std::vector<size_t> base(nt + 1, 0);
 #pragma omp parallel num_threads(nt)
   {
     const int t = omp_get_thread_num(), nth = omp_get_num_threads();
     const int r0 = (int)((long long)n * t / nth), r1 = (int)((long long)n * (t + 1) / nth);
-    int* c = cnt.data() + (size_t)t * n;
-    std::fill(c, c + n, 0);
+    int l = INT_MAX, h = -1;
     for (int r = r0; r < r1; r++) {
       int own = 0;
-      for (int e = rp[r]; e < rp[r + 1]; e++)
-        if (ci[e] != r) {
+      for (int e = rp[r]; e < rp[r + 1]; e++) {
+        const int x = ci[e];
+        if (x != r) {
           own++;
-          c[ci[e]]++;
+          l = std::min(l, x);
+          h = std::max(h, x);
         }
+      }
       off[r + 1] = own;
     }
+    lo[t] = l;
+    hi[t] = h;
 #pragma omp barrier
+#pragma omp single
+    {
+      for (int u = 0; u < nth; u++) base[u + 1] = base[u] + (size_t)std::max(0, hi[u] - lo[u] + 1);
+      cnt.resize(base[nth]);
+    }
+    int* c = cnt.data() + base[t];  // counter of column x at c[x - l]
+    std::fill(c, c + std::max(0, h - l + 1), 0);
+    for (int r = r0; r < r1; r++)
+      for (int e = rp[r]; e < rp[r + 1]; e++)
+        if (ci[e] != r) c[ci[e] - l]++;
+#pragma omp barrier
+    // per column: the threads' counts turned into their offsets inside the
+    // column, the column's total in cstart[x + 1]
 #pragma omp for schedule(static)
     for (int x = 0; x < n; x++) {
       int sum = 0;
       for (int u = 0; u < nth; u++) {
-        int& v = cnt[(size_t)u * n + x];
+        if (x < lo[u] || x > hi[u]) continue;
+        int& v = cnt[base[u] + (x - lo[u])];
         const int k = v;
         v = sum;
         sum += k;
       }
       cstart[x + 1] = sum;
     }
+    // prefix sums (parallel, in two passes): cstart over the column totals,
+    // off over own + column counts
+    const int x0 = (int)((long long)n * t / nth), x1 = (int)((long long)n * (t + 1) / nth);
+    {
+      int s1 = 0, s2 = 0;
+      for (int i = x0; i < x1; i++) {
+        s1 += off[i + 1] + cstart[i + 1];
+        s2 += cstart[i + 1];
+      }
+      sa[t + 1] = s1;
+      sb[t + 1] = s2;
+    }
+#pragma omp barrier
+    {
+      int s1 = 0, s2 = 0;
+      for (int u = 0; u < t; u++) {
+        s1 += sa[u + 1];
+        s2 += sb[u + 1];
+      }
+      for (int i = x0; i < x1; i++) {
+        s1 += off[i + 1] + cstart[i + 1];
+        s2 += cstart[i + 1];
+        off[i + 1] = s1;
+        cstart[i + 1] = s2;
+      }
+    }
+#pragma omp barrier
 #pragma omp single
     {
-      for (int i = 0; i < n; i++) {
-        off[i + 1] += off[i] + cstart[i + 1];
-        cstart[i + 1] += cstart[i];
-      }
       tr.resize(cstart[n]);
       adj.resize(off[n]);
     }
     for (int r = r0; r < r1; r++)
       for (int e = rp[r]; e < rp[r + 1]; e++) {
         const int x = ci[e];
-        if (x != r) tr[cstart[x] + c[x]++] = r;
+        if (x != r) tr[cstart[x] + c[x - l]++] = r;
       }
 #pragma omp barrier
 #pragma omp for schedule(static)
