@@ -27,8 +27,8 @@ banded workload (key "cpu_complete": both banded workloads); the reference
 arm (--impl reference) reports itself unavailable, because one complete CPU
 solve of the 1M-row sparse workload takes tens of minutes.  Key "ensemble":
 128 independent banded systems (N log-uniform in [2e3, 2e5], K in
-{8, 16, 32, 64, 128}) solved by one batched call and one by one (--ensemble
-sets the count, 0 skips it).
+{8, 16, 32, 64, 128}) solved by one batched call and one by one, each leg
+twice, best of the two (--ensemble sets the count, 0 skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -518,16 +518,17 @@ def main():
     # ---- banded workloads: GPU forms, then the complete CPU oracle runs ----------
     banded = [b for b in args.banded.split(",") if b]
     if banded:
-        # at least 5 timed steps, 15 for the 200k-row preset (~20 ms a step),
-        # whose median a cluster of host stalls can otherwise reach
-        line["banded"] = {name: time_banded(sap, torch, name, warm, max(args.steps, 5 if BANDED[name]["n"] >= 10**6 else 15),
+        # at least 9 timed steps, 15 for the 200k-row preset (~20 ms a step):
+        # host stalls on a shared machine come in clusters that can reach
+        # the median of fewer steps
+        line["banded"] = {name: time_banded(sap, torch, name, warm, max(args.steps, 9 if BANDED[name]["n"] >= 10**6 else 15),
                                             ws) for name in banded}
     if args.ensemble > 0:
         # batched ensemble of independent banded systems (N log-uniform in
         # [2e3, 2e5], K in {8..128}, FP32 preconditioner, FGMRES to 1e-10):
         # one solve_batch call against the same systems solved one by one
         from saplibrary_b200 import ensemble
-        line["ensemble"] = ensemble.run(count=args.ensemble, seed=3, P=8, prec="float")
+        line["ensemble"] = ensemble.run(count=args.ensemble, seed=3, P=8, prec="float", reps=2)
     if rank == 0 and not args.no_cpu_baseline:
         cpu_runs = {}
         for name in banded:
