@@ -26,6 +26,30 @@
 namespace sapb {
 namespace rp {
 
+void prefix_sum(int* a, int n) {
+  const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
+  if (nt == 1 || n < (1 << 16)) {
+    for (int i = 0; i < n; i++) a[i + 1] += a[i];
+    return;
+  }
+  std::vector<int> part(nt + 1, 0);
+#pragma omp parallel num_threads(nt)
+  {
+    const int t = omp_get_thread_num(), nth = omp_get_num_threads();
+    const int i0 = (int)((long long)n * t / nth), i1 = (int)((long long)n * (t + 1) / nth);
+    int s = 0;
+    for (int i = i0; i < i1; i++) s += a[i + 1];
+    part[t + 1] = s;
+#pragma omp barrier
+    int run = a[0];
+    for (int u = 0; u < t; u++) run += part[u + 1];
+    for (int i = i0; i < i1; i++) {
+      run += a[i + 1];
+      a[i + 1] = run;
+    }
+  }
+}
+
 namespace {
 
 constexpr double kInf = 1e37;  // Graph<T>::LOC_INFINITY (graph.h:287-288)
@@ -72,7 +96,7 @@ void permute_rows_with(int n, const std::vector<int>& rp, const std::vector<int>
   out_rp[0] = 0;
 #pragma omp parallel for schedule(static)
   for (int r = 0; r < n; r++) out_rp[newpos[r] + 1] = rp[r + 1] - rp[r];
-  for (int i = 0; i < n; i++) out_rp[i + 1] += out_rp[i];
+  prefix_sum(out_rp.data(), n);
   out_ci.resize(ci.size());
   out_val.resize(ci.size());
   const int* cm = colmap ? colmap->data() : nullptr;
@@ -886,7 +910,7 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     for (int e = rp0[i]; e < rp0[i + 1]; e++) c += std::abs(i - ci0[e]) <= dkeep;
     m_rp[i + 1] = c;
   }
-  for (int i = 0; i < n; i++) m_rp[i + 1] += m_rp[i];
+  prefix_sum(m_rp.data(), n);
   m_ci.resize(m_rp[n]);
   m_val.resize(m_rp[n]);
 #pragma omp parallel for schedule(static, 4096)
@@ -946,10 +970,8 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
     ocnt[j + 1] = oc;
     couples_right[j] = right;
   }
-  for (int i = 0; i < n; i++) {
-    d_rp[i + 1] += d_rp[i];
-    ocnt[i + 1] += ocnt[i];
-  }
+  prefix_sum(d_rp.data(), n);
+  prefix_sum(ocnt.data(), n);
   d_ci.resize(d_rp[n]);
   d_val.resize(d_rp[n]);
   offd_idx.resize(ocnt[n]);

@@ -21,6 +21,11 @@ struct Error : public std::runtime_error {
 
 namespace rp {
 
+// a[i + 1] += a[i] for i = 0 .. n-1 (running sums of a[1..n] after a[0]),
+// in parallel blocks above a size threshold; integer sums, so the result
+// equals the serial loop's.
+void prefix_sum(int* a, int n);
+
 // T is the preconditioner value type: the reference runs the whole
 // reordering on the matrix converted to it (precond.h:1667-1713).
 template <typename T>

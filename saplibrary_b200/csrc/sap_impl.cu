@@ -426,7 +426,7 @@ class PrecondT : public PrecBase {
       for (int e = A.rp_h[i]; e < A.rp_h[i + 1]; e++) c += (T)A.v_h[e] != T(0);
       pl.in_rp[i + 1] = c;
     }
-    for (int i = 0; i < n; i++) pl.in_rp[i + 1] += pl.in_rp[i];
+    rp::prefix_sum(pl.in_rp.data(), n);
     pl.in_ci.resize(pl.in_rp[n]);
     pl.in_val.resize(pl.in_rp[n]);
 #pragma omp parallel for schedule(static, 4096)
