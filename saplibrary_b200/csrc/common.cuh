@@ -5,7 +5,12 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdlib>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <new>
+#include <unordered_map>
 #include <utility>
 #include <cstdint>
 #include <cstdio>
@@ -131,6 +136,101 @@ struct DefaultInitAllocator : std::allocator<T> {
 };
 template <typename T>
 using HostVec = std::vector<T, DefaultInitAllocator<T>>;
+
+// Page-locked host blocks kept for reuse (PinnedPoolAllocator): a block
+// released by one host copy of a matrix is taken by the next copy that fits
+// in it (at most twice its size), so repeated copies neither fault in fresh
+// pages nor go through the driver's pageable staging when they are
+// uploaded.  Free blocks beyond kMaxFreeBytes go back to the driver, largest
+// first.  Where page-locked memory cannot be had, blocks come from malloc.
+// The pool is never destroyed (no driver call during static teardown).
+class PinnedPool {
+ public:
+  static PinnedPool& instance() {
+    static PinnedPool* pool = new PinnedPool();
+    return *pool;
+  }
+  void* take(size_t bytes) {
+    if (bytes == 0) bytes = 1;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      auto it = free_.lower_bound(bytes);
+      if (it != free_.end() && it->first / 2 <= bytes) {
+        void* p = it->second;
+        used_[p] = it->first;
+        free_bytes_ -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) == cudaSuccess && p) {
+      std::lock_guard<std::mutex> lk(mu_);
+      used_[p] = bytes;
+      return p;
+    }
+    (void)cudaGetLastError();  // a failed allocation is not sticky: clear it
+    p = std::malloc(bytes);
+    if (!p) throw std::bad_alloc();
+    std::lock_guard<std::mutex> lk(mu_);
+    plain_[p] = bytes;
+    return p;
+  }
+  void give(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu_);
+    auto pl = plain_.find(p);
+    if (pl != plain_.end()) {
+      plain_.erase(pl);
+      std::free(p);
+      return;
+    }
+    auto it = used_.find(p);
+    if (it == used_.end()) return;
+    free_.emplace(it->second, p);
+    free_bytes_ += it->second;
+    used_.erase(it);
+    while (free_bytes_ > kMaxFreeBytes && !free_.empty()) {
+      auto big = std::prev(free_.end());
+      free_bytes_ -= big->first;
+      cudaFreeHost(big->second);
+      free_.erase(big);
+    }
+  }
+
+ private:
+  static constexpr size_t kMaxFreeBytes = size_t(1) << 31;
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  std::unordered_map<void*, size_t> used_, plain_;
+  size_t free_bytes_ = 0;
+};
+
+// Allocator over PinnedPool with the construction of DefaultInitAllocator
+// (elements left uninitialised until the copy writes them).
+template <typename T>
+struct PinnedPoolAllocator {
+  using value_type = T;
+  PinnedPoolAllocator() = default;
+  template <typename U>
+  PinnedPoolAllocator(const PinnedPoolAllocator<U>&) noexcept {}
+  T* allocate(size_t n) { return static_cast<T*>(PinnedPool::instance().take(n * sizeof(T))); }
+  void deallocate(T* p, size_t) noexcept { PinnedPool::instance().give(p); }
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+  template <typename U>
+  bool operator==(const PinnedPoolAllocator<U>&) const noexcept { return true; }
+  template <typename U>
+  bool operator!=(const PinnedPoolAllocator<U>&) const noexcept { return false; }
+};
+template <typename T>
+using PinnedHostVec = std::vector<T, PinnedPoolAllocator<T>>;
 
 // Page-locked host buffer (grow-only) for device->host copies at full speed.
 template <typename T>

@@ -76,12 +76,16 @@ struct Banded {
 
 struct Csr {
   int n = 0, nnz = 0;
+  // host copies (reordering runs on the host), page-locked blocks from a
+  // pool: the uploads run at full speed and repeated copies reuse warm
+  // pages.  Declared before the device buffers, so that they go back to the
+  // pool only after those are freed (cudaFree waits for copies in flight).
+  PinnedHostVec<int> rp_h, ci_h;
+  PinnedHostVec<double> v_h;
   DBuf<int> rp, ci;
   DBuf<double> v;
   DBuf<int> blk;  // row blocks of k_spmv_csr_blocks
   int nblk = 0;
-  HostVec<int> rp_h, ci_h;  // host copies of the pattern (reordering runs on the host)
-  HostVec<double> v_h;
 };
 
 struct Spmv {
