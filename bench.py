@@ -477,12 +477,19 @@ def main():
         for _ in range(2):
             step_e2e()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        # every step timed on its own (the result is on the host when a step
+        # returns): the median is the value, the mean is reported beside it
+        # (host stalls of a shared machine land in single steps)
+        e2e_steps = []
         for _ in range(args.steps):
+            t0 = time.perf_counter()
             step_e2e()
-        e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, ws)
+            e2e_steps.append(time.perf_counter() - t0)
+        e2e_s = max_over_ranks(sorted(e2e_steps)[len(e2e_steps) // 2], ws)
         h2d = rp.nbytes + ci.nbytes + v.nbytes + 2 * n * 8
-        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": n * 8}
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": n * 8,
+               "mean_s": max_over_ranks(sum(e2e_steps) / len(e2e_steps), ws),
+               "step_s": [round(t, 4) for t in e2e_steps]}
         del solver_h
 
     # ---- roofline of the dominant kernel: the block-sweep gemv (k_tgemv) ----------
