@@ -83,26 +83,29 @@ void csr_from_keys(int n, const std::vector<int>& key, const std::vector<int>& c
   out_rp[n] = (int)m;
 }
 
-// Rows moved as whole units: row r of (rp, ci, val) becomes row newpos[r]
+// Rows moved as whole units: row oldrow[k] of (rp, ci, val) becomes row k
 // with its entries in their order and columns relabelled through colmap
 // (none when null).  This is exactly what the stable counting sort by
-// key = newpos[row] (csr_from_keys) produces, built row-parallel.
-// value_of(r, e) gives the value written for entry e of row r.
+// key = new position of the row (csr_from_keys) produces, built in parallel
+// over the new rows (the writes stream; a band-like result keeps the reads
+// through colmap and value_of near each other).
+// value_of(r, e) gives the value written for entry e of old row r.
 template <typename V, typename F>
 void permute_rows_with(int n, const std::vector<int>& rp, const std::vector<int>& ci, F value_of,
-                       const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
+                       const int* oldrow, const std::vector<int>* colmap, std::vector<int>& out_rp,
                        std::vector<int>& out_ci, std::vector<V>& out_val) {
   out_rp.resize(n + 1);
   out_rp[0] = 0;
 #pragma omp parallel for schedule(static)
-  for (int r = 0; r < n; r++) out_rp[newpos[r] + 1] = rp[r + 1] - rp[r];
+  for (int k = 0; k < n; k++) out_rp[k + 1] = rp[oldrow[k] + 1] - rp[oldrow[k]];
   prefix_sum(out_rp.data(), n);
   out_ci.resize(ci.size());
   out_val.resize(ci.size());
   const int* cm = colmap ? colmap->data() : nullptr;
 #pragma omp parallel for schedule(static, 4096)
-  for (int r = 0; r < n; r++) {
-    int d = out_rp[newpos[r]];
+  for (int k = 0; k < n; k++) {
+    const int r = oldrow[k];
+    int d = out_rp[k];
     for (int e = rp[r]; e < rp[r + 1]; e++, d++) {
       out_ci[d] = cm ? cm[ci[e]] : ci[e];
       out_val[d] = value_of(r, e);
@@ -112,10 +115,10 @@ void permute_rows_with(int n, const std::vector<int>& rp, const std::vector<int>
 
 template <typename V>
 void permute_rows(int n, const std::vector<int>& rp, const std::vector<int>& ci, const std::vector<V>& val,
-                  const std::vector<int>& newpos, const std::vector<int>* colmap, std::vector<int>& out_rp,
+                  const std::vector<int>& oldrow, const std::vector<int>* colmap, std::vector<int>& out_rp,
                   std::vector<int>& out_ci, std::vector<V>& out_val) {
   const V* v = val.data();
-  permute_rows_with(n, rp, ci, [v](int, int e) { return v[e]; }, newpos, colmap, out_rp, out_ci, out_val);
+  permute_rows_with(n, rp, ci, [v](int, int e) { return v[e]; }, oldrow.data(), colmap, out_rp, out_ci, out_val);
 }
 
 int partition_of(int r, int q, int rem) {
@@ -180,6 +183,15 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     best_r[i] = best >= 0 ? Ci[best] : -1;
   }
   int* own = owner.data();
+  // a first pass of plain stores leaves in owner[r] one of the columns that
+  // chose r (writes to different rows overlap; atomic updates would not);
+  // the second lowers it to the smallest, atomically, where it is not
+  // already (only rows chosen by several columns)
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    const int r = best_r[i];
+    if (r >= 0 && i < __atomic_load_n(own + r, __ATOMIC_RELAXED)) __atomic_store_n(own + r, i, __ATOMIC_RELAXED);
+  }
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     const int r = best_r[i];
@@ -188,13 +200,19 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
     while (i < cur && !__atomic_compare_exchange_n(own + r, &cur, i, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
     }
   }
+  // the claims written on each side in index order (scattered byte writes
+  // from many threads would share cache lines)
+#pragma omp parallel for schedule(static, 4096)
+  for (int r = 0; r < n; r++) {
+    if (own[r] == INT_MAX) continue;
+    row_done[r] = 1;
+    match[r] = own[r];
+  }
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     const int r = best_r[i];
     if (r >= 0 && own[r] == i) {
       col_done[i] = 1;
-      row_done[r] = 1;
-      match[r] = i;
       rev_match[i] = best_e[i];
     }
   }
@@ -306,8 +324,9 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   const int* cip = Ci.data();
   const T* a = in_val.data();
   const bool sc = scale;
+  // (row match[c] moves to position c)
   permute_rows_with(
-      n, Rp, Ci, [=](int i, int e) { return sc ? (T)(rs[i] * cs[cip[e]]) * a[e] : a[e]; }, db_row_perm, nullptr,
+      n, Rp, Ci, [=](int i, int e) { return sc ? (T)(rs[i] * cs[cip[e]]) * a[e] : a[e]; }, match.data(), nullptr,
       m_rp, m_ci, m_val);
 }
 
@@ -795,7 +814,7 @@ int Pipeline<T>::rcm() {
   tmp_rp.swap(m_rp);
   tmp_ci.swap(m_ci);
   tmp_val.swap(m_val);
-  permute_rows(n, tmp_rp, tmp_ci, tmp_val, rcm_pos, &rcm_pos, m_rp, m_ci, m_val);
+  permute_rows(n, tmp_rp, tmp_ci, tmp_val, rcm_order, &rcm_pos, m_rp, m_ci, m_val);
   return best_bw;
 }
 
@@ -1120,7 +1139,7 @@ void Pipeline<T>::second_level(int K, int P) {
   tmp_rp.swap(d_rp);
   tmp_ci.swap(d_ci);
   tmp_val.swap(d_val);
-  permute_rows(n, tmp_rp, tmp_ci, tmp_val, second_pos, &second_pos, d_rp, d_ci, d_val);
+  permute_rows(n, tmp_rp, tmp_ci, tmp_val, second_order, &second_pos, d_rp, d_ci, d_val);
   first_rows.assign(std::max(P - 1, 0), 0);
   int last = 0;
   for (int i = 0; i < P - 1; i++) {
