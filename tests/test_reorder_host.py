@@ -156,3 +156,39 @@ def test_db_greedy_conflicts_match_oracle(seed):
     for dtype, threads in (("float", 1), ("double", 5), ("float", 8)):
         check_against_oracle(rp, ci, v, 6, dtype, 1e-3, threads)
 
+
+def symmetric_permuted(m, fill, reach, seed):
+    """The convection-diffusion matrix under a random symmetric permutation
+    (rows and columns alike): DB restores the diagonal but not the band, so
+    RCM lowers the bandwidth and its order is kept."""
+    rp, ci, v, _ = convection_diffusion_csr(m=m, fill_per_row=fill, fill_reach=reach, seed=seed,
+                                            permute_rows=False)
+    n = rp.size - 1
+    p = np.random.default_rng(seed).permutation(n)
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    nr, nc = p[rows], p[ci]
+    order = np.lexsort((nc, nr))
+    nr, nc, nv = nr[order], nc[order], v[order]
+    out_rp = np.zeros(n + 1, np.int64)
+    np.add.at(out_rp, nr + 1, 1)
+    return np.cumsum(out_rp).astype(np.int32), nc.astype(np.int32), nv
+
+
+@pytest.mark.parametrize("m,fill,reach,kept", [
+    (90, 1, 30, True),      # RCM order kept (bandwidth 8,060 -> 168)
+    (400, 0, 1, True),      # kept, batches above the serial threshold (parallel BFS)
+    (200, 2, 3000, False),  # long-range fill: every trial gives its order up
+    (400, 2, 2000, False),  # given up, parallel BFS, levels still drive the second trial
+])
+def test_rcm_orders_kept_and_given_up(m, fill, reach, kept):
+    """The BFS trials track their bandwidth and give an order up as soon as
+    it cannot be kept (only its levels are filled from then on); kept and
+    given-up orders both match the oracle at any thread count."""
+    if kept:
+        rp, ci, v = symmetric_permuted(m, fill, reach, m)
+    else:
+        rp, ci, v, _ = convection_diffusion_csr(m=m, fill_per_row=fill, fill_reach=reach, seed=m)
+    for threads in (1, 4, 8):
+        r = check_against_oracle(rp, ci, v, 8, "double", 1e-4, threads)
+        assert (r["k_reorder"] < r["k_db"]) == kept
+
