@@ -573,7 +573,7 @@ static bool cm_bfs(int root, int nb, int ne, int trial, const std::vector<int>& 
 static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& off, const std::vector<int>& adj,
                           const std::vector<int>& degree, std::vector<int>& pushed, std::vector<int>& level,
                           std::vector<int>& order, std::vector<int>& claim, int give_up = 0,
-                          bool* gave_up = nullptr, int* bandwidth = nullptr, bool keep_levels = false) {
+                          bool* gave_up = nullptr, bool keep_levels = false) {
   constexpr int kSerialBatch = 384;
   const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
   int h0 = 0, t0 = 1, scan = 0, serial_total = 0;
@@ -728,7 +728,6 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
       }
     }
   }
-  if (bandwidth) *bandwidth = bw;
   return ok;
 }
 
@@ -788,7 +787,7 @@ int Pipeline<T>::rcm() {
     // gives it up as soon as it cannot; the first trial still fills its
     // levels (the next trial's root comes from them), the last one stops
     bool gave_up = false;
-    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, best_bw, &gave_up, nullptr,
+    if (!cm_bfs_levels(root, n, trial, off, adj, degree, pushed, level, order, claim, best_bw, &gave_up,
                        trial == 0))
       break;
     if (!gave_up) {
