@@ -742,7 +742,8 @@ int Pipeline<T>::rcm() {
   const int nz = (int)m_ci.size();
   std::vector<int>& row = ws_i0;
   row.resize(nz);
-  std::vector<int> degree(n);
+  std::vector<int>& degree = bfs_degree;
+  degree.resize(n);
 #pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) row[e] = i;

@@ -72,7 +72,7 @@ class Pipeline {
   std::vector<int> db_match, db_bset, db_irn, db_prev, db_owner;
   std::vector<char> db_rowdone, db_coldone, db_inb, db_visited;
   std::vector<char> bfs_tried;
-  std::vector<int> bfs_pushed, bfs_level, bfs_order, bfs_claim;
+  std::vector<int> bfs_pushed, bfs_level, bfs_order, bfs_claim, bfs_degree;
   // per partition of the second level: its adjacency, row lengths and BFS
   // queue (kept, so that the partitions' threads do not allocate and fault
   // in new pages side by side on every setup)
