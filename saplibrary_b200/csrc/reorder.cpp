@@ -936,17 +936,31 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   for (int i = 0; i < n; i++) {
     const int a = m_rp[i];
     int w = a;
+    bool ascending = true;
     for (int e = rp0[i]; e < rp0[i + 1]; e++) {
       if (std::abs(i - ci0[e]) > dkeep) continue;
-      // insertion by decreasing column (columns of a row are distinct)
-      int t = w++;
-      while (t > a && m_ci[t - 1] < ci0[e]) {
-        m_ci[t] = m_ci[t - 1];
-        m_val[t] = m_val[t - 1];
-        t--;
+      ascending = ascending && (w == a || m_ci[w - 1] < ci0[e]);
+      m_ci[w] = ci0[e];
+      m_val[w++] = v0[e];
+    }
+    // decreasing column order (the columns of a row are distinct, so the
+    // order is unique): a row kept in increasing order is reversed, any
+    // other sorted by insertion
+    if (ascending) {
+      std::reverse(m_ci.begin() + a, m_ci.begin() + w);
+      std::reverse(m_val.begin() + a, m_val.begin() + w);
+    } else {
+      for (int q = a + 1; q < w; q++) {
+        const int c = m_ci[q];
+        const T x = m_val[q];
+        int t = q;
+        for (; t > a && m_ci[t - 1] < c; t--) {
+          m_ci[t] = m_ci[t - 1];
+          m_val[t] = m_val[t - 1];
+        }
+        m_ci[t] = c;
+        m_val[t] = x;
       }
-      m_ci[t] = ci0[e];
-      m_val[t] = v0[e];
     }
   }
   return kres;
