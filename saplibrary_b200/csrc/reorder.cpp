@@ -1173,13 +1173,18 @@ void Pipeline<T>::assemble_var_band(int P) {
 #pragma omp parallel
   {
     std::vector<int> kp(P, 0);
+    // the diagonal blocks' entries lie in their row's partition: one
+    // division per row (the range test keeps any other entry exact)
+    auto first = [&](int p) { return p * q + std::min(p, rem); };
 #pragma omp for schedule(static) nowait
-    for (int j = 0; j < n; j++)
+    for (int j = 0; j < n; j++) {
+      const int pr = partition_of(j, q, rem), lo = first(pr), hi = first(pr + 1);
       for (int e = d_rp[j]; e < d_rp[j + 1]; e++) {
         const int l = d_ci[e];
-        const int p = partition_of(l, q, rem);
+        const int p = (l >= lo && l < hi) ? pr : partition_of(l, q, rem);
         kp[p] = std::max(kp[p], std::abs(l - j));
       }
+    }
 #pragma omp critical
     for (int p = 0; p < P; p++) part_k[p] = std::max(part_k[p], kp[p]);
   }
