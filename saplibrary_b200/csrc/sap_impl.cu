@@ -494,15 +494,29 @@ class PrecondT : public PrecBase {
     K = pl.K;
     P = pl.P;
     var_band = pl.var_band;
-    final_pos_h = pl.final_pos;
-    final_order_h = pl.final_order;
-    db_row_perm_h = pl.db_row_perm;
+    // the permutations kept for sap_solver_get_reorder (copied in parallel)
+    auto keep = [](std::vector<int>& dst, const std::vector<int>& src) {
+      dst.resize(src.size());
+      const long long m = (long long)src.size();
+#pragma omp parallel for schedule(static)
+      for (int c = 0; c < 16; c++) std::copy(src.begin() + m * c / 16, src.begin() + m * (c + 1) / 16, dst.begin() + m * c / 16);
+    };
+    keep(final_pos_h, pl.final_pos);
+    keep(final_order_h, pl.final_order);
+    keep(db_row_perm_h, pl.db_row_perm);
     first_rows_h = pl.first_rows;
     part_k_h = pl.part_k;
-    // leftTrans / rightTrans as gathers and scatters in band order
+    // leftTrans / rightTrans as gathers and scatters in band order, built in
+    // a page-locked buffer kept across setups and uploaded asynchronously
+    // (later synchronisations on the stream precede the buffer's reuse)
     {
-      std::vector<int> gin(n), sout(n);
-      std::vector<T> sn(n), cn(n);
+      const size_t tw = ((size_t)n * sizeof(T) + sizeof(int) - 1) / sizeof(int);
+      SAPB_CUDA(cudaStreamSynchronize(st));  // the previous setup's uploads from the buffer are done
+      int* pin = gather_pin.reserve(2 * (size_t)n + 2 * tw);
+      int* gin = pin;
+      int* sout = pin + n;
+      T* sn = reinterpret_cast<T*>(pin + 2 * (size_t)n);
+      T* cn = reinterpret_cast<T*>(pin + 2 * (size_t)n + tw);
 #pragma omp parallel for schedule(static, 4096)
       for (int q = 0; q < n; q++) {
         gin[pl.final_pos[q]] = q;
@@ -510,10 +524,10 @@ class PrecondT : public PrecBase {
         sout[q] = pl.final_order[q];
         cn[q] = pl.scale ? (T)pl.col_scale[pl.final_order[q]] : T(1);
       }
-      gin_d.upload(gin, st);
-      sout_d.upload(sout, st);
-      sin_d.upload(sn, st);
-      cout_d.upload(cn, st);
+      gin_d.upload(gin, n, st);
+      sout_d.upload(sout, n, st);
+      sin_d.upload(sn, n, st);
+      cout_d.upload(cn, n, st);
     }
     reordered = true;
     if (!var_band) {
@@ -536,7 +550,6 @@ class PrecondT : public PrecBase {
     parts_h.resize(P);
     const int q = n / P, r = n % P;
     long long off = 0;
-    std::vector<int> partcol(n);
     for (int p = 0; p < P; p++) {
       PartDev d{};
       d.start = p * q + std::min(p, r);
@@ -546,10 +559,13 @@ class PrecondT : public PrecBase {
       d.boff = off;
       off += (long long)d.size * (2 * d.K + 1);
       parts_h[p] = d;
-      for (int i = d.start; i < d.start + d.size; i++) partcol[i] = p;
     }
+    partcol_h.resize(n);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < P; p++)
+      std::fill(partcol_h.begin() + parts_h[p].start, partcol_h.begin() + parts_h[p].start + parts_h[p].size, p);
     parts_d.upload(parts_h, st);
-    partcol_d.upload(partcol, st);
+    partcol_d.upload(partcol_h, st);
     boff_total = off;
     upload_coo(pl.d_rp, pl.d_ci, pl.d_val);
     cp_idx.upload(pl.offd_idx, st);
@@ -569,6 +585,8 @@ class PrecondT : public PrecBase {
   DBuf<double> db_wd, db_md;          // DB weights and row maxima on the device
   PinnedBuf<double> db_wh, db_mh;     // and their page-locked host copies
   PinnedBuf<int> coo_pin;  // staging of the COO uploads
+  PinnedBuf<int> gather_pin;  // staging of the band-order gathers and scales
+  std::vector<int> partcol_h;  // partition of every band row (kept across setups)
 
   // device COO (band rows, columns, values) of a CSR in band order
   // (through a page-locked staging buffer: rows, columns and values are
