@@ -827,10 +827,14 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   const int nz = (int)m_ci.size();
   // The reference's bucketed list: entries ordered by distance |i - j|, rows
   // ascending and CSR order inside a distance group.  Group d occupies
-  // [gstart[d], gstart[d+1]); only the values are needed (for the squares).
-  // Built in parallel as a stable bucket sort: every thread counts the
-  // distances of its block of rows, the counts become per-(distance, thread)
-  // offsets, and each thread places its rows' values in order.
+  // [gstart[d], gstart[d+1]); only the values are needed (for the squares),
+  // and only of the groups the walk below reaches.  Built in parallel as a
+  // stable bucket sort: every thread counts the distances of its block of
+  // rows (and sums their squares in double), the counts become
+  // per-(distance, block) offsets, and each block's values are placed in
+  // order.  Values are placed for the groups down to a few below where the
+  // same walk over the double sums stops; the exact walk fills the rest
+  // first if it goes further.
   // The sum of squares of all entries is a sequential sum in entry order
   // (the reference's order): one extra thread runs it meanwhile.
   T total = T(0);
@@ -845,53 +849,101 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) dmax = std::max(dmax, std::abs(i - m_ci[e]));
   const int nd = dmax + 1;
   std::vector<int>& gstart = ws_i1;
-  gstart.assign(n + 1, 0);
+  gstart.resize(nd + 1);
   std::vector<T>& bv = ws_t0;
   bv.resize(nz);
-  const int nt = std::max(1, std::min(omp_get_max_threads(), 16));
+  const int nb = std::max(1, std::min(omp_get_max_threads(), 16));  // row blocks
   std::vector<int>& cnt = ws_cnt;
-  cnt.resize((size_t)nt * nd);
-#pragma omp parallel num_threads(nt)
-  {
-    const int t = omp_get_thread_num(), nth = omp_get_num_threads();
-    const int r0 = (int)((long long)n * t / nth), r1 = (int)((long long)n * (t + 1) / nth);
-    int* c = cnt.data() + (size_t)t * nd;
+  cnt.resize((size_t)nb * nd);
+  std::vector<double> sq((size_t)nb * nd);
+  auto block = [&](int u) { return (int)((long long)n * u / nb); };
+#pragma omp parallel for schedule(static, 1) num_threads(nb)
+  for (int u = 0; u < nb; u++) {
+    int* c = cnt.data() + (size_t)u * nd;
+    double* q = sq.data() + (size_t)u * nd;
     std::fill(c, c + nd, 0);
-    for (int i = r0; i < r1; i++)
-      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) c[std::abs(i - m_ci[e])]++;
-#pragma omp barrier
-#pragma omp single
-    {
-      int run = 0;
-      for (int d = 0; d < nd; d++) {
-        gstart[d] = run;
-        for (int u = 0; u < nth; u++) {
-          int& v = cnt[(size_t)u * nd + d];
-          const int k = v;
-          v = run;
-          run += k;
-        }
+    std::fill(q, q + nd, 0.0);
+    for (int i = block(u); i < block(u + 1); i++)
+      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) {
+        const int d = std::abs(i - m_ci[e]);
+        c[d]++;
+        q[d] += (double)m_val[e] * (double)m_val[e];
       }
-      for (int d = nd; d <= n; d++) gstart[d] = run;
-    }
-    for (int i = r0; i < r1; i++)
-      for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bv[c[std::abs(i - m_ci[e])]++] = m_val[e];
   }
+  std::vector<double> gsq(nd, 0.0);
+  {
+    int run = 0;
+    for (int d = 0; d < nd; d++) {
+      gstart[d] = run;
+      for (int u = 0; u < nb; u++) {
+        int& v = cnt[(size_t)u * nd + d];
+        const int k = v;
+        v = run;
+        run += k;
+        gsq[d] += sq[(size_t)u * nd + d];
+      }
+    }
+    gstart[nd] = run;
+  }
+  // place the values of groups [lo, hi)
+  auto place = [&](int lo, int hi) {
+#pragma omp parallel for schedule(static, 1) num_threads(nb)
+    for (int u = 0; u < nb; u++) {
+      int* c = cnt.data() + (size_t)u * nd;
+      for (int i = block(u); i < block(u + 1); i++)
+        for (int e = m_rp[i]; e < m_rp[i + 1]; e++) {
+          const int d = std::abs(i - m_ci[e]);
+          if (d >= lo && d < hi) bv[c[d]++] = m_val[e];
+        }
+    }
+  };
+  auto lower = [&](int g) {
+    do g--; while (g > 0 && gstart[g] == gstart[g + 1]);
+    return g;
+  };
+  // where the walk stops on the double sums
+  int filled = nd;
+  {
+    double tot = 0.0;
+    for (int d = 0; d < nd; d++) tot += gsq[d];
+    const double keep_a = (1.0 - (double)frac) * tot;
+    double kept_a = tot;
+    int g = lower(nd);
+    while (g > max_bw) {
+      kept_a -= gsq[g];
+      g = lower(g);
+    }
+    if (kept_a >= keep_a)
+      while (g > 0 && kept_a - gsq[g] >= keep_a) {
+        kept_a -= gsq[g];
+        g = lower(g);
+      }
+    constexpr int kSlack = 8;  // groups placed below the predicted stop
+    filled = std::max(0, g - kSlack);
+    // SAPB_DROPOFF_PLACE=all places every group first, =none none (the
+    // walk then places them when it reaches the first): both only for tests
+    const char* env = std::getenv("SAPB_DROPOFF_PLACE");
+    if (env && std::string(env) == "all") filled = 0;
+    if (env && std::string(env) == "none") filled = nd;
+    if (filled < nd) place(filled, nd);
+  }
+  auto need = [&](int g) {  // group g's values placed
+    if (g < filled) {
+      place(0, filled);
+      filled = 0;
+    }
+  };
   squares.join();
   const T keep_min = (T(1) - frac) * total;
   T kept = total;
   // walk the groups from the longest distance down, summing squares from
   // the end of the list backwards (the reference's order)
-  auto lower = [&](int g) {
-    do g--; while (g > 0 && gstart[g] == gstart[g + 1]);
-    return g;
-  };
-  int g = n;
-  g = lower(g);  // the top non-empty group
+  int g = lower(nd);  // the top non-empty group
   int kres = g;
   {
     T s = T(0);
     while (g > max_bw) {
+      need(g);
       for (int p = gstart[g + 1] - 1; p >= gstart[g]; p--) s = s + bv[p] * bv[p];
       g = lower(g);
     }
@@ -902,6 +954,7 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     for (;;) {
       const int d = g;
       if (d == 0) { kres = 0; break; }
+      need(g);
       T band = T(0);
       for (int p = gstart[g + 1] - 1; p >= gstart[g]; p--) band = band + bv[p] * bv[p];
       if (kept - band < keep_min) break;

@@ -192,3 +192,15 @@ def test_rcm_orders_kept_and_given_up(m, fill, reach, kept):
         r = check_against_oracle(rp, ci, v, 8, "double", 1e-4, threads)
         assert (r["k_reorder"] < r["k_db"]) == kept
 
+
+@pytest.mark.parametrize("place", ["all", "none"])
+def test_drop_off_group_placement_modes(place, monkeypatch):
+    """Drop-off places the values of the distance groups its walk is
+    predicted to reach (from double sums) and the rest when the exact walk
+    goes further; placing all groups first, or none (every group placed on
+    demand), gives the same outputs, equal to the oracle's."""
+    monkeypatch.setenv("SAPB_DROPOFF_PLACE", place)
+    rp, ci, v, _ = convection_diffusion_csr(m=120, fill_reach=600, seed=12)
+    for drop, dtype, threads in ((1e-4, "float", 4), (1e-2, "double", 3), (0.0, "float", 1)):
+        check_against_oracle(rp, ci, v, 8, dtype, drop, threads)
+
