@@ -843,8 +843,10 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
     for (int e = 0; e < nz; e++) s = s + m_val[e] * m_val[e];
     total = s;
   });
+  // the passes beside it leave that thread a core
+  const int nb = std::max(1, std::min(omp_get_max_threads() - 1, 16));  // threads and row blocks
   int dmax = 0;
-#pragma omp parallel for schedule(static, 4096) reduction(max : dmax)
+#pragma omp parallel for schedule(static, 4096) reduction(max : dmax) num_threads(nb)
   for (int i = 0; i < n; i++)
     for (int e = m_rp[i]; e < m_rp[i + 1]; e++) dmax = std::max(dmax, std::abs(i - m_ci[e]));
   const int nd = dmax + 1;
@@ -852,7 +854,6 @@ int Pipeline<T>::drop_off(T frac, int max_bw) {
   gstart.resize(nd + 1);
   std::vector<T>& bv = ws_t0;
   bv.resize(nz);
-  const int nb = std::max(1, std::min(omp_get_max_threads(), 16));  // row blocks
   std::vector<int>& cnt = ws_cnt;
   cnt.resize((size_t)nb * nd);
   std::vector<double> sq((size_t)nb * nd);
