@@ -19,6 +19,7 @@
 #include <limits>
 #include <queue>
 #include <thread>
+#include <type_traits>
 #include <utility>
 
 #include <omp.h>
@@ -169,19 +170,29 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
   std::vector<int>& owner = pfill(db_owner, n, INT_MAX);
   best_e.resize(n);
   best_r.resize(n);
+  // every row holds its largest entry at weight log(1) = +0, so the row
+  // minima u are +0 as a rule, and weight - (+0) is weight bit for bit: the
+  // scattered reads of u are then skipped
+  bool u_zero = true;
+#pragma omp parallel for schedule(static) reduction(&& : u_zero)
+  for (int i = 0; i < n; i++) u_zero = u_zero && u[i] == 0.0 && !std::signbit(u[i]);
+  auto column_best = [&](auto skip_u) {
 #pragma omp parallel for schedule(static, 4096)
-  for (int i = 0; i < n; i++) {
-    int best = -1;
-    double vi = kInf;
-    for (int e = Rp[i]; e < Rp[i + 1]; e++) {
-      if (weight[e] > kInf / 2.0) continue;
-      double red = weight[e] - u[Ci[e]];
-      if (vi > red) { vi = red; best = e; }
+    for (int i = 0; i < n; i++) {
+      int best = -1;
+      double vi = kInf;
+      for (int e = Rp[i]; e < Rp[i + 1]; e++) {
+        if (weight[e] > kInf / 2.0) continue;
+        const double red = decltype(skip_u)::value ? weight[e] : weight[e] - u[Ci[e]];
+        if (vi > red) { vi = red; best = e; }
+      }
+      v[i] = vi;
+      best_e[i] = best;
+      best_r[i] = best >= 0 ? Ci[best] : -1;
     }
-    v[i] = vi;
-    best_e[i] = best;
-    best_r[i] = best >= 0 ? Ci[best] : -1;
-  }
+  };
+  if (u_zero) column_best(std::true_type{});
+  else column_best(std::false_type{});
   int* own = owner.data();
   // a first pass of plain stores leaves in owner[r] one of the columns that
   // chose r (writes to different rows overlap; atomic updates would not);
