@@ -750,19 +750,11 @@ static bool cm_bfs_levels(int root, int n, int trial, const std::vector<int>& of
 // bandwidth of the current order.
 template <typename T>
 int Pipeline<T>::rcm() {
-  const int nz = (int)m_ci.size();
-  std::vector<int>& row = ws_i0;
-  row.resize(nz);
   std::vector<int>& degree = bfs_degree;
   degree.resize(n);
 #pragma omp parallel for schedule(static, 4096)
-  for (int i = 0; i < n; i++) {
-    for (int e = m_rp[i]; e < m_rp[i + 1]; e++) row[e] = i;
-    degree[i] = m_rp[i + 1] - m_rp[i];
-  }
-  int best_bw = 0;
-#pragma omp parallel for reduction(max : best_bw) schedule(static)
-  for (int e = 0; e < nz; e++) best_bw = std::max(best_bw, std::abs(row[e] - m_ci[e]));
+  for (int i = 0; i < n; i++) degree[i] = m_rp[i + 1] - m_rp[i];
+  int best_bw = k_db;  // the current order's bandwidth (same matrix)
   std::vector<int>& off = ws_off;
   std::vector<int>& adj = ws_adj;
   symmetric_adjacency_csr(n, m_rp, m_ci, off, adj, ws_cnt, ws_i1, ws_i2);
@@ -806,8 +798,11 @@ int Pipeline<T>::rcm() {
 #pragma omp parallel for schedule(static)
       for (int k = 0; k < n; k++) rcm_pos[order[k]] = k;
       int bw = 0;
-#pragma omp parallel for reduction(max : bw) schedule(static)
-      for (int e = 0; e < nz; e++) bw = std::max(bw, std::abs(rcm_pos[row[e]] - rcm_pos[m_ci[e]]));
+#pragma omp parallel for reduction(max : bw) schedule(static, 4096)
+      for (int i = 0; i < n; i++) {
+        const int pi = rcm_pos[i];
+        for (int e = m_rp[i]; e < m_rp[i + 1]; e++) bw = std::max(bw, std::abs(pi - rcm_pos[m_ci[e]]));
+      }
       if (best_bw > bw) {
         best_bw = bw;
         rcm_order = order;
