@@ -346,28 +346,30 @@ void Pipeline<T>::db(const double* weight, const double* rowmax) {
 // graph.h:1764-1809).
 // obase: node x's range is off[x - obase]; 0 gives an array of n + 1 over
 // all nodes, nb one of ne - nb + 1 over the partition's nodes only.
-static void symmetric_adjacency(const std::vector<int>& er, const std::vector<int>& ec, int e0, int e1, int nb,
-                                int ne, int n, std::vector<int>& off, std::vector<int>& adj, int obase,
-                                std::vector<int>& pos) {
-  // each edge (r, c), r != c, contributes (r -> c) then (c -> r); a node's
-  // neighbours keep the order of these contributions
+static void symmetric_adjacency(const std::vector<int>& rp, const std::vector<int>& ci, int nb, int ne, int n,
+                                std::vector<int>& off, std::vector<int>& adj, int obase, std::vector<int>& pos) {
+  // the edges are the entries of rows [nb, ne) in CSR order; each edge
+  // (r, c), r != c, contributes (r -> c) then (c -> r); a node's neighbours
+  // keep the order of these contributions
   off.assign(obase ? ne - nb + 1 : n + 1, 0);
   auto o = [&](int x) -> int& { return off[x - obase]; };  // x in [nb, ne]
-  for (int e = e0; e < e1; e++) {
-    if (er[e] == ec[e]) continue;
-    o(er[e])++;
-    o(ec[e])++;
-  }
+  for (int r = nb; r < ne; r++)
+    for (int e = rp[r]; e < rp[r + 1]; e++) {
+      if (ci[e] == r) continue;
+      o(r)++;
+      o(ci[e])++;
+    }
   for (int i = nb + 1; i <= ne; i++) o(i) += o(i - 1);
   for (int i = ne - 1; i >= nb; i--) o(i) = i > nb ? o(i - 1) : 0;  // exclusive starts
   adj.resize(o(ne));
   pos.assign(off.begin() + (nb - obase), off.begin() + (ne - obase));
-  for (int e = e0; e < e1; e++) {
-    const int r = er[e], c = ec[e];
-    if (r == c) continue;
-    adj[pos[r - nb]++] = c;
-    adj[pos[c - nb]++] = r;
-  }
+  for (int r = nb; r < ne; r++)
+    for (int e = rp[r]; e < rp[r + 1]; e++) {
+      const int c = ci[e];
+      if (r == c) continue;
+      adj[pos[r - nb]++] = c;
+      adj[pos[c - nb]++] = r;
+    }
 }
 
 // The same adjacency for a whole CSR matrix (rows rp, columns ci), built in
@@ -1104,12 +1106,6 @@ void Pipeline<T>::assemble_coupling(int K, int P) {
 template <typename T>
 void Pipeline<T>::second_level(int K, int P) {
   const int q = n / P, rem = n % P;
-  const int dz = (int)d_ci.size();
-  std::vector<int>& row = ws_i0;
-  row.resize(dz);
-#pragma omp parallel for schedule(static)
-  for (int i = 0; i < n; i++)
-    for (int e = d_rp[i]; e < d_rp[i + 1]; e++) row[e] = i;
   pfill(second_order, n, 0);
   pfill(second_pos, n, 0);
   std::vector<int>& order = pfill(bfs_order, n, 0);
@@ -1128,15 +1124,15 @@ void Pipeline<T>::second_level(int K, int P) {
   // is then redone serially in order, as the reference does.
   auto part = [&](int p, bool serial) -> bool {
     const int nb = pnb[p], ne = pnb[p + 1];
-    const int e0 = d_rp[nb], e1 = d_rp[ne];
     for (int i = nb; i < ne; i++) second_order[i] = i;
     int best_bw = 0;
-    for (int e = e0; e < e1; e++) best_bw = std::max(best_bw, std::abs(row[e] - d_ci[e]));
+    for (int i = nb; i < ne; i++)
+      for (int e = d_rp[i]; e < d_rp[i + 1]; e++) best_bw = std::max(best_bw, std::abs(i - d_ci[e]));
     PartScratch& sc = part_scratch[p];
     std::vector<int>& off = sc.off;
     std::vector<int>& adj = sc.adj;
     const int obase = serial ? 0 : nb;
-    symmetric_adjacency(row, d_ci, e0, e1, nb, ne, n, off, adj, obase, sc.pos);
+    symmetric_adjacency(d_rp, d_ci, nb, ne, n, off, adj, obase, sc.pos);
     // row lengths of the partition's nodes as the reference computes them:
     // its transform covers row_offsets[nb+1 .. ne), one element short, so the
     // partition's last node keeps degree 0 (graph.h:1622-1625), which makes
@@ -1187,7 +1183,10 @@ void Pipeline<T>::second_level(int K, int P) {
       if (!gave_up) {
         for (int k = nb; k < ne; k++) second_pos[order[k]] = k;
         int bw = 0;
-        for (int e = e0; e < e1; e++) bw = std::max(bw, std::abs(second_pos[row[e]] - second_pos[d_ci[e]]));
+        for (int i = nb; i < ne; i++) {
+          const int pi = second_pos[i];
+          for (int e = d_rp[i]; e < d_rp[i + 1]; e++) bw = std::max(bw, std::abs(pi - second_pos[d_ci[e]]));
+        }
         if (best_bw > bw) {
           best_bw = bw;
           std::copy(order.begin() + nb, order.begin() + ne, second_order.begin() + nb);
