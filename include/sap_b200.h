@@ -282,6 +282,14 @@ int sap_reorder_host(int n, int nnz, const int* row_offsets, const int* column_i
                      int num_partitions, const sap_options* opts, int prec_dtype, int threads,
                      sap_reorder_info* info, int* db_row_perm, int* final_pos, int* final_order, int* first_rows,
                      int* part_k);
+/* Wall time (ms) of the stages of the calling thread's last successful
+ * sap_reorder_host, in order ("db", "rcm", "drop_off", then for a variable
+ * band "coupling", "second_level", "assemble", and "compose"): *count is
+ * set to their number, and up to cap of them are written to names (static
+ * strings) and ms (either may be NULL).  Extension, no reference
+ * counterpart (the reference's Stats hold timeDB, timeReorder and
+ * timeDropoff for a setup). */
+int sap_reorder_host_stages(int cap, const char** names, double* ms, int* count);
 /* The cudaStream_t all device work of this solver is enqueued on. */
 void* sap_solver_stream(const sap_solver* s);
 /* Layout of the wide-band block path after setup: the block size and the

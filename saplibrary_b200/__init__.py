@@ -133,6 +133,7 @@ _sig = {
     "sap_solver_stream": (_vp, [_vp]),
     "sap_solver_get_reorder": (_i, [_vp, _i, _vp, ctypes.POINTER(ctypes.c_int64)]),
     "sap_reorder_host": (_i, [_i, _i, _vp, _vp, _vp, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "sap_reorder_host_stages": (_i, [_i, _vp, _vp, ctypes.POINTER(_i)]),
     "sap_blas_dots": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_blas_dots_noalloc": (_i, [_i, _i, _pp, _pp, _vp, _vp]),
     "sap_tc_gemm_batched": (_i, [_i, _i, _i, ctypes.c_float, _vp, _i, ctypes.c_longlong, _vp, _i, ctypes.c_longlong,
@@ -248,9 +249,10 @@ def reorder_host(row_offsets, column_indices, values, num_partitions: int, opts:
                  prec: str = "float", threads: int = 0) -> dict:
     """The host reordering of a CSR setup on its own, without a device
     (`sap_reorder_host`): DB, RCM, drop-off, second level and the composed
-    permutations.  Returns K, P, k_db, k_reorder, var_band, drop_actual and
+    permutations.  Returns K, P, k_db, k_reorder, var_band, drop_actual,
     the arrays dbRowPerm, finalPerm, finalReordering, first_rows, ks (the
-    names of Solver.getReorder)."""
+    names of Solver.getReorder) and stage_ms (wall time of each stage,
+    `sap_reorder_host_stages`)."""
     rp = np.ascontiguousarray(row_offsets, np.int32)
     ci = np.ascontiguousarray(column_indices, np.int32)
     v = np.ascontiguousarray(values, np.float64)
@@ -271,6 +273,11 @@ def reorder_host(row_offsets, column_indices, values, num_partitions: int, opts:
     res["ks"] = out["ks"][:info.P]
     for k in ("dbRowPerm", "finalPerm", "finalReordering"):
         res[k] = out[k]
+    cnt = _i(0)
+    names, ms = (ctypes.c_char_p * 16)(), (ctypes.c_double * 16)()
+    _check(_lib.sap_reorder_host_stages(16, ctypes.cast(names, ctypes.c_void_p), ctypes.cast(ms, ctypes.c_void_p),
+                                        ctypes.byref(cnt)))
+    res["stage_ms"] = {names[i].decode(): ms[i] for i in range(min(cnt.value, 16))}
     return res
 
 

@@ -1326,6 +1326,9 @@ void set_last_error(const std::string& msg);
 
 namespace {
 
+// stage times of the calling thread's last sap_reorder_host
+thread_local std::vector<std::pair<const char*, double>> g_last_stages;
+
 // The host part of a CSR setup on its own: explicit zeros removed in T,
 // DB weights log(rowmax / |a|) computed on the host (std::log), the
 // pipeline, and its outputs copied out.
@@ -1341,25 +1344,32 @@ int reorder_host(int n, int nnz, const int* rp, const int* ci, const double* v, 
   pl.drop_frac = o.dropOffFraction;
   pl.max_bandwidth = o.maxBandwidth;
   pl.var_band = o.variableBandwidth != 0;
+  // (row-parallel: count, prefix, fill; then the weights per row)
   pl.in_rp.assign(n + 1, 0);
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; i++) {
     int c = 0;
     for (int e = rp[i]; e < rp[i + 1]; e++) c += (T)v[e] != T(0);
-    pl.in_rp[i + 1] = pl.in_rp[i] + c;
+    pl.in_rp[i + 1] = c;
   }
+  rp::prefix_sum(pl.in_rp.data(), n);
   pl.in_ci.resize(pl.in_rp[n]);
   pl.in_val.resize(pl.in_rp[n]);
-  for (int i = 0, d = 0; i < n; i++)
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; i++) {
+    int d = pl.in_rp[i];
     for (int e = rp[i]; e < rp[i + 1]; e++)
       if ((T)v[e] != T(0)) {
         pl.in_ci[d] = ci[e];
         pl.in_val[d++] = (T)v[e];
       }
+  }
   pl.nnz = (int)pl.in_ci.size();
   std::vector<double> w, rmax;
   if (pl.do_db) {
     w.resize(pl.nnz);
     rmax.resize(n);
+#pragma omp parallel for schedule(static, 4096)
     for (int i = 0; i < n; i++) {
       double m = 0.0;
       for (int e = pl.in_rp[i]; e < pl.in_rp[i + 1]; e++) m = std::max(m, std::fabs((double)pl.in_val[e]));
@@ -1368,6 +1378,7 @@ int reorder_host(int n, int nnz, const int* rp, const int* ci, const double* v, 
     }
   }
   pl.run(w.data(), rmax.data());
+  g_last_stages = pl.stage_ms;
   info->K = pl.K;
   info->P = pl.P;
   info->k_db = pl.k_db;
@@ -1401,16 +1412,19 @@ extern "C" int sap_reorder_host(int n, int nnz, const int* rp, const int* ci, co
     set_last_error("row offsets inconsistent with nnz");
     return SAP_ERR_INVALID_ARGUMENT;
   }
-  for (int i = 0; i < n; i++)
-    if (rp[i] > rp[i + 1]) {
-      set_last_error("row offsets not monotone");
-      return SAP_ERR_INVALID_ARGUMENT;
-    }
-  for (int e = 0; e < nnz; e++)
-    if (ci[e] < 0 || ci[e] >= n) {
-      set_last_error("column index out of range");
-      return SAP_ERR_INVALID_ARGUMENT;
-    }
+  int bad_rp = 0, bad_ci = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad_rp)
+  for (int i = 0; i < n; i++) bad_rp |= rp[i] > rp[i + 1];
+  if (bad_rp) {
+    set_last_error("row offsets not monotone");
+    return SAP_ERR_INVALID_ARGUMENT;
+  }
+#pragma omp parallel for schedule(static) reduction(| : bad_ci)
+  for (int e = 0; e < nnz; e++) bad_ci |= ci[e] < 0 || ci[e] >= n;
+  if (bad_ci) {
+    set_last_error("column index out of range");
+    return SAP_ERR_INVALID_ARGUMENT;
+  }
   const int saved = omp_get_max_threads();
   if (threads > 0) omp_set_num_threads(threads);
   int rc = SAP_OK;
@@ -1429,4 +1443,18 @@ extern "C" int sap_reorder_host(int n, int nnz, const int* rp, const int* ci, co
   }
   if (threads > 0) omp_set_num_threads(saved);
   return rc;
+}
+
+extern "C" int sap_reorder_host_stages(int cap, const char** names, double* ms, int* count) {
+  using namespace sapb;
+  if (!count || cap < 0) {
+    set_last_error("invalid arguments to sap_reorder_host_stages");
+    return SAP_ERR_INVALID_ARGUMENT;
+  }
+  *count = (int)g_last_stages.size();
+  for (int i = 0; i < cap && i < *count; i++) {
+    if (names) names[i] = g_last_stages[i].first;
+    if (ms) ms[i] = g_last_stages[i].second;
+  }
+  return SAP_OK;
 }

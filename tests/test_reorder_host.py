@@ -204,3 +204,12 @@ def test_drop_off_group_placement_modes(place, monkeypatch):
     for drop, dtype, threads in ((1e-4, "float", 4), (1e-2, "double", 3), (0.0, "float", 1)):
         check_against_oracle(rp, ci, v, 8, dtype, drop, threads)
 
+
+def test_stage_times_are_reported():
+    """sap_reorder_host_stages returns the last call's stage times in order."""
+    rp, ci, v, _ = convection_diffusion_csr(m=80, fill_reach=400, seed=8)
+    r = sap.reorder_host(rp, ci, v, 6, sap.Options(dropOffFraction=1e-4), prec="float", threads=2)
+    assert list(r["stage_ms"]) == ["db", "rcm", "drop_off", "coupling", "second_level", "assemble", "compose"]
+    assert all(t >= 0.0 for t in r["stage_ms"].values())
+    assert sap._lib.sap_reorder_host_stages(-1, None, None, None) == -100  # SAP_ERR_INVALID_ARGUMENT
+
