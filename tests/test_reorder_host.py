@@ -213,3 +213,41 @@ def test_stage_times_are_reported():
     assert all(t >= 0.0 for t in r["stage_ms"].values())
     assert sap._lib.sap_reorder_host_stages(-1, None, None, None) == -100  # SAP_ERR_INVALID_ARGUMENT
 
+
+def test_seeded_mix_with_bandwidth_caps():
+    """A seeded mix of the families above with drop-off fractions up to 5 %,
+    maximum bandwidths that cut (first drop-off phase) or skip RCM (<= 64),
+    1 to 19 partitions and 1 to 8 host threads, all against the oracle."""
+    rng = np.random.default_rng(123)
+    for it in range(24):
+        kind, seed = it % 4, int(rng.integers(1 << 30))
+        if kind == 0:
+            m = int(rng.integers(10, 90))
+            rp, ci, v, _ = convection_diffusion_csr(m=m, fill_per_row=int(rng.integers(0, 3)),
+                                                    fill_reach=int(rng.integers(8, 6 * m)), seed=seed)
+        elif kind == 1:
+            rp, ci, v = random_sparse(int(rng.integers(200, 3000)), seed, band=int(rng.integers(5, 80)))
+        elif kind == 2:
+            rp, ci, v = random_unscaled(int(rng.integers(200, 2500)), seed, reach=int(rng.integers(5, 100)))
+        else:
+            m = int(rng.integers(10, 60))
+            rp, ci, v = symmetric_permuted(m, int(rng.integers(0, 3)), int(rng.integers(8, 3 * m)), seed)
+        P, dtype = int(rng.integers(1, 20)), ["float", "double"][it % 2]
+        drop = float(rng.choice([0.0, 1e-5, 1e-4, 1e-3, 1e-2, 0.05]))
+        threads = int(rng.integers(1, 9))
+        maxbw = int(rng.choice([2**31 - 1, 2**31 - 1, int(rng.integers(1, 200)), 64, 65, 300]))
+        o = oracle.SparsePrecond(P, dtype=dtype, dropFrac=drop, maxBandwidth=maxbw)
+        rc = o.setup(rp, ci, v, factor=False, band=False)
+        opts = sap.Options(dropOffFraction=drop, maxBandwidth=maxbw)
+        if rc != 0:
+            with pytest.raises(sap.SystemError) as ei:
+                sap.reorder_host(rp, ci, v, P, opts, prec=dtype, threads=threads)
+            assert ei.value.reason == rc
+            continue
+        r = sap.reorder_host(rp, ci, v, P, opts, prec=dtype, threads=threads)
+        inf = o.info()
+        assert (r["K"], r["P"], r["k_db"], r["k_reorder"]) == (inf.K, inf.P, inf.k_db, inf.k_reorder), it
+        assert r["drop_actual"] == inf.drop_actual, it
+        for name in ARRAYS:
+            assert np.array_equal(r[name], o.ints(name)), (it, name)
+
